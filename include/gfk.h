@@ -1,0 +1,208 @@
+/*
+ * gfk.h — C ABI of libgfk, the B200 (sm_100a) Green's-function bank engine.
+ *
+ * libgfk computes what the reference's Go package internal/fk computes: the
+ * vertical surface displacement of a layered viscoelastic half-space per newton
+ * of vertical surface point force, integrated over horizontal wavenumber with a
+ * static-asymptote-subtracted trapezoid Hankel (J0) rule, for many ranges and
+ * frequencies at once. It also assembles the float32 range-major payload of an
+ * internal/bank file and writes the file.
+ *
+ * Every entry point takes plain C types: pointers, sizes and the structs below.
+ * Host pointers are host memory owned by the caller (pinned memory is faster but
+ * not required); device pointers are named d_* and live on the context's device.
+ * A context serialises its calls on one CUDA stream and is not thread-safe:
+ * concurrent callers either share one context behind a lock or use one each.
+ *
+ * Each function documents the reference interface it replaces as
+ * path:line within the reference project.
+ */
+#ifndef GFK_H
+#define GFK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+/* Each mirrors one class of Go error value returned by the reference. */
+enum gfk_status {
+    GFK_OK = 0,
+    GFK_EARG = 1,       /* non-positive k, f or r; empty range set
+                           (internal/fk/fk.go:277-279, 397-402, 465-474) */
+    GFK_ESTACK = 2,     /* layer.Stack.Validate failed (internal/layer/layer.go:53-73) */
+    GFK_EGUARD = 3,     /* k*h past MaxLayerPhase at the pole wavenumber
+                           (internal/fk/fk.go:242, 251-266); GFK_REFERENCE_DIRECT only */
+    GFK_ESINGULAR = 4,  /* singular layer propagator or surface system
+                           (internal/fk/fk.go:293-295, 322-324) */
+    GFK_ENONFINITE = 5, /* a result was NaN or Inf */
+    GFK_ETIMEOUT = 6,   /* a bounded device-side wait ran out */
+    GFK_ECUDA = 7,      /* CUDA runtime error; the message names the call */
+    GFK_ENOMEM = 8,     /* device or host allocation failed */
+    GFK_EIO = 9,        /* bank file could not be written or read */
+    GFK_ELIMIT = 10     /* a size beyond a documented maximum */
+};
+
+/* ---- how the boundary-value problem is solved --------------------------- */
+enum gfk_formulation {
+    /* The reference algorithm restated: direct 4x4 complex propagators
+     * exp(A k h) = E diag(e^(lambda k h)) E^-1, pivoted 4x4 surface solve,
+     * Qp = 2.25*Qs, real frequency, MaxLayerPhase guard on
+     * (internal/fk/fk.go:119-327, internal/fk/cmat.go:12-96). */
+    GFK_REFERENCE_DIRECT = 0,
+    /* Complex Dunkin second-compound (minor) propagation of the half-space's
+     * decaying 2-plane up to the surface, with closed-form, cancellation-free
+     * layer compounds; no k*h limit. Honours per-layer Qp and a complex
+     * frequency offset omega_imag. Design source internal/propmat/propmat.go:168-315. */
+    GFK_DUNKIN = 1
+};
+
+enum gfk_quadrature {
+    GFK_PLAIN_FP64 = 0,    /* FP64 wavenumber sum on the FP64 pipe */
+    GFK_SPLIT_INT8 = 1     /* shared-grid sum as an exact-integer-sliced tensor-core GEMM
+                              (tcgen05 kind::i8, s32 accumulate), FP64 recombination */
+};
+
+/* ---- medium --------------------------------------------------------------- */
+/* One homogeneous layer: internal/layer/layer.go:24-36 (layer.Layer). */
+typedef struct gfk_layer {
+    double thickness_m;   /* ignored for the last entry, the half-space */
+    double vp_mps;
+    double vs_mps;
+    double density_kgm3;
+    double qs;            /* <= 0: the medium's default_q, then 30 (fk.go:67-75) */
+    double qp;            /* <= 0: 2.25*Qs. Ignored by GFK_REFERENCE_DIRECT (fk.go:121-122) */
+} gfk_layer;
+
+/* fk.Medium (internal/fk/fk.go:37-53): layers[0..count-1], last = half-space. */
+typedef struct gfk_medium {
+    const gfk_layer *layers;
+    int32_t count;
+    int32_t _pad;
+    double ref_freq_hz;   /* Medium.RefFreq; <= 0 uses 30 Hz (fk.go:60-65) */
+    double default_q;     /* Medium.DefaultQ; <= 0 uses 30 (fk.go:67-75) */
+    double sls_tau_sigma; /* Medium.Relax (visco.SLS, internal/visco/visco.go:42-47):  */
+    double sls_tau_eps;   /* both > 0 replaces Kjartansson constant Q with one SLS    */
+} gfk_medium;
+
+/* fk.Integration (internal/fk/fk.go:330-341). */
+typedef struct gfk_integration {
+    int32_t samples;      /* <= 0: GridFor's own count (single-range calls: 20000) */
+    int32_t _pad;
+    double kmax_factor;   /* <= 0: 30 */
+} gfk_integration;
+
+/* fk.Grid (internal/fk/fk.go:446-449). */
+typedef struct gfk_grid {
+    double kmax;
+    int32_t samples;
+    int32_t _pad;
+} gfk_grid;
+
+typedef struct gfk_solve {
+    int32_t formulation;  /* enum gfk_formulation */
+    int32_t quadrature;   /* enum gfk_quadrature */
+    int32_t guard;        /* nonzero applies the MaxLayerPhase refusal; forced on by
+                             GFK_REFERENCE_DIRECT */
+    int32_t _pad;
+    double omega_imag;    /* complex-frequency offset w_I (rad/s): every frequency is
+                             evaluated at w - i*w_I. Must be 0 for GFK_REFERENCE_DIRECT. */
+} gfk_solve;
+
+/* ---- context -------------------------------------------------------------- */
+typedef struct gfk_ctx gfk_ctx;
+
+/* Creates a context on CUDA device `device`: one stream, a scratch arena. */
+int gfk_open(int device, gfk_ctx **out);
+int gfk_close(gfk_ctx *ctx);
+/* Short name of a status code. */
+const char *gfk_status_string(int status);
+/* Full message of the context's last failure, worded like the Go error. */
+const char *gfk_last_error(const gfk_ctx *ctx);
+/* Number of libgfk kernels launched by this context since it was opened. */
+int64_t gfk_kernel_launches(const gfk_ctx *ctx);
+
+/* ---- host-only helpers (no device work) ---------------------------------- */
+/* layer.Stack.Validate (internal/layer/layer.go:53-73). */
+int gfk_stack_validate(const gfk_medium *m);
+/* Medium.checkLayerPhase (internal/fk/fk.go:251-266): GFK_EGUARD past the limit. */
+int gfk_check_layer_phase(const gfk_medium *m, double freq_hz);
+/* Medium.GridFor (internal/fk/fk.go:464-495). */
+int gfk_grid_for(const gfk_medium *m, const double *ranges_m, int32_t nr,
+                 double freq_hz, gfk_integration opt, gfk_grid *out);
+
+/* ---- the path ------------------------------------------------------------- */
+/* Medium.SurfaceResponse (internal/fk/fk.go:276-327), batched over n (k, f)
+ * pairs. out holds n complex values as (re, im) pairs. */
+int gfk_surface_response(gfk_ctx *ctx, const gfk_medium *m, const gfk_solve *s,
+                         const double *k, const double *freq_hz, int64_t n,
+                         double *out);
+
+/* Medium.StaticCoefficient (internal/fk/fk.go:365-371). out: one (re, im). */
+int gfk_static_coefficient(gfk_ctx *ctx, const gfk_medium *m, const gfk_solve *s,
+                           double freq_hz, double k_far, double *out);
+
+/* Medium.VerticalDisplacement (internal/fk/fk.go:396-443). out: one (re, im). */
+int gfk_vertical_displacement(gfk_ctx *ctx, const gfk_medium *m, const gfk_solve *s,
+                              double range_m, double freq_hz, gfk_integration opt,
+                              double *out);
+
+/* Medium.VerticalDisplacementMulti (internal/fk/fk.go:506-550): one frequency,
+ * nr ranges. out: nr (re, im) pairs. */
+int gfk_vertical_displacement_multi(gfk_ctx *ctx, const gfk_medium *m, const gfk_solve *s,
+                                    const double *ranges_m, int32_t nr, double freq_hz,
+                                    gfk_integration opt, double *out);
+
+/* The bank build's per-bin loop (cmd/geobank/main.go:133-167) as one call:
+ * VerticalDisplacementMulti at nf frequencies. out: [nf][nr] (re, im) pairs.
+ * status_per_f (may be NULL): per-frequency status; the call returns the first
+ * non-OK one in frequency order, as geobank aborts on its first error
+ * (cmd/geobank/main.go:143-150,168-170). Results of failed frequencies are 0. */
+int gfk_bank_spectra(gfk_ctx *ctx, const gfk_medium *m, const gfk_solve *s,
+                     const double *ranges_m, int32_t nr,
+                     const double *freqs_hz, int32_t nf, gfk_integration opt,
+                     double *out, int32_t *status_per_f);
+
+/* ---- plans: device-resident repeated builds ------------------------------ */
+/* A plan fixes (medium, solve, ranges, frequencies, integration) and owns the
+ * device buffers; executing it recomputes everything (layer constants, static
+ * coefficients, propagators, J0 table, quadrature) on the context's stream with
+ * no host transfers. Used by the benchmark and by callers that keep results in
+ * device memory. */
+typedef struct gfk_plan gfk_plan;
+int gfk_plan_create(gfk_ctx *ctx, const gfk_medium *m, const gfk_solve *s,
+                    const double *ranges_m, int32_t nr,
+                    const double *freqs_hz, int32_t nf, gfk_integration opt,
+                    gfk_plan **out);
+int gfk_plan_execute(gfk_plan *p);
+/* Device pointer to the [nf][nr] complex128 result of the last execute. */
+int gfk_plan_result_device(gfk_plan *p, const double **d_out);
+/* Copies the result (and per-frequency status) of the last execute to the host. */
+int gfk_plan_download(gfk_plan *p, double *out, int32_t *status_per_f);
+/* Number of kernel launches one execute performs. */
+int32_t gfk_plan_launches_per_execute(const gfk_plan *p);
+/* Average duration in ms of the dominant kernel (the quadrature or the
+ * propagator, whichever took longer) over the executes since the last reset,
+ * timed with CUDA events on the plan's stream; name receives its label. */
+int gfk_plan_kernel_times(gfk_plan *p, double *prop_ms, double *quad_ms,
+                          double *other_ms, int32_t reset);
+int gfk_plan_destroy(gfk_plan *p);
+
+/* ---- bank file (internal/bank/format.go:32-46, 215-240) ------------------ */
+/* Packs an FP64 [nf][nr] result into the bank's float32 payload: range-major
+ * [count][bins] (re, im) pairs with bin = first_bin + f index; bins outside
+ * [first_bin, first_bin+nf) stay zero (cmd/geobank/main.go:116-121,161-165).
+ * Host memory in and out; payload has 2*count*bins floats. */
+int gfk_bank_pack(const double *spectra, int32_t nf, int32_t nr,
+                  int32_t first_bin, int32_t bins, float *payload);
+/* Writes magic "GEOBANK\0", uint32 version 1, uint32 header length, the JSON
+ * header, zero padding to a 4096-byte boundary, then the little-endian payload. */
+int gfk_bank_write(const char *path, const char *header_json,
+                   const float *payload, int64_t nfloats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GFK_H */
