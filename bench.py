@@ -1,0 +1,342 @@
+"""Benchmark: GF bank cells/s on the graded-soil workload.
+
+One step = one full Green's-function bank of the graded-soil workload
+(10 finite layers over a half-space, 2048 frequencies x 16384 wavenumbers x
+1024 ranges, complex Dunkin propagators in FP64, shared-grid quadrature),
+recomputed from the medium: layer constants, static coefficients, the
+propagator over every (f, k), the J0 table and the wavenumber sum.
+
+  value  cells/s with the medium already on the device (gfk_plan_execute),
+         timed with CUDA events on the plan's stream, L2 flushed between steps
+  e2e    cells/s through the host C ABI (gfk_bank_spectra): host medium and
+         grids in, the FP64 bank read back to pinned host memory, every step
+
+Multi-GPU (torchrun): every rank builds its own bank (weak scaling, no
+collective on the data path); the timing is the max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import ctypes
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "GF bank cells/s at relL2≤1e-6 vs FP64; surrogate speedup at ≤1% error"
+UNIT = "cells/s"
+
+
+def dist_init(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        if dist.get_backend() == "nccl":
+            dist.barrier(device_ids=[torch.cuda.current_device()])
+        else:
+            dist.barrier()
+
+
+def allmax(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def fp64_gemm_peak(torch):
+    """cuBLAS FP64 GEMM throughput (TFLOP/s), best of 5, as the FP64 denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_baseline(gfk, wl, threads, target_s=15.0):
+    """The oracle's restatement of the reference algorithm (reference-direct:
+    Qp = 2.25 Qs, real frequency, guard) on a bounded sample of the workload:
+    all ranges, the full wavenumber grid, frequencies from the band the
+    reference answers, on `threads` host threads."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    O.build()
+    st = [(l.thickness, l.vp, l.vs, l.density, l.qs, 0.0) for l in wl.stack]
+    m = O.OracleMedium(st)
+    answered = np.array([O.check_layer_phase(m, f) == 0 for f in wl.freqs])
+    band = wl.freqs[answered]
+    # one probe frequency per thread to size the sample
+    probe = band[np.linspace(0, len(band) - 1, threads).astype(int)]
+    t0 = time.perf_counter()
+    O.bank_spectra(m, wl.ranges, probe, samples=wl.samples, kmax=wl.kmax, threads=threads)
+    per_round = time.perf_counter() - t0
+    rounds = max(1, int(target_s / max(per_round, 1e-3)))
+    sample = band[np.linspace(0, len(band) - 1, min(len(band), rounds * threads)).astype(int)]
+    t0 = time.perf_counter()
+    _, status = O.bank_spectra(m, wl.ranges, sample, samples=wl.samples, kmax=wl.kmax, threads=threads)
+    dt = time.perf_counter() - t0
+    cells = len(sample) * len(wl.ranges)
+    return {"value": cells / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(sample)} of the {len(band)} bins the reference answers (<= guard), all "
+                      f"{len(wl.ranges)} ranges, {wl.samples} wavenumbers, reference-direct restatement "
+                      f"(oracle/gfk_oracle.c), {dt:.1f} s",
+            "status_ok": bool((status == 0).all())}
+
+
+def run_reference(args):
+    rank, world, local = dist_init(args)
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    import __graft_entry__
+    gfk = __graft_entry__.load_package()
+    wl = gfk.workloads.graded_soil()
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_baseline(gfk, wl, threads, target_s=2.0)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cb = cpu_baseline(gfk, wl, threads, target_s=8.0)
+        vals.append(cb["value"])
+    dt = time.perf_counter() - t0
+    value = statistics.mean(vals)
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / max(args.steps, 1),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "config": config_of(wl, "reference-direct restatement on host cores"),
+           "cpu_baseline": dict(cb, value=value),
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def config_of(wl, note):
+    return {"workload": f"{wl.name}: 10 finite 0.8 m layers (Vs 120->600 m/s, Vp=2Vs, rho 1600->2100, "
+                        f"Qs 10->60, Qp=2Qs) over a half-space; {len(wl.freqs)} bins 0-500 Hz (fs 1 kHz), "
+                        f"{wl.samples} wavenumbers to {wl.kmax:.1f} rad/m, {len(wl.ranges)} ranges "
+                        f"{wl.ranges[0]:g}-{wl.ranges[-1]:g} m, w_I = pi/T",
+            "soils": 1, "frequencies": len(wl.freqs), "wavenumbers": wl.samples, "ranges": len(wl.ranges),
+            "cells_per_step": wl.cells(), "l2": "intermediates (537 MB integrand, 134 MB J0 table) exceed L2; "
+                                                  "L2 also flushed (256 MiB write) between timed steps",
+            "note": note}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gfk", choices=["gfk", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank, world, local = dist_init(args)
+    torch.cuda.set_device(local)
+    import __graft_entry__
+    gfk = __graft_entry__.load_package()
+    wl = gfk.workloads.graded_soil()
+    eng = gfk.Engine(local)
+    med = wl.medium(gfk.DUNKIN, engine=eng)
+    plan = gfk.Plan(med, wl.ranges, wl.freqs, wl.integration(), engine=eng)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    for _ in range(max(args.warmup, 0)):
+        plan.execute()
+    got, status = plan.download()
+    assert (status == 0).all() and np.isfinite(got).all()
+    plan.kernel_times(reset=True)
+
+    # --- device-resident timing -----------------------------------------
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = eng.kernel_launches()
+    barrier(world)
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    step_ms = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        plan.execute()
+    torch.cuda.synchronize()
+    barrier(world)
+    wall = time.perf_counter() - t_wall
+    launches = eng.kernel_launches() - launches0
+    prop_ms, quad_ms, other_ms = plan.kernel_times(reset=True)
+    step_ms = prop_ms + quad_ms + other_ms
+    clk = clocks.stop()
+    step_ms = allmax(step_ms, world)
+    cells_all = wl.cells() * world
+    value = cells_all / (step_ms * 1e-3)
+
+    # --- end-to-end through the host C ABI ------------------------------
+    out_host = torch.empty((len(wl.freqs), 2 * len(wl.ranges)), dtype=torch.float64, pin_memory=True)
+    status_host = torch.zeros(len(wl.freqs), dtype=torch.int32, pin_memory=True)
+    N = gfk._native
+    r = np.ascontiguousarray(wl.ranges)
+    f = np.ascontiguousarray(wl.freqs)
+
+    def e2e_call():
+        from gfk_b200.fk import _c_medium
+        with _c_medium(med) as cm:
+            st = N.lib().gfk_bank_spectra(eng.ctx, ctypes.byref(cm), ctypes.byref(med._solve()),
+                                          r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r),
+                                          f.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(f),
+                                          wl.integration().c(),
+                                          ctypes.cast(out_host.data_ptr(), ctypes.POINTER(ctypes.c_double)),
+                                          ctypes.cast(status_host.data_ptr(), ctypes.POINTER(ctypes.c_int32)))
+        eng.check(st)
+
+    e2e_call()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_call()
+    e2e_s = allmax((time.perf_counter() - t0) / max(args.steps, 1), world)
+    e2e_value = cells_all / e2e_s
+    nl = len(wl.stack)
+    h2d = nl * 48 + len(r) * 8 + len(f) * (8 + 8 + 8 + 4 + 8)
+    d2h = len(f) * len(r) * 16 + len(f) * 4
+
+    # --- roofline of the dominant kernel --------------------------------
+    peaks = measured_peaks()
+    fp64_peak = fp64_gemm_peak(torch)
+    lfin = nl - 1
+    f_prop = len(f) * wl.samples * (700 * lfin + 300)   # algorithmic FP64 flops per propagator launch
+    f_quad = 4 * len(f) * wl.samples * len(r)           # complex x real MAC, per quadrature launch
+    if prop_ms >= quad_ms:
+        dom, ach = "k_prop (Dunkin propagator)", f_prop / (prop_ms * 1e-3) / 1e12
+    else:
+        dom, ach = "k_quad_gemm (FP64 wavenumber sum)", f_quad / (quad_ms * 1e-3) / 1e12
+    roof_time = (f_prop + f_quad) / (fp64_peak * 1e12)
+    roofline = {"bound": "fp64", "kernel": dom, "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": ach / fp64_peak, "traffic": None,
+                "peak_source": "measured here: cuBLAS FP64 GEMM 8192^3 best of 5 (MEASURED_PEAKS.json has no FP64 "
+                               "figure)",
+                "algorithmic_flops": {"propagator": f_prop, "quadrature": f_quad},
+                "step_frac_of_fp64_roofline": roof_time / (step_ms * 1e-3),
+                "kernel_ms": {"propagator": prop_ms, "quadrature": quad_ms, "other": other_ms},
+                "hbm_gbs_peak": peaks.get("hbm_gbs")}
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(gfk, wl, os.cpu_count() or 1)
+        cb.pop("status_ok", None)
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": dict(config_of(wl, "Dunkin formulation, FP64 propagators and FP64 quadrature"),
+                              parallelism=f"replicas{world}" if world > 1 else "single"),
+               "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                       "ms_per_step": e2e_s * 1e3},
+               "gpu_launches": launches, "clocks": clk, "roofline": roofline,
+               "wall_s_timed_region": wall}
+        if cb:
+            out["cpu_baseline"] = cb
+        print(json.dumps(out))
+    plan.close()
+    eng.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

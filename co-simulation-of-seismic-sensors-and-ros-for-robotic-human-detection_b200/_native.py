@@ -1,0 +1,109 @@
+"""ctypes binding of libgfk (include/gfk.h).
+
+There is no fallback: if libgfk.so is missing or cannot be loaded, importing
+the engine raises, and if no CUDA device is present, opening a context raises.
+"""
+import ctypes
+import pathlib
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "_lib" / "libgfk.so"
+
+# status codes (enum gfk_status)
+OK, EARG, ESTACK, EGUARD, ESINGULAR, ENONFINITE, ETIMEOUT, ECUDA, ENOMEM, EIO, ELIMIT = range(11)
+STATUS_NAMES = {OK: "OK", EARG: "EARG", ESTACK: "ESTACK", EGUARD: "EGUARD", ESINGULAR: "ESINGULAR",
+                ENONFINITE: "ENONFINITE", ETIMEOUT: "ETIMEOUT", ECUDA: "ECUDA", ENOMEM: "ENOMEM", EIO: "EIO",
+                ELIMIT: "ELIMIT"}
+
+REFERENCE_DIRECT = 0
+DUNKIN = 1
+PLAIN_FP64 = 0
+SPLIT_INT8 = 1
+
+# every symbol include/gfk.h declares
+EXPORTS = [
+    "gfk_open", "gfk_close", "gfk_status_string", "gfk_last_error", "gfk_kernel_launches",
+    "gfk_stack_validate", "gfk_check_layer_phase", "gfk_grid_for",
+    "gfk_surface_response", "gfk_static_coefficient", "gfk_vertical_displacement",
+    "gfk_vertical_displacement_multi", "gfk_bank_spectra",
+    "gfk_plan_create", "gfk_plan_execute", "gfk_plan_result_device", "gfk_plan_download",
+    "gfk_plan_launches_per_execute", "gfk_plan_kernel_times", "gfk_plan_destroy",
+    "gfk_bank_pack", "gfk_bank_write",
+]
+
+
+class GfkLayer(ctypes.Structure):
+    _fields_ = [("thickness_m", ctypes.c_double), ("vp_mps", ctypes.c_double), ("vs_mps", ctypes.c_double),
+                ("density_kgm3", ctypes.c_double), ("qs", ctypes.c_double), ("qp", ctypes.c_double)]
+
+
+class GfkMedium(ctypes.Structure):
+    _fields_ = [("layers", ctypes.POINTER(GfkLayer)), ("count", ctypes.c_int32), ("_pad", ctypes.c_int32),
+                ("ref_freq_hz", ctypes.c_double), ("default_q", ctypes.c_double),
+                ("sls_tau_sigma", ctypes.c_double), ("sls_tau_eps", ctypes.c_double)]
+
+
+class GfkIntegration(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_int32), ("_pad", ctypes.c_int32), ("kmax_factor", ctypes.c_double),
+                ("kmax", ctypes.c_double)]
+
+
+class GfkGrid(ctypes.Structure):
+    _fields_ = [("kmax", ctypes.c_double), ("samples", ctypes.c_int32), ("_pad", ctypes.c_int32)]
+
+
+class GfkSolve(ctypes.Structure):
+    _fields_ = [("formulation", ctypes.c_int32), ("quadrature", ctypes.c_int32), ("guard", ctypes.c_int32),
+                ("_pad", ctypes.c_int32), ("omega_imag", ctypes.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libgfk; raises if the library is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"libgfk is not built ({LIB_PATH} missing); run build.build() — "
+                           "there is no CPU fallback")
+    L = ctypes.CDLL(str(LIB_PATH))
+    P, d, i32, i64 = ctypes.POINTER, ctypes.c_double, ctypes.c_int32, ctypes.c_int64
+    vp = ctypes.c_void_p
+    sig = {
+        "gfk_open": (ctypes.c_int, [ctypes.c_int, P(vp)]),
+        "gfk_close": (ctypes.c_int, [vp]),
+        "gfk_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+        "gfk_last_error": (ctypes.c_char_p, [vp]),
+        "gfk_kernel_launches": (i64, [vp]),
+        "gfk_stack_validate": (ctypes.c_int, [P(GfkMedium)]),
+        "gfk_check_layer_phase": (ctypes.c_int, [P(GfkMedium), d]),
+        "gfk_grid_for": (ctypes.c_int, [P(GfkMedium), P(d), i32, d, GfkIntegration, P(GfkGrid)]),
+        "gfk_surface_response": (ctypes.c_int, [vp, P(GfkMedium), P(GfkSolve), P(d), P(d), i64, P(d)]),
+        "gfk_static_coefficient": (ctypes.c_int, [vp, P(GfkMedium), P(GfkSolve), d, d, P(d)]),
+        "gfk_vertical_displacement": (ctypes.c_int, [vp, P(GfkMedium), P(GfkSolve), d, d, GfkIntegration, P(d)]),
+        "gfk_vertical_displacement_multi": (ctypes.c_int, [vp, P(GfkMedium), P(GfkSolve), P(d), i32, d,
+                                                           GfkIntegration, P(d)]),
+        "gfk_bank_spectra": (ctypes.c_int, [vp, P(GfkMedium), P(GfkSolve), P(d), i32, P(d), i32, GfkIntegration,
+                                            P(d), P(i32)]),
+        "gfk_plan_create": (ctypes.c_int, [vp, P(GfkMedium), P(GfkSolve), P(d), i32, P(d), i32, GfkIntegration,
+                                           P(vp)]),
+        "gfk_plan_execute": (ctypes.c_int, [vp]),
+        "gfk_plan_result_device": (ctypes.c_int, [vp, P(vp)]),
+        "gfk_plan_download": (ctypes.c_int, [vp, P(d), P(i32)]),
+        "gfk_plan_launches_per_execute": (i32, [vp]),
+        "gfk_plan_kernel_times": (ctypes.c_int, [vp, P(d), P(d), P(d), i32]),
+        "gfk_plan_destroy": (ctypes.c_int, [vp]),
+        "gfk_bank_pack": (ctypes.c_int, [P(d), i32, i32, i32, i32, P(ctypes.c_float)]),
+        "gfk_bank_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, P(ctypes.c_float), i64]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def status_string(code):
+    return lib().gfk_status_string(code).decode()

@@ -1,0 +1,846 @@
+// gfk_host.cu — the C ABI of libgfk (include/gfk.h): contexts, plans, the
+// reference's host-side rules (validation, guard, GridFor) and the bank file.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gfk.h"
+#include "gfk_kernels.cuh"
+
+
+
+// ------------------------------------------------------------------ ctx --
+
+struct gfk_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    int64_t launches = 0;
+};
+
+namespace {
+
+int fail(gfk_ctx* ctx, int status, const char* fmt, ...) {
+    if (ctx) {
+        char buf[1024];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        ctx->last_error = buf;
+    }
+    return status;
+}
+
+#define GFK_CUDA(ctx, call)                                                                        \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail((ctx), e_ == cudaErrorMemoryAllocation ? GFK_ENOMEM : GFK_ECUDA, "%s: %s", \
+                        #call, cudaGetErrorString(e_));                                            \
+    } while (0)
+
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double kMaxLayerPhase = 16.0;  // internal/fk/fk.go:242
+
+double q_of(const gfk_medium* m, const gfk_layer& l) {  // fk.go:67-75
+    if (l.qs > 0) return l.qs;
+    if (m->default_q > 0) return m->default_q;
+    return 30.0;
+}
+
+bool has_sls(const gfk_medium* m) { return m->sls_tau_sigma > 0 && m->sls_tau_eps > 0; }
+
+double slowest_vs(const gfk_medium* m) {  // layer.go:93-100
+    double s = m->layers[0].vs_mps;
+    for (int i = 0; i < m->count; i++) s = std::min(s, m->layers[i].vs_mps);
+    return s;
+}
+
+double reference_modulus(const gfk_medium* m) {  // fk.go:216-222
+    const gfk_layer& l0 = m->layers[0];
+    double r = l0.density_kgm3 * l0.vs_mps * l0.vs_mps;
+    for (int i = 0; i < m->count; i++) {
+        const gfk_layer& l = m->layers[i];
+        r = std::max(r, l.density_kgm3 * l.vs_mps * l.vs_mps);
+    }
+    return r;
+}
+
+// visco.SLS.Q (visco.go:84-90) at real f.
+double sls_q(const gfk_medium* m, double f) {
+    const double w = kTwoPi * f;
+    // M = (1 + i w te)/(1 + i w ts); Q = Re M / Im M
+    const double a = 1.0, b = w * m->sls_tau_eps, c = 1.0, d = w * m->sls_tau_sigma;
+    const double den = c * c + d * d;
+    const double re = (a * c + b * d) / den, im = (b * c - a * d) / den;
+    if (im == 0) return INFINITY;
+    return re / im;
+}
+
+double pole_q(const gfk_medium* m, double f) {  // fk.go:83-88
+    if (has_sls(m)) return sls_q(m, f);
+    return q_of(m, m->layers[m->count - 1]);
+}
+
+int validate(gfk_ctx* ctx, const gfk_medium* m) {  // layer.go:53-73
+    if (!m || !m->layers || m->count <= 0)
+        return fail(ctx, GFK_ESTACK, "layer: a stack needs at least a half-space");
+    if (m->count > gfk::kMaxLayers)
+        return fail(ctx, GFK_ELIMIT, "layer: %d layers, this build handles at most %d", m->count, gfk::kMaxLayers);
+    for (int i = 0; i < m->count; i++) {
+        const gfk_layer& l = m->layers[i];
+        const bool fin = std::isfinite(l.vs_mps) && std::isfinite(l.vp_mps) && std::isfinite(l.density_kgm3) &&
+                         std::isfinite(l.qs) && std::isfinite(l.qp) &&
+                         (i == m->count - 1 || std::isfinite(l.thickness_m));
+        if (!fin) return fail(ctx, GFK_ESTACK, "layer %d: parameters must be finite", i);
+        if (l.vs_mps <= 0) return fail(ctx, GFK_ESTACK, "layer %d: Vs must be positive, got %g m/s", i, l.vs_mps);
+        if (l.vp_mps <= 0) return fail(ctx, GFK_ESTACK, "layer %d: Vp must be positive, got %g m/s", i, l.vp_mps);
+        if (l.density_kgm3 <= 0)
+            return fail(ctx, GFK_ESTACK, "layer %d: density must be positive, got %g kg/m^3", i, l.density_kgm3);
+        if (l.vp_mps <= M_SQRT2 * l.vs_mps)
+            return fail(ctx, GFK_ESTACK, "layer %d: Vp=%g must exceed sqrt(2)*Vs=%g for a non-negative Poisson ratio",
+                        i, l.vp_mps, M_SQRT2 * l.vs_mps);
+        if (i < m->count - 1 && l.thickness_m <= 0)
+            return fail(ctx, GFK_ESTACK, "layer %d: thickness must be positive, got %g m", i, l.thickness_m);
+    }
+    return GFK_OK;
+}
+
+int check_layer_phase(gfk_ctx* ctx, const gfk_medium* m, double f) {  // fk.go:251-266
+    if (!m || !m->layers || m->count <= 0) return fail(ctx, GFK_ESTACK, "layer: a stack needs at least a half-space");
+    const double slowest = slowest_vs(m);
+    const double k = kTwoPi * f / (0.87 * slowest);
+    for (int i = 0; i < m->count - 1; i++) {
+        const double h = m->layers[i].thickness_m;
+        const double kh = k * h;
+        if (kh > kMaxLayerPhase)
+            return fail(ctx, GFK_EGUARD,
+                        "fk: layer %d is %g m thick, which is k*h = %.1f at %g Hz and past the %.0f this propagator "
+                        "stays accurate to; it would return a plausible wrong number rather than fail. Band-limit to "
+                        "%.0f Hz for this stack, or reformulate the solve with compound matrices as internal/propmat does",
+                        i, h, kh, f, kMaxLayerPhase, kMaxLayerPhase * 0.87 * slowest / (kTwoPi * h));
+    }
+    return GFK_OK;
+}
+
+int grid_for(gfk_ctx* ctx, const gfk_medium* m, const double* ranges, int nr, double f, gfk_integration opt,
+             gfk_grid* out) {  // fk.go:464-495
+    if (nr <= 0 || !ranges) return fail(ctx, GFK_EARG, "fk: no ranges given");
+    if (!m || !m->layers || m->count <= 0) return fail(ctx, GFK_ESTACK, "layer: a stack needs at least a half-space");
+    double rmin = INFINITY, rmax = 0;
+    for (int i = 0; i < nr; i++) {
+        if (!(ranges[i] > 0)) return fail(ctx, GFK_EARG, "fk: range must be positive, got %g m", ranges[i]);
+        rmin = std::min(rmin, ranges[i]);
+        rmax = std::max(rmax, ranges[i]);
+    }
+    const double kbody = kTwoPi * f / slowest_vs(m);
+    const double kmf = opt.kmax_factor > 0 ? opt.kmax_factor : 30;
+    const double kmax = std::max(opt.kmax > 0 ? opt.kmax : kmf * kbody, 40 / rmin);
+    double dk = kTwoPi / (8 * rmax);
+    const double q = pole_q(m, f);
+    if (kbody > 0 && q > 0) dk = std::min(dk, kbody / (2 * q) / 4);
+    const double nn = std::ceil(kmax / dk);
+    int n = nn > 2.0e9 ? 2000000000 : (int)nn;
+    if (opt.samples > 0) n = opt.samples;
+    if (n < 64) n = 64;
+    out->kmax = kmax;
+    out->samples = n;
+    out->_pad = 0;
+    return GFK_OK;
+}
+
+gfk::MediumP medium_params(const gfk_medium* m) {
+    gfk::MediumP p;
+    p.ref_freq = m->ref_freq_hz;
+    p.default_q = m->default_q;
+    p.tau_sigma = m->sls_tau_sigma;
+    p.tau_eps = m->sls_tau_eps;
+    p.count = m->count;
+    p.sls = has_sls(m) ? 1 : 0;
+    return p;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- plans --
+
+// How a plan sets its wavenumber grid per frequency.
+enum GridMode { kGridMulti = 0, kGridSingle = 1 };
+
+struct TimedSeg {
+    int kind;  // 0 prop, 1 quad, 2 other
+    cudaEvent_t a, b;
+    bool pending;
+};
+
+struct gfk_plan {
+    gfk_ctx* ctx = nullptr;
+    std::vector<gfk_layer> layers;
+    gfk_medium med{};
+    gfk_solve solve{};
+    std::vector<double> ranges, freqs;
+    std::vector<int32_t> host_status;  // per f, set on the host (guard, args)
+    std::vector<int> nk;
+    std::vector<double> dk, kfar;
+    std::vector<int64_t> off;
+    bool shared = false;
+    double mu_ref = 0;
+    int nf = 0, nr = 0, nl = 0, max_nk = 0;
+    int64_t total_k = 0;
+    // chunks over frequency: [f_begin, f_end) with REM offset base
+    std::vector<int> chunk_begin;
+    // device
+    gfk::LayerP* d_layers = nullptr;
+    double *d_freqs = nullptr, *d_ranges = nullptr, *d_dk = nullptr, *d_kfar = nullptr, *d_W = nullptr;
+    int* d_nk = nullptr;
+    int64_t* d_off = nullptr;
+    gfk::LayerC* d_lc = nullptr;
+    cd *d_wc2 = nullptr, *d_C = nullptr, *d_rem = nullptr, *d_G = nullptr;
+    int* d_status = nullptr;
+    int64_t rem_capacity = 0;  // complex values
+    int32_t launches_per_exec = 0;
+    // timing
+    std::vector<TimedSeg> segs;
+    size_t seg_next = 0;
+    double acc_ms[3] = {0, 0, 0};
+    int acc_execs = 0;
+    bool executed = false;
+};
+
+namespace {
+
+const int64_t kDefaultRemBudget = int64_t(4) << 30;  // bytes of integrand per chunk
+
+void plan_free(gfk_plan* p) {
+    if (!p) return;
+    cudaStream_t s = p->ctx ? p->ctx->stream : nullptr;
+    void* ptrs[] = {p->d_layers, p->d_freqs, p->d_ranges, p->d_dk,  p->d_kfar, p->d_W, p->d_nk,
+                    p->d_off,    p->d_lc,    p->d_wc2,    p->d_C,   p->d_rem,  p->d_G, p->d_status};
+    for (void* q : ptrs)
+        if (q) cudaFreeAsync(q, s);
+    for (auto& sg : p->segs) {
+        cudaEventDestroy(sg.a);
+        cudaEventDestroy(sg.b);
+    }
+    if (s) cudaStreamSynchronize(s);
+}
+
+template <class T>
+int dalloc(gfk_ctx* ctx, T** ptr, size_t count) {
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMallocAsync((void**)ptr, bytes, ctx->stream);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return fail(ctx, GFK_ENOMEM, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    return GFK_OK;
+}
+
+template <class T>
+int h2d(gfk_ctx* ctx, T* dst, const T* src, size_t count) {
+    if (count == 0) return GFK_OK;
+    GFK_CUDA(ctx, cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    return GFK_OK;
+}
+
+int begin_seg(gfk_plan* p, int kind, size_t* slot) {
+    gfk_ctx* ctx = p->ctx;
+    if (p->segs.size() < 256) {
+        TimedSeg sg{kind, nullptr, nullptr, false};
+        GFK_CUDA(ctx, cudaEventCreate(&sg.a));
+        GFK_CUDA(ctx, cudaEventCreate(&sg.b));
+        p->segs.push_back(sg);
+        *slot = p->segs.size() - 1;
+    } else {
+        *slot = p->seg_next % p->segs.size();
+        TimedSeg& old = p->segs[*slot];
+        if (old.pending) {
+            GFK_CUDA(ctx, cudaEventSynchronize(old.b));
+            float ms = 0;
+            cudaEventElapsedTime(&ms, old.a, old.b);
+            p->acc_ms[old.kind] += ms;
+            old.pending = false;
+        }
+    }
+    p->seg_next++;
+    p->segs[*slot].kind = kind;
+    GFK_CUDA(ctx, cudaEventRecord(p->segs[*slot].a, ctx->stream));
+    return GFK_OK;
+}
+
+int end_seg(gfk_plan* p, size_t slot) {
+    GFK_CUDA(p->ctx, cudaEventRecord(p->segs[slot].b, p->ctx->stream));
+    p->segs[slot].pending = true;
+    return GFK_OK;
+}
+
+int flush_segs(gfk_plan* p) {
+    for (auto& sg : p->segs) {
+        if (!sg.pending) continue;
+        GFK_CUDA(p->ctx, cudaEventSynchronize(sg.b));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, sg.a, sg.b);
+        p->acc_ms[sg.kind] += ms;
+        sg.pending = false;
+    }
+    return GFK_OK;
+}
+
+int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const double* ranges, int32_t nr,
+               const double* freqs, int32_t nf, gfk_integration opt, GridMode mode, gfk_plan** out) {
+    *out = nullptr;
+    if (!ctx) return GFK_EARG;
+    if (!s) return fail(ctx, GFK_EARG, "solve options missing");
+    if (s->formulation != GFK_REFERENCE_DIRECT && s->formulation != GFK_DUNKIN)
+        return fail(ctx, GFK_EARG, "unknown formulation %d", s->formulation);
+    if (s->quadrature != GFK_PLAIN_FP64)
+        return fail(ctx, GFK_EARG, "quadrature %d is not available in this build", s->quadrature);
+    if (s->formulation == GFK_REFERENCE_DIRECT && s->omega_imag != 0)
+        return fail(ctx, GFK_EARG, "the reference formulation evaluates at real frequencies; omega_imag must be 0");
+    if (!(s->omega_imag >= 0) || !std::isfinite(s->omega_imag))
+        return fail(ctx, GFK_EARG, "omega_imag must be finite and non-negative, got %g", s->omega_imag);
+    if (nf < 0 || nr < 0 || (nf > 0 && !freqs)) return fail(ctx, GFK_EARG, "fk: bad frequency list");
+    if (nr <= 0 || !ranges) return fail(ctx, GFK_EARG, "fk: no ranges given");
+    for (int j = 0; j < nr; j++)
+        if (!(ranges[j] > 0)) return fail(ctx, GFK_EARG, "fk: range must be positive, got %g m", ranges[j]);
+    if (!m || !m->layers || m->count <= 0) return fail(ctx, GFK_ESTACK, "layer: a stack needs at least a half-space");
+    if (m->count > gfk::kMaxLayers)
+        return fail(ctx, GFK_ELIMIT, "layer: %d layers, this build handles at most %d", m->count, gfk::kMaxLayers);
+
+    gfk_plan* p = new gfk_plan();
+    p->ctx = ctx;
+    p->layers.assign(m->layers, m->layers + m->count);
+    p->med = *m;
+    p->med.layers = p->layers.data();
+    p->solve = *s;
+    p->ranges.assign(ranges, ranges + nr);
+    p->freqs.assign(freqs, freqs + nf);
+    p->nf = nf;
+    p->nr = nr;
+    p->nl = m->count;
+    const bool guard = s->guard || s->formulation == GFK_REFERENCE_DIRECT;
+    const int stack_status = validate(ctx, &p->med);
+    const std::string stack_msg = ctx->last_error;
+    p->mu_ref = stack_status ? 0.0 : reference_modulus(&p->med);
+    double rmin = INFINITY;
+    for (double r : p->ranges) rmin = std::min(rmin, r);
+    const double slowest = slowest_vs(&p->med);
+    p->host_status.assign(nf, GFK_OK);
+    p->nk.assign(nf, 0);
+    p->dk.assign(nf, 0.0);
+    p->kfar.assign(nf, 0.0);
+    p->off.assign(nf, 0);
+    std::string first_msg;
+    int64_t total = 0;
+    double g_kmax = -1;
+    int g_n = -1;
+    bool shared = true;
+    for (int f = 0; f < nf; f++) {
+        const double fr = p->freqs[f];
+        int st = GFK_OK;
+        if (guard) st = check_layer_phase(ctx, &p->med, fr);
+        gfk_grid g{0, 0, 0};
+        if (!st) {
+            if (mode == kGridMulti) {
+                st = grid_for(ctx, &p->med, p->ranges.data(), nr, fr, opt, &g);
+            } else {  // Medium.VerticalDisplacement's own rule (fk.go:407-421)
+                const double kbody = kTwoPi * fr / slowest;
+                const double kmf = opt.kmax_factor > 0 ? opt.kmax_factor : 30;
+                g.kmax = std::max(opt.kmax > 0 ? opt.kmax : kmf * kbody, 40 / p->ranges[0]);
+                g.samples = opt.samples > 0 ? opt.samples : 20000;
+            }
+        }
+        if (!st && !(fr > 0))
+            st = fail(ctx, GFK_EARG, "fk: wavenumber and frequency must be positive, got %g and %g",
+                      std::max(200 * kTwoPi * fr / slowest, 400 / rmin), fr);
+        if (!st && stack_status) {
+            st = stack_status;
+            ctx->last_error = stack_msg;
+        }
+        if (st) {
+            p->host_status[f] = st;
+            if (first_msg.empty()) first_msg = ctx->last_error;
+            shared = false;
+            continue;
+        }
+        const double kbody = kTwoPi * fr / slowest;
+        p->kfar[f] = std::max(200 * kbody, 400 / rmin);
+        p->nk[f] = g.samples;
+        p->dk[f] = g.kmax / g.samples;
+        p->off[f] = total;
+        total += g.samples;
+        p->max_nk = std::max(p->max_nk, g.samples);
+        if (g_n < 0) {
+            g_n = g.samples;
+            g_kmax = g.kmax;
+        } else if (g_n != g.samples || g_kmax != g.kmax) {
+            shared = false;
+        }
+    }
+    ctx->last_error = first_msg;
+    p->total_k = total;
+    p->shared = shared && g_n > 0;
+    // frequency chunks bounded by the integrand budget
+    const int64_t budget = kDefaultRemBudget / (int64_t)sizeof(cd);
+    int64_t acc = 0, cap = 0;
+    p->chunk_begin.push_back(0);
+    for (int f = 0; f < nf; f++) {
+        if (acc > 0 && acc + p->nk[f] > budget) {
+            p->chunk_begin.push_back(f);
+            cap = std::max(cap, acc);
+            acc = 0;
+        }
+        acc += p->nk[f];
+    }
+    cap = std::max(cap, acc);
+    p->chunk_begin.push_back(nf);
+    p->rem_capacity = cap;
+
+    // device buffers
+    int st = GFK_OK;
+    const size_t nfa = std::max(nf, 1);
+    if (!st) st = dalloc(ctx, &p->d_layers, p->nl);
+    if (!st) st = dalloc(ctx, &p->d_freqs, nfa);
+    if (!st) st = dalloc(ctx, &p->d_ranges, nr);
+    if (!st) st = dalloc(ctx, &p->d_dk, nfa);
+    if (!st) st = dalloc(ctx, &p->d_kfar, nfa);
+    if (!st) st = dalloc(ctx, &p->d_nk, nfa);
+    if (!st) st = dalloc(ctx, &p->d_off, nfa);
+    if (!st) st = dalloc(ctx, &p->d_lc, nfa * p->nl);
+    if (!st) st = dalloc(ctx, &p->d_wc2, nfa);
+    if (!st) st = dalloc(ctx, &p->d_C, nfa);
+    if (!st) st = dalloc(ctx, &p->d_G, nfa * nr);
+    if (!st) st = dalloc(ctx, &p->d_status, nfa);
+    if (!st) st = dalloc(ctx, &p->d_rem, (size_t)std::max<int64_t>(cap, 1));
+    if (!st && p->shared) st = dalloc(ctx, &p->d_W, (size_t)g_n * nr);
+    if (st) {
+        plan_free(p);
+        delete p;
+        return st;
+    }
+    std::vector<gfk::LayerP> lp(p->nl);
+    for (int i = 0; i < p->nl; i++) {
+        const gfk_layer& l = p->layers[i];
+        lp[i] = gfk::LayerP{l.thickness_m, l.vp_mps, l.vs_mps, l.density_kgm3, l.qs, l.qp};
+    }
+    // offsets are relative to their chunk's start
+    std::vector<int64_t> roff(nf);
+    for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++) {
+        const int fb = p->chunk_begin[c], fe = p->chunk_begin[c + 1];
+        const int64_t base = fb < nf ? p->off[fb] : 0;
+        for (int f = fb; f < fe; f++) roff[f] = p->off[f] - base;
+    }
+    if (!st) st = h2d(ctx, p->d_layers, lp.data(), lp.size());
+    if (!st) st = h2d(ctx, p->d_freqs, p->freqs.data(), nf);
+    if (!st) st = h2d(ctx, p->d_ranges, p->ranges.data(), nr);
+    if (!st) st = h2d(ctx, p->d_dk, p->dk.data(), nf);
+    if (!st) st = h2d(ctx, p->d_kfar, p->kfar.data(), nf);
+    if (!st) st = h2d(ctx, p->d_nk, p->nk.data(), nf);
+    if (!st) st = h2d(ctx, p->d_off, roff.data(), nf);
+    if (st) {
+        plan_free(p);
+        delete p;
+        return st;
+    }
+    const int nchunks = (int)p->chunk_begin.size() - 1;
+    p->launches_per_exec = 2 + 3 * nchunks + (p->shared ? 1 : 0);
+    *out = p;
+    return GFK_OK;
+}
+
+int plan_exec(gfk_plan* p) {
+    gfk_ctx* ctx = p->ctx;
+    cudaStream_t s = ctx->stream;
+    const int nf = p->nf;
+    if (nf == 0) {
+        p->executed = true;
+        return GFK_OK;
+    }
+    const int form = p->solve.formulation;
+    GFK_CUDA(ctx, cudaMemsetAsync(p->d_status, 0, sizeof(int) * nf, s));
+    size_t seg;
+    int st = begin_seg(p, 2, &seg);
+    if (st) return st;
+    gfk::launch_layer_consts(s, p->d_layers, medium_params(&p->med), p->d_freqs, nf, p->solve.omega_imag, p->mu_ref,
+                             form, p->d_lc, p->d_wc2);
+    gfk::launch_static(s, p->d_lc, p->nl, p->d_freqs, p->d_wc2, p->d_kfar, nf, p->mu_ref, form, p->d_C, p->d_status);
+    if (p->shared) gfk::launch_j0_table(s, p->d_ranges, p->nr, p->nk[0], p->dk[0], p->d_W);
+    if ((st = end_seg(p, seg))) return st;
+    ctx->launches += 2 + (p->shared ? 1 : 0);
+    for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++) {
+        const int fb = p->chunk_begin[c], fe = p->chunk_begin[c + 1];
+        const int cnf = fe - fb;
+        if (cnf <= 0) continue;
+        int cmax = 0;
+        for (int f = fb; f < fe; f++) cmax = std::max(cmax, p->nk[f]);
+        if ((st = begin_seg(p, 0, &seg))) return st;
+        gfk::launch_prop(s, p->d_lc + (size_t)fb * p->nl, p->nl, p->d_freqs + fb, p->d_wc2 + fb, cnf, p->d_nk + fb,
+                         p->d_dk + fb, p->d_off + fb, cmax, p->d_C + fb, p->mu_ref, form, p->d_rem, p->d_status + fb);
+        if ((st = end_seg(p, seg))) return st;
+        if ((st = begin_seg(p, 1, &seg))) return st;
+        if (p->shared)
+            gfk::launch_quad_gemm(s, p->d_rem, p->d_W, p->d_C + fb, p->d_ranges, cnf, p->nk[0], p->nr, p->dk[0],
+                                  p->d_G + (size_t)fb * p->nr);
+        else
+            gfk::launch_quad_ragged(s, p->d_rem, p->d_C + fb, p->d_ranges, cnf, p->nr, p->d_nk + fb, p->d_dk + fb,
+                                    p->d_off + fb, p->d_G + (size_t)fb * p->nr);
+        if ((st = end_seg(p, seg))) return st;
+        ctx->launches += 2;
+    }
+    GFK_CUDA(ctx, cudaGetLastError());
+    p->acc_execs++;
+    p->executed = true;
+    return GFK_OK;
+}
+
+int plan_download(gfk_plan* p, double* out, int32_t* status) {
+    gfk_ctx* ctx = p->ctx;
+    const int nf = p->nf, nr = p->nr;
+    if (nf == 0) return GFK_OK;
+    std::vector<int> dst(nf);
+    if (out)
+        GFK_CUDA(ctx, cudaMemcpyAsync(out, p->d_G, sizeof(cd) * (size_t)nf * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    GFK_CUDA(ctx, cudaMemcpyAsync(dst.data(), p->d_status, sizeof(int) * nf, cudaMemcpyDeviceToHost, ctx->stream));
+    GFK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    int first = GFK_OK;
+    std::string msg = ctx->last_error;
+    for (int f = 0; f < nf; f++) {
+        int st = p->host_status[f];
+        if (!st && (dst[f] & gfk::kStSingular)) {
+            st = GFK_ESINGULAR;
+            if (first == GFK_OK)
+                msg = "fk: layer propagator or surface system is singular at f=" + std::to_string(p->freqs[f]);
+        } else if (!st && (dst[f] & gfk::kStNonfinite)) {
+            st = GFK_ENONFINITE;
+            if (first == GFK_OK) msg = "fk: non-finite response at f=" + std::to_string(p->freqs[f]);
+        }
+        if (st && out) std::memset(out + (size_t)2 * nr * f, 0, sizeof(double) * 2 * nr);
+        if (status) status[f] = st;
+        if (st && first == GFK_OK) first = st;
+    }
+    if (first) ctx->last_error = msg;
+    return first;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ ABI --
+
+extern "C" {
+
+const char* gfk_status_string(int status) {
+    switch (status) {
+        case GFK_OK: return "ok";
+        case GFK_EARG: return "invalid argument";
+        case GFK_ESTACK: return "invalid layer stack";
+        case GFK_EGUARD: return "layer phase past MaxLayerPhase";
+        case GFK_ESINGULAR: return "singular propagator or surface system";
+        case GFK_ENONFINITE: return "non-finite result";
+        case GFK_ETIMEOUT: return "device wait timed out";
+        case GFK_ECUDA: return "CUDA error";
+        case GFK_ENOMEM: return "out of memory";
+        case GFK_EIO: return "bank file I/O error";
+        case GFK_ELIMIT: return "size beyond limit";
+        default: return "unknown status";
+    }
+}
+
+int gfk_open(int device, gfk_ctx** out) {
+    if (!out) return GFK_EARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return GFK_ECUDA;
+    if (device < 0 || device >= n) return GFK_EARG;
+    gfk_ctx* c = new gfk_ctx();
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return GFK_ECUDA;
+    }
+    // keep freed stream-ordered allocations cached for the next call
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    *out = c;
+    return GFK_OK;
+}
+
+int gfk_close(gfk_ctx* ctx) {
+    if (!ctx) return GFK_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+    return GFK_OK;
+}
+
+const char* gfk_last_error(const gfk_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int64_t gfk_kernel_launches(const gfk_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int gfk_stack_validate(const gfk_medium* m) { return validate(nullptr, m); }
+
+int gfk_check_layer_phase(const gfk_medium* m, double freq_hz) { return check_layer_phase(nullptr, m, freq_hz); }
+
+int gfk_grid_for(const gfk_medium* m, const double* ranges, int32_t nr, double freq_hz, gfk_integration opt,
+                 gfk_grid* out) {
+    if (!out) return GFK_EARG;
+    return grid_for(nullptr, m, ranges, nr, freq_hz, opt, out);
+}
+
+int gfk_plan_create(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const double* ranges, int32_t nr,
+                    const double* freqs, int32_t nf, gfk_integration opt, gfk_plan** out) {
+    if (!out) return GFK_EARG;
+    if (!ctx) return GFK_EARG;
+    cudaSetDevice(ctx->device);
+    return plan_build(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, out);
+}
+
+int gfk_plan_execute(gfk_plan* p) {
+    if (!p) return GFK_EARG;
+    cudaSetDevice(p->ctx->device);
+    return plan_exec(p);
+}
+
+int gfk_plan_result_device(gfk_plan* p, const double** d_out) {
+    if (!p || !d_out) return GFK_EARG;
+    *d_out = reinterpret_cast<const double*>(p->d_G);
+    return GFK_OK;
+}
+
+int gfk_plan_download(gfk_plan* p, double* out, int32_t* status_per_f) {
+    if (!p) return GFK_EARG;
+    if (!p->executed) return fail(p->ctx, GFK_EARG, "plan has not been executed");
+    return plan_download(p, out, status_per_f);
+}
+
+int32_t gfk_plan_launches_per_execute(const gfk_plan* p) { return p ? p->launches_per_exec : 0; }
+
+int gfk_plan_kernel_times(gfk_plan* p, double* prop_ms, double* quad_ms, double* other_ms, int32_t reset) {
+    if (!p) return GFK_EARG;
+    int st = flush_segs(p);
+    if (st) return st;
+    const double n = p->acc_execs > 0 ? p->acc_execs : 1;
+    if (prop_ms) *prop_ms = p->acc_ms[0] / n;
+    if (quad_ms) *quad_ms = p->acc_ms[1] / n;
+    if (other_ms) *other_ms = p->acc_ms[2] / n;
+    if (reset) {
+        p->acc_ms[0] = p->acc_ms[1] = p->acc_ms[2] = 0;
+        p->acc_execs = 0;
+    }
+    return GFK_OK;
+}
+
+int gfk_plan_destroy(gfk_plan* p) {
+    if (!p) return GFK_OK;
+    cudaSetDevice(p->ctx->device);
+    plan_free(p);
+    delete p;
+    return GFK_OK;
+}
+
+int gfk_bank_spectra(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const double* ranges, int32_t nr,
+                     const double* freqs, int32_t nf, gfk_integration opt, double* out, int32_t* status_per_f) {
+    if (!ctx) return GFK_EARG;
+    cudaSetDevice(ctx->device);
+    gfk_plan* p = nullptr;
+    int st = plan_build(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, &p);
+    if (st) return st;
+    st = plan_exec(p);
+    if (!st) st = plan_download(p, out, status_per_f);
+    std::string msg = ctx->last_error;
+    plan_free(p);
+    delete p;
+    ctx->last_error = msg;
+    return st;
+}
+
+int gfk_vertical_displacement_multi(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const double* ranges,
+                                    int32_t nr, double freq_hz, gfk_integration opt, double* out) {
+    int32_t status = 0;
+    return gfk_bank_spectra(ctx, m, s, ranges, nr, &freq_hz, 1, opt, out, &status);
+}
+
+int gfk_vertical_displacement(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, double range_m, double freq_hz,
+                              gfk_integration opt, double* out) {
+    if (!ctx) return GFK_EARG;
+    if (!(range_m > 0)) return fail(ctx, GFK_EARG, "fk: range must be positive, got %g m", range_m);
+    if (!(freq_hz > 0)) return fail(ctx, GFK_EARG, "fk: frequency must be positive, got %g Hz", freq_hz);
+    cudaSetDevice(ctx->device);
+    gfk_plan* p = nullptr;
+    int st = plan_build(ctx, m, s, &range_m, 1, &freq_hz, 1, opt, kGridSingle, &p);
+    if (st) return st;
+    // a single range always takes the per-frequency (sequential-sum) quadrature
+    p->shared = false;
+    st = plan_exec(p);
+    int32_t fst = 0;
+    if (!st) st = plan_download(p, out, &fst);
+    std::string msg = ctx->last_error;
+    plan_free(p);
+    delete p;
+    ctx->last_error = msg;
+    return st;
+}
+
+// (k, f) pairs: the pairs are grouped by frequency into one single-range
+// plan each would be wasteful; instead a plan over the unique frequencies
+// supplies the layer constants and a pair kernel evaluates each k.
+}  // extern "C"
+
+namespace gfk {
+__global__ void k_pairs(const LayerC* __restrict__ lc, int nl, const double* __restrict__ freqs,
+                        const cd* __restrict__ wc2, const int* __restrict__ fidx, const double* __restrict__ k,
+                        int64_t n, double mu_ref, int formulation, cd* __restrict__ out, int* __restrict__ status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int f = fidx[i];
+    cd u;
+    if (formulation == 0) {
+        bool ok;
+        u = direct_u(lc + (size_t)f * nl, nl, kTwoPi * freqs[f], k[i], mu_ref, ok);
+        if (!ok) {
+            atomicOr(status, kStSingular);
+            u = mk(0.0);
+        }
+    } else {
+        u = dunkin_u(lc + (size_t)f * nl, nl, wc2[f], k[i], mu_ref);
+    }
+    if (!(isfinite(u.re) && isfinite(u.im))) atomicOr(status, kStNonfinite);
+    out[i] = u;
+}
+}  // namespace gfk
+
+extern "C" int gfk_surface_response(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const double* k,
+                                    const double* freq_hz, int64_t n, double* out) {
+    if (!ctx) return GFK_EARG;
+    if (n < 0 || (n > 0 && (!k || !freq_hz || !out))) return fail(ctx, GFK_EARG, "fk: bad (k, f) arrays");
+    if (n == 0) return GFK_OK;
+    if (!s) return fail(ctx, GFK_EARG, "solve options missing");
+    if (s->formulation == GFK_REFERENCE_DIRECT && s->omega_imag != 0)
+        return fail(ctx, GFK_EARG, "the reference formulation evaluates at real frequencies; omega_imag must be 0");
+    for (int64_t i = 0; i < n; i++)
+        if (!(k[i] > 0) || !(freq_hz[i] > 0))
+            return fail(ctx, GFK_EARG, "fk: wavenumber and frequency must be positive, got %g and %g", k[i],
+                        freq_hz[i]);
+    int st = validate(ctx, m);
+    if (st) return st;
+    cudaSetDevice(ctx->device);
+    std::vector<double> uf(freq_hz, freq_hz + n);
+    std::sort(uf.begin(), uf.end());
+    uf.erase(std::unique(uf.begin(), uf.end()), uf.end());
+    std::vector<int> fidx(n);
+    for (int64_t i = 0; i < n; i++)
+        fidx[i] = (int)(std::lower_bound(uf.begin(), uf.end(), freq_hz[i]) - uf.begin());
+    const int nf = (int)uf.size(), nl = m->count;
+    const double mu_ref = reference_modulus(m);
+    std::vector<gfk::LayerP> lp(nl);
+    for (int i = 0; i < nl; i++) {
+        const gfk_layer& l = m->layers[i];
+        lp[i] = gfk::LayerP{l.thickness_m, l.vp_mps, l.vs_mps, l.density_kgm3, l.qs, l.qp};
+    }
+    gfk::LayerP* d_layers = nullptr;
+    double *d_f = nullptr, *d_k = nullptr;
+    int *d_fidx = nullptr, *d_status = nullptr;
+    gfk::LayerC* d_lc = nullptr;
+    cd *d_wc2 = nullptr, *d_out = nullptr;
+    st = dalloc(ctx, &d_layers, nl);
+    if (!st) st = dalloc(ctx, &d_f, nf);
+    if (!st) st = dalloc(ctx, &d_k, n);
+    if (!st) st = dalloc(ctx, &d_fidx, n);
+    if (!st) st = dalloc(ctx, &d_status, 1);
+    if (!st) st = dalloc(ctx, &d_lc, (size_t)nf * nl);
+    if (!st) st = dalloc(ctx, &d_wc2, nf);
+    if (!st) st = dalloc(ctx, &d_out, n);
+    if (!st) st = h2d(ctx, d_layers, lp.data(), nl);
+    if (!st) st = h2d(ctx, d_f, uf.data(), nf);
+    if (!st) st = h2d(ctx, d_k, k, n);
+    if (!st) st = h2d(ctx, d_fidx, fidx.data(), n);
+    int hstat = 0;
+    if (!st) {
+        cudaMemsetAsync(d_status, 0, sizeof(int), ctx->stream);
+        gfk::launch_layer_consts(ctx->stream, d_layers, medium_params(m), d_f, nf, s->omega_imag, mu_ref,
+                                 s->formulation, d_lc, d_wc2);
+        gfk::k_pairs<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
+            d_lc, nl, d_f, d_wc2, d_fidx, d_k, n, mu_ref, s->formulation, d_out, d_status);
+        ctx->launches += 2;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = fail(ctx, GFK_ECUDA, "k_pairs launch: %s", cudaGetErrorString(e));
+    }
+    if (!st) {
+        cudaMemcpyAsync(out, d_out, sizeof(cd) * n, cudaMemcpyDeviceToHost, ctx->stream);
+        cudaMemcpyAsync(&hstat, d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = fail(ctx, GFK_ECUDA, "surface response: %s", cudaGetErrorString(e));
+    }
+    void* ptrs[] = {d_layers, d_f, d_k, d_fidx, d_status, d_lc, d_wc2, d_out};
+    for (void* q : ptrs)
+        if (q) cudaFreeAsync(q, ctx->stream);
+    if (st) return st;
+    if (hstat & gfk::kStSingular)
+        return fail(ctx, GFK_ESINGULAR, "fk: layer propagator or surface system is singular");
+    if (hstat & gfk::kStNonfinite) return fail(ctx, GFK_ENONFINITE, "fk: non-finite surface response");
+    return GFK_OK;
+}
+
+extern "C" int gfk_static_coefficient(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, double freq_hz,
+                                      double k_far, double* out) {
+    double u[2];
+    int st = gfk_surface_response(ctx, m, s, &k_far, &freq_hz, 1, u);
+    if (st) return st;
+    out[0] = k_far * u[0];
+    out[1] = k_far * u[1];
+    return GFK_OK;
+}
+
+// ------------------------------------------------------------ bank file --
+
+extern "C" int gfk_bank_pack(const double* spectra, int32_t nf, int32_t nr, int32_t first_bin, int32_t bins,
+                             float* payload) {
+    if (nf < 0 || nr <= 0 || bins <= 0 || !payload || (nf > 0 && !spectra)) return GFK_EARG;
+    std::memset(payload, 0, sizeof(float) * 2 * (size_t)nr * bins);
+    for (int f = 0; f < nf; f++) {
+        const int bin = first_bin + f;
+        if (bin < 0 || bin >= bins) continue;
+        for (int j = 0; j < nr; j++) {
+            const size_t o = 2 * ((size_t)j * bins + bin);
+            payload[o] = (float)spectra[2 * ((size_t)f * nr + j)];
+            payload[o + 1] = (float)spectra[2 * ((size_t)f * nr + j) + 1];
+        }
+    }
+    return GFK_OK;
+}
+
+extern "C" int gfk_bank_write(const char* path, const char* header_json, const float* payload, int64_t nfloats) {
+    // internal/bank/format.go:215-240
+    if (!path || !header_json || nfloats < 0 || (nfloats > 0 && !payload)) return GFK_EARG;
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return GFK_EIO;
+    static const unsigned char magic[8] = {'G', 'E', 'O', 'B', 'A', 'N', 'K', 0};
+    const size_t hlen = std::strlen(header_json);
+    auto le32 = [](uint32_t v, unsigned char* b) {
+        b[0] = v & 0xff; b[1] = (v >> 8) & 0xff; b[2] = (v >> 16) & 0xff; b[3] = (v >> 24) & 0xff;
+    };
+    unsigned char hdr[16];
+    std::memcpy(hdr, magic, 8);
+    le32(1u, hdr + 8);
+    le32((uint32_t)hlen, hdr + 12);
+    bool ok = std::fwrite(hdr, 1, 16, fp) == 16 && std::fwrite(header_json, 1, hlen, fp) == hlen;
+    size_t pos = 16 + hlen;
+    static const unsigned char zeros[4096] = {0};
+    const size_t pad = (4096 - pos % 4096) % 4096;
+    if (ok && pad) ok = std::fwrite(zeros, 1, pad, fp) == pad;
+    // payload: little-endian float32 (this library targets little-endian hosts)
+    if (ok && nfloats > 0) ok = std::fwrite(payload, sizeof(float), (size_t)nfloats, fp) == (size_t)nfloats;
+    ok = (std::fclose(fp) == 0) && ok;
+    return ok ? GFK_OK : GFK_EIO;
+}

@@ -1,0 +1,312 @@
+// gfk_kernels.cu — FP64 kernels of the Green's-function bank path.
+//
+//   k_layer_consts  per (frequency, layer): complex velocities -> solver constants
+//                   (fk.go:96-128 hoisted out of the wavenumber loop)
+//   k_static        per frequency: C = k_far u(k_far) (fk.go:365-371, 521)
+//   k_prop          per (frequency, wavenumber): the layered solve and the
+//                   static-subtracted integrand k u - C (fk.go:534-544)
+//   k_j0_table      the shared-grid Hankel weights w_i J0(k_i r_j) dk (fk.go:540-546)
+//   k_quad_gemm     the shared-grid wavenumber sum as an FP64 complex x real GEMM
+//   k_quad_ragged   per-frequency grids: the same sum with J0 in the loop
+//   k_bank_pack     FP64 [f][r] -> float32 range-major bank payload
+//                   (internal/bank/format.go:185-193)
+#include "gfk_kernels.cuh"
+
+namespace gfk {
+
+// ------------------------------------------------------------ constants --
+
+__global__ void k_layer_consts(const LayerP* __restrict__ layers, MediumP med, const double* __restrict__ freqs,
+                               int nf, double wi, double mu_ref, int formulation, LayerC* __restrict__ lc,
+                               cd* __restrict__ wc2) {
+    const int nl = med.count;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nf * nl) return;
+    const int f = idx / nl, l = idx - f * nl;
+    const double fr = freqs[f];
+    const LayerP L = layers[l];
+    const double q = q_of(med, L);
+    LayerC out;
+    if (formulation == 0) {
+        // Medium.propsOf (fk.go:119-128): Qp = 2.25 Qs, real frequency
+        const cd a = complex_velocity(med, L.vp, 2.25 * q, fr, 0.0);
+        const cd b = complex_velocity(med, L.vs, q, fr, 0.0);
+        out.c[0] = a;
+        out.c[1] = b;
+        out.c[2] = (L.rho * b) * b;
+        out.c[3] = mk(L.rho);
+    } else {
+        const double qp = L.qp > 0 ? L.qp : 2.25 * q;
+        const cd a = complex_velocity(med, L.vp, qp, fr, wi);
+        const cd b = complex_velocity(med, L.vs, q, fr, wi);
+        const cd a2 = a * a, b2 = b * b;
+        out.c[0] = 1.0 / a2;
+        out.c[1] = 1.0 / b2;
+        out.c[2] = b2 / a2;
+        out.c[3] = (L.rho * b2) / mu_ref;
+    }
+    out.h = L.h;
+    out.pad = 0.0;
+    lc[idx] = out;
+    if (l == 0) {
+        const cd wc = mk(kTwoPi * fr, -wi);
+        wc2[f] = wc * wc;
+    }
+}
+
+void launch_layer_consts(cudaStream_t s, const LayerP* layers, MediumP med, const double* freqs, int nf,
+                         double wi, double mu_ref, int formulation, LayerC* lc, cd* wc2) {
+    const int n = nf * med.count;
+    k_layer_consts<<<(n + 127) / 128, 128, 0, s>>>(layers, med, freqs, nf, wi, mu_ref, formulation, lc, wc2);
+}
+
+__device__ __forceinline__ bool finite_cd(cd a) { return isfinite(a.re) && isfinite(a.im); }
+
+// ------------------------------------------------------ static coefficient --
+
+__global__ void k_static(const LayerC* __restrict__ lc, int nl, const double* __restrict__ freqs,
+                         const cd* __restrict__ wc2, const double* __restrict__ kfar, int nf, double mu_ref,
+                         int formulation, cd* __restrict__ C, int* __restrict__ status) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const double k = kfar[f];
+    if (!(k > 0)) {
+        C[f] = mk(0.0);
+        return;
+    }
+    cd u;
+    if (formulation == 0) {
+        bool ok;
+        u = direct_u(lc + (size_t)f * nl, nl, kTwoPi * freqs[f], k, mu_ref, ok);
+        if (!ok) atomicOr(status + f, kStSingular);
+    } else {
+        u = dunkin_u(lc + (size_t)f * nl, nl, wc2[f], k, mu_ref);
+    }
+    cd c = k * u;
+    if (!finite_cd(c)) {
+        atomicOr(status + f, kStNonfinite);
+        c = mk(0.0);
+    }
+    C[f] = c;
+}
+
+void launch_static(cudaStream_t s, const LayerC* lc, int nl, const double* freqs, const cd* wc2,
+                   const double* kfar, int nf, double mu_ref, int formulation, cd* C, int* status) {
+    k_static<<<(nf + 63) / 64, 64, 0, s>>>(lc, nl, freqs, wc2, kfar, nf, mu_ref, formulation, C, status);
+}
+
+// ------------------------------------------------------------ propagator --
+
+constexpr int kPropThreads = 128;
+
+template <int FORM>
+__global__ __launch_bounds__(kPropThreads) void k_prop(const LayerC* __restrict__ lc, int nl,
+                                                       const double* __restrict__ freqs, const cd* __restrict__ wc2,
+                                                       const int* __restrict__ nk, const double* __restrict__ dk,
+                                                       const int64_t* __restrict__ off, const cd* __restrict__ C,
+                                                       double mu_ref, cd* __restrict__ rem, int* __restrict__ status) {
+    __shared__ LayerC s_lc[kMaxLayers];
+    const int f = blockIdx.y;
+    for (int l = threadIdx.x; l < nl; l += blockDim.x) s_lc[l] = lc[(size_t)f * nl + l];
+    __syncthreads();
+    const int n = nk[f];
+    const int i = blockIdx.x * kPropThreads + threadIdx.x + 1;
+    if (i > n) return;
+    const double k = (double)i * dk[f];
+    cd u;
+    if (FORM == 0) {
+        bool ok;
+        u = direct_u(s_lc, nl, kTwoPi * freqs[f], k, mu_ref, ok);
+        if (!ok) atomicOr(status + f, kStSingular);
+    } else {
+        u = dunkin_u(s_lc, nl, wc2[f], k, mu_ref);
+    }
+    cd r = k * u - C[f];
+    if (!finite_cd(r)) {
+        atomicOr(status + f, kStNonfinite);
+        r = mk(0.0);
+    }
+    rem[off[f] + (i - 1)] = r;
+}
+
+void launch_prop(cudaStream_t s, const LayerC* lc, int nl, const double* freqs, const cd* wc2, int nf,
+                 const int* nk, const double* dk, const int64_t* off, int max_nk, const cd* C, double mu_ref,
+                 int formulation, cd* rem, int* status) {
+    if (nf <= 0 || max_nk <= 0) return;
+    dim3 grid((max_nk + kPropThreads - 1) / kPropThreads, nf);
+    if (formulation == 0)
+        k_prop<0><<<grid, kPropThreads, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status);
+    else
+        k_prop<1><<<grid, kPropThreads, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status);
+}
+
+// -------------------------------------------------------------- J0 table --
+
+__global__ void k_j0_table(const double* __restrict__ ranges, int nr, int nk, double dk, double* __restrict__ W) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)nk * nr) return;
+    const int i = (int)(idx / nr) + 1;
+    const int j = (int)(idx - (int64_t)(i - 1) * nr);
+    const double k = (double)i * dk;
+    const double w = i == nk ? 0.5 : 1.0;
+    W[idx] = (w * j0(k * ranges[j])) * dk;
+}
+
+void launch_j0_table(cudaStream_t s, const double* ranges, int nr, int nk, double dk, double* W) {
+    const int64_t n = (int64_t)nk * nr;
+    k_j0_table<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(ranges, nr, nk, dk, W);
+}
+
+// ----------------------------------------------------- FP64 quadrature --
+//
+// G[f][j] = C_f/r_j - (dk/2) C_f + sum_i rem[f][i] W[i][j]:
+// a complex (nf x nk) by real (nk x nr) product on the FP64 pipe.
+// Block tile 64 f x 64 r x 16 k, 256 threads, 4 x 4 complex accumulators each,
+// register-staged double buffering of the shared-memory tiles.
+
+constexpr int QBM = 64, QBN = 64, QBK = 16;
+
+__global__ __launch_bounds__(256) void k_quad_gemm(const cd* __restrict__ rem, const double* __restrict__ W,
+                                                   const cd* __restrict__ C, const double* __restrict__ ranges,
+                                                   int nf, int nk, int nr, double dk, cd* __restrict__ G) {
+    __shared__ __align__(16) cd sA[2][QBK][QBM];
+    __shared__ __align__(16) double sB[2][QBK][QBN];
+    const int tid = threadIdx.x;
+    const int tr = tid & 15, tf = tid >> 4;
+    const int f0 = blockIdx.y * QBM, r0 = blockIdx.x * QBN;
+    // global -> register staging: A 4 complex along k, B 4 doubles along r
+    const int af = tid >> 2, ak = (tid & 3) * 4;
+    const int bk = tid >> 4, br = (tid & 15) * 4;
+    cd ra[4];
+    double rb[4];
+    auto load = [&](int kt) {
+        const int kb = kt * QBK;
+        const int gf = f0 + af;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int gk = kb + ak + q;
+            ra[q] = (gf < nf && gk < nk) ? rem[(size_t)gf * nk + gk] : mk(0.0);
+        }
+        const int gk = kb + bk;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int gr = r0 + br + q;
+            rb[q] = (gk < nk && gr < nr) ? W[(size_t)gk * nr + gr] : 0.0;
+        }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) sA[buf][ak + q][af] = ra[q];
+#pragma unroll
+        for (int q = 0; q < 4; q++) sB[buf][bk][br + q] = rb[q];
+    };
+    cd acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = mk(0.0);
+    const int ktiles = (nk + QBK - 1) / QBK;
+    load(0);
+    store(0);
+    __syncthreads();
+    for (int kt = 0; kt < ktiles; kt++) {
+        const int buf = kt & 1;
+        if (kt + 1 < ktiles) load(kt + 1);
+#pragma unroll
+        for (int kk = 0; kk < QBK; kk++) {
+            cd av[4];
+            double bv[4];
+#pragma unroll
+            for (int a = 0; a < 4; a++) av[a] = sA[buf][kk][tf * 4 + a];
+#pragma unroll
+            for (int b = 0; b < 4; b++) bv[b] = sB[buf][kk][tr * 4 + b];
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int b = 0; b < 4; b++) {
+                    acc[a][b].re = fma(av[a].re, bv[b], acc[a][b].re);
+                    acc[a][b].im = fma(av[a].im, bv[b], acc[a][b].im);
+                }
+        }
+        if (kt + 1 < ktiles) {
+            store(buf ^ 1);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        const int f = f0 + tf * 4 + a;
+        if (f >= nf) continue;
+        const cd c = C[f];
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const int j = r0 + tr * 4 + b;
+            if (j >= nr) continue;
+            const cd head = c / ranges[j] - (0.5 * dk) * c;  // fk.go:529-532
+            G[(size_t)f * nr + j] = head + acc[a][b];
+        }
+    }
+}
+
+void launch_quad_gemm(cudaStream_t s, const cd* rem, const double* W, const cd* C, const double* ranges, int nf,
+                      int nk, int nr, double dk, cd* G) {
+    dim3 grid((nr + QBN - 1) / QBN, (nf + QBM - 1) / QBM);
+    k_quad_gemm<<<grid, 256, 0, s>>>(rem, W, C, ranges, nf, nk, nr, dk, G);
+}
+
+// ---------------------------------------------- per-frequency-grid sum --
+// The reference's own order: the boundary term, then i = 1..n in sequence
+// (fk.go:529-548), one range per thread.
+
+__global__ __launch_bounds__(128) void k_quad_ragged(const cd* __restrict__ rem, const cd* __restrict__ C,
+                                                     const double* __restrict__ ranges, int nf, int nr,
+                                                     const int* __restrict__ nk, const double* __restrict__ dk,
+                                                     const int64_t* __restrict__ off, cd* __restrict__ G) {
+    const int f = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nr) return;
+    const int n = nk[f];
+    const double d = dk[f];
+    const double r = ranges[j];
+    const cd c = C[f];
+    cd acc = c / r - (0.5 * d) * c;
+    const cd* row = rem + off[f];
+    for (int i = 1; i <= n; i++) {
+        const double k = (double)i * d;
+        const double w = i == n ? 0.5 : 1.0;
+        const double wt = (w * j0(k * r)) * d;
+        const cd v = row[i - 1];
+        acc.re = fma(wt, v.re, acc.re);
+        acc.im = fma(wt, v.im, acc.im);
+    }
+    G[(size_t)f * nr + j] = acc;
+}
+
+void launch_quad_ragged(cudaStream_t s, const cd* rem, const cd* C, const double* ranges, int nf, int nr,
+                        const int* nk, const double* dk, const int64_t* off, cd* G) {
+    dim3 grid((nr + 127) / 128, nf);
+    k_quad_ragged<<<grid, 128, 0, s>>>(rem, C, ranges, nf, nr, nk, dk, off, G);
+}
+
+// ------------------------------------------------------------ bank pack --
+
+__global__ void k_bank_pack(const cd* __restrict__ G, int nf, int nr, int first_bin, int bins,
+                            float* __restrict__ payload) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)nf * nr) return;
+    const int j = (int)(idx / nf);
+    const int f = (int)(idx - (int64_t)j * nf);
+    const int bin = first_bin + f;
+    if (bin < 0 || bin >= bins) return;
+    const cd v = G[(size_t)f * nr + j];
+    const size_t o = 2 * ((size_t)j * bins + bin);
+    payload[o] = (float)v.re;
+    payload[o + 1] = (float)v.im;
+}
+
+void launch_bank_pack(cudaStream_t s, const cd* G, int nf, int nr, int first_bin, int bins, float* payload) {
+    const int64_t n = (int64_t)nf * nr;
+    k_bank_pack<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(G, nf, nr, first_bin, bins, payload);
+}
+
+}  // namespace gfk

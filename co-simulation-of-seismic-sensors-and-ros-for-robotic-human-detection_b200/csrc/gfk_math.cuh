@@ -1,0 +1,82 @@
+// gfk_math.cuh — complex FP64 arithmetic for the f-k kernels.
+//
+// A plain struct rather than cuComplex/thrust so every operation is visible and
+// the compiler keeps everything in registers. The elementary functions call
+// CUDA's real sqrt/exp/expm1/sincos/hypot/atan/pow/log; the complex forms
+// are the textbook identities named at each function.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+#define GFK_HD __host__ __device__ __forceinline__
+
+struct cd {
+    double re, im;
+};
+
+GFK_HD cd mk(double r, double i = 0.0) { return cd{r, i}; }
+GFK_HD cd operator+(cd a, cd b) { return cd{a.re + b.re, a.im + b.im}; }
+GFK_HD cd operator-(cd a, cd b) { return cd{a.re - b.re, a.im - b.im}; }
+GFK_HD cd operator-(cd a) { return cd{-a.re, -a.im}; }
+GFK_HD cd operator*(cd a, cd b) { return cd{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+GFK_HD cd operator*(double s, cd a) { return cd{s * a.re, s * a.im}; }
+GFK_HD cd operator*(cd a, double s) { return cd{s * a.re, s * a.im}; }
+GFK_HD cd operator+(cd a, double s) { return cd{a.re + s, a.im}; }
+GFK_HD cd operator+(double s, cd a) { return cd{a.re + s, a.im}; }
+GFK_HD cd operator-(double s, cd a) { return cd{s - a.re, -a.im}; }
+GFK_HD cd operator-(cd a, double s) { return cd{a.re - s, a.im}; }
+GFK_HD cd& operator+=(cd& a, cd b) { a.re += b.re; a.im += b.im; return a; }
+GFK_HD cd& operator-=(cd& a, cd b) { a.re -= b.re; a.im -= b.im; return a; }
+GFK_HD cd cmul_i(cd a) { return cd{-a.im, a.re}; }  // i*a
+
+// Smith's algorithm (R. L. Smith, CACM 5(8):435, 1962), the robust complex
+// division Go's runtime also uses.
+GFK_HD cd operator/(cd n, cd m) {
+    if (fabs(m.re) >= fabs(m.im)) {
+        double ratio = m.im / m.re;
+        double denom = m.re + ratio * m.im;
+        return cd{(n.re + n.im * ratio) / denom, (n.im - n.re * ratio) / denom};
+    }
+    double ratio = m.re / m.im;
+    double denom = m.im + ratio * m.re;
+    return cd{(n.re * ratio + n.im) / denom, (n.im * ratio - n.re) / denom};
+}
+GFK_HD cd operator/(cd n, double s) { return cd{n.re / s, n.im / s}; }
+GFK_HD cd operator/(double s, cd m) { return cd{s, 0.0} / m; }
+
+GFK_HD double cabs_(cd a) { return hypot(a.re, a.im); }
+GFK_HD double cnorm1(cd a) { return fmax(fabs(a.re), fabs(a.im)); }
+
+// Principal square root: with t = sqrt((|x| + |z|)/2), sqrt(z) is (t, y/2t)
+// for x >= 0 and (|y|/2t, copysign(t, y)) otherwise. Re >= 0 always.
+GFK_HD cd csqrt_(cd z) {
+    if (z.re == 0.0 && z.im == 0.0) return cd{0.0, z.im};
+    double t = sqrt(0.5 * (fabs(z.re) + hypot(z.re, z.im)));
+    if (z.re >= 0.0) return cd{t, z.im / (2.0 * t)};
+    return cd{fabs(z.im) / (2.0 * t), copysign(t, z.im)};
+}
+
+// exp(x + iy) = e^x (cos y + i sin y).
+GFK_HD cd cexp_(cd z) {
+    double s, c;
+    sincos(z.im, &s, &c);
+    double e = exp(z.re);
+    return cd{e * c, e * s};
+}
+
+// exp(z) - 1 without cancellation for small |z|:
+//   Re = expm1(x) cos y - 2 sin^2(y/2),  Im = e^x sin y.
+GFK_HD cd cexpm1_(cd z) {
+    double sh, ch;
+    sincos(0.5 * z.im, &sh, &ch);
+    double s = 2.0 * sh * ch;
+    double c = 1.0 - 2.0 * sh * sh;
+    double em = expm1(z.re);
+    return cd{em * c - 2.0 * sh * sh, (em + 1.0) * s};
+}
+
+// log(z) = log|z| + i arg z.
+GFK_HD cd clog_(cd z) { return cd{log(hypot(z.re, z.im)), atan2(z.im, z.re)}; }
+
+// Scale by 2^e exactly.
+GFK_HD cd cldexp(cd a, int e) { return cd{ldexp(a.re, e), ldexp(a.im, e)}; }

@@ -92,6 +92,10 @@ typedef struct gfk_integration {
     int32_t samples;      /* <= 0: GridFor's own count (single-range calls: 20000) */
     int32_t _pad;
     double kmax_factor;   /* <= 0: 30 */
+    double kmax;          /* > 0: use this in place of kmax_factor*k_body at every
+                             frequency, i.e. k_max = max(kmax, 40/r_min). It is what
+                             Integration{KMaxFactor: kmax/k_body(f)} expresses per
+                             frequency, made exact so one grid serves all of them. */
 } gfk_integration;
 
 /* fk.Grid (internal/fk/fk.go:446-449). */

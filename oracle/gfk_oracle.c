@@ -298,8 +298,7 @@ static void layer_terms(const lconst *L, cx c2, lterms *t) {
     t->ra = csqrt_re_pos(1 - t->ea);
     t->rb = csqrt_re_pos(1 - t->eb);
     cx ra = t->ra, rb = t->rb, ea = t->ea, eb = t->eb, kap = t->kap;
-    double abs_eb = cabs(eb);
-    if (abs_eb < 0.5) {
+    if (fmax(fabs(creal(eb)), fabs(cimag(eb))) < 0.35) {
         /* the small-c forms: every O(eb) numerator written without cancellation */
         t->u1 = (kap + 1 - ea) / (1 + ra * rb);
         cx s = ra + rb;
@@ -359,11 +358,16 @@ static void dunkin_layer_up(const lterms *t, double zeta, cx m[6]) {
     /* exp(-T zeta) compound, normalised by exp(-(ra+rb) zeta) */
     cx Ea = cexp(-ra * zeta), Eb = cexp(-rb * zeta);
     cx delta = (t->eb - t->ea) / (ra + rb); /* ra - rb without cancellation */
-    cx W;
-    if (cabs(delta * zeta) < 1)
-        W = 2 * rb * cexp(-(ra + rb) * zeta / 2) * csinh(delta * zeta / 2) / t->eb;
-    else
+    cx W, dz = delta * zeta;
+    if (fmax(fabs(creal(dz)), fabs(cimag(dz))) < 0.5) {
+        /* Eb - Ea = Eb (1 - exp(-dz)) = -Eb expm1(-dz), expm1 of a complex
+           argument as expm1(x) cos y - 2 sin^2(y/2) + i e^x sin y */
+        double x = -creal(dz), y = -cimag(dz);
+        cx em1 = (expm1(x) * cos(y) - 2 * sin(y / 2) * sin(y / 2)) + I * (exp(x) * sin(y));
+        W = rb * (-Eb * em1) / t->eb;
+    } else {
         W = rb * (Eb - Ea) / t->eb;
+    }
     cx z[6];
     z[0] = y[0];
     z[1] = Ea * Eb * y[1] - Eb * W * y[2] - W * Ea * y[3] + W * W * y[4];
@@ -481,7 +485,7 @@ int or_grid_for(const gfk_medium *m, const double *ranges, int nr, double f, gfk
     }
     double kbody = TWO_PI * f / slowest_vs(m);
     double kmf = opt.kmax_factor > 0 ? opt.kmax_factor : 30;
-    double kmax = fmax(kmf * kbody, 40 / rmin);
+    double kmax = fmax(opt.kmax > 0 ? opt.kmax : kmf * kbody, 40 / rmin);
     double dk = TWO_PI / (8 * rmax);
     double q = pole_q(m, f);
     if (kbody > 0 && q > 0) dk = fmin(dk, kbody / (2 * q) / 4);
@@ -548,7 +552,7 @@ int or_vertical_displacement(const gfk_medium *m, const gfk_solve *s, double r, 
     }
     double kbody = TWO_PI * f / slowest_vs(m);
     double kmf = opt.kmax_factor > 0 ? opt.kmax_factor : 30;
-    double kmax = fmax(kmf * kbody, 40 / r);
+    double kmax = fmax(opt.kmax > 0 ? opt.kmax : kmf * kbody, 40 / r);
     fctx c;
     int st = fctx_init(&c, m, s, f);
     if (st) return st;

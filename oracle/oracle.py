@@ -46,7 +46,7 @@ class Medium(ctypes.Structure):
 
 class Integration(ctypes.Structure):
     _fields_ = [("samples", ctypes.c_int32), ("_pad", ctypes.c_int32),
-                ("kmax_factor", ctypes.c_double)]
+                ("kmax_factor", ctypes.c_double), ("kmax", ctypes.c_double)]
 
 
 class Grid(ctypes.Structure):
@@ -109,8 +109,8 @@ def _medium(m):
     return m if isinstance(m, OracleMedium) else OracleMedium(m)
 
 
-def _integ(samples=0, kmax_factor=0.0):
-    return Integration(int(samples), 0, float(kmax_factor))
+def _integ(samples=0, kmax_factor=0.0, kmax=0.0):
+    return Integration(int(samples), 0, float(kmax_factor), float(kmax))
 
 
 def surface_response(medium, k, f, formulation=REFERENCE_DIRECT, omega_imag=0.0):
@@ -133,43 +133,43 @@ def static_coefficient(medium, f, k_far, formulation=REFERENCE_DIRECT, omega_ima
     return complex(out[0], out[1])
 
 
-def grid_for(medium, ranges, f, samples=0, kmax_factor=0.0):
+def grid_for(medium, ranges, f, samples=0, kmax_factor=0.0, kmax=0.0):
     m = _medium(medium)
     r = np.ascontiguousarray(ranges, dtype=np.float64)
     g = Grid()
     st = lib().or_grid_for(ctypes.byref(m.c), r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r),
-                           f, _integ(samples, kmax_factor), ctypes.byref(g))
+                           f, _integ(samples, kmax_factor, kmax), ctypes.byref(g))
     if st:
         raise OracleError(st)
     return g.kmax, g.samples
 
 
-def vertical_displacement_multi(medium, ranges, f, samples=0, kmax_factor=0.0,
+def vertical_displacement_multi(medium, ranges, f, samples=0, kmax_factor=0.0, kmax=0.0,
                                 formulation=REFERENCE_DIRECT, omega_imag=0.0, guard=0):
     m = _medium(medium)
     r = np.ascontiguousarray(ranges, dtype=np.float64)
     out = np.zeros(2 * len(r))
     st = lib().or_vertical_displacement_multi(
         ctypes.byref(m.c), ctypes.byref(_solve(formulation, omega_imag, guard)),
-        r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r), f, _integ(samples, kmax_factor),
+        r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r), f, _integ(samples, kmax_factor, kmax),
         out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
     if st:
         raise OracleError(st)
     return out[0::2] + 1j * out[1::2]
 
 
-def vertical_displacement(medium, r, f, samples=0, kmax_factor=0.0,
+def vertical_displacement(medium, r, f, samples=0, kmax_factor=0.0, kmax=0.0,
                           formulation=REFERENCE_DIRECT, omega_imag=0.0, guard=0):
     m = _medium(medium)
     out = (ctypes.c_double * 2)()
     st = lib().or_vertical_displacement(ctypes.byref(m.c), ctypes.byref(_solve(formulation, omega_imag, guard)),
-                                        r, f, _integ(samples, kmax_factor), out)
+                                        r, f, _integ(samples, kmax_factor, kmax), out)
     if st:
         raise OracleError(st)
     return complex(out[0], out[1])
 
 
-def bank_spectra(medium, ranges, freqs, samples=0, kmax_factor=0.0, formulation=REFERENCE_DIRECT,
+def bank_spectra(medium, ranges, freqs, samples=0, kmax_factor=0.0, kmax=0.0, formulation=REFERENCE_DIRECT,
                  omega_imag=0.0, guard=0, threads=None):
     """[nf, nr] complex128 and per-frequency status, threaded over frequency."""
     m = _medium(medium)
@@ -181,7 +181,7 @@ def bank_spectra(medium, ranges, freqs, samples=0, kmax_factor=0.0, formulation=
     P = ctypes.POINTER
     lib().or_bank_spectra(ctypes.byref(m.c), ctypes.byref(_solve(formulation, omega_imag, guard)),
                           r.ctypes.data_as(P(ctypes.c_double)), len(r),
-                          f.ctypes.data_as(P(ctypes.c_double)), len(f), _integ(samples, kmax_factor),
+                          f.ctypes.data_as(P(ctypes.c_double)), len(f), _integ(samples, kmax_factor, kmax),
                           out.ctypes.data_as(P(ctypes.c_double)), status.ctypes.data_as(P(ctypes.c_int32)),
                           threads)
     return out[:, 0::2] + 1j * out[:, 1::2], status

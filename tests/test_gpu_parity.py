@@ -1,0 +1,243 @@
+"""GPU parity: libgfk through its C ABI against the CPU oracle and the
+high-precision golden values. Tolerances: rel-L2 <= 1e-9 for the FP64 Dunkin
+path (same algorithm, different rounding), <= 1e-6 for the reference-direct
+path (the direct eigenbasis loses digits at large k/k_body in both
+implementations, differently)."""
+import json
+import math
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, as_tuples, rel_l2
+
+import closed_forms as CF
+
+pytestmark = pytest.mark.gpu
+MP = json.loads((GOLDEN / "surface_response_mp.json").read_text())
+
+
+def medium_of(gfk, tuples, **kw):
+    return gfk.Medium(gfk.Stack(gfk.Layer(*t) for t in tuples), **kw)
+
+
+@pytest.mark.parametrize("form", [0, 1], ids=["reference_direct", "dunkin"])
+def test_surface_response_against_high_precision(gfk, engine, form):
+    worst = 0.0
+    groups = {}
+    for c in MP["cases"]:
+        st = MP["media"][c["medium"]]
+        if form == 0 and (c["qp_mode"] != "reference" or c["kh"] > 16):
+            continue
+        if form == 1 and c["qp_mode"] == "reference":
+            st = [tuple(l[:5]) + (0.0,) for l in st]
+        groups.setdefault((c["medium"], c["qp_mode"], c["omega_imag"]), (st, []))[1].append(c)
+    n = 0
+    for (name, qpm, wi), (st, cases) in groups.items():
+        m = medium_of(gfk, st, formulation=form, omega_imag=wi, engine=engine)
+        k = np.array([c["k"] for c in cases])
+        f = np.array([c["f"] for c in cases])
+        got = m.surface_response(k, f)
+        want = np.array([complex(*c["u"]) for c in cases])
+        worst = max(worst, float(np.max(np.abs(got - want) / np.abs(want))))
+        n += len(cases)
+    assert n > 40
+    assert worst < (1e-6 if form == 0 else 1e-12), worst
+
+
+def test_surface_response_matches_oracle_pointwise(gfk, engine, oracle):
+    wl = gfk.workloads.graded_soil()
+    st = as_tuples(wl.stack)
+    rng = np.random.default_rng(7)
+    k = rng.uniform(0.005, 80.0, 400)
+    f = rng.uniform(0.2, 500.0, 400)
+    m = medium_of(gfk, st, formulation=1, omega_imag=wl.omega_imag, engine=engine)
+    got = m.surface_response(k, f)
+    want = np.array([oracle.surface_response(st, ki, fi, 1, wl.omega_imag) for ki, fi in zip(k, f)])
+    assert np.max(np.abs(got - want) / np.abs(want)) < 1e-11
+
+
+def test_reference_mode_per_frequency_grid(gfk, engine, oracle):
+    """VerticalDisplacementMulti with the reference's own GridFor grids (the
+    ragged path), soft_over_stiff and loam, against the oracle."""
+    for st in ([(3.0, 400.0, 160.0, 1600.0, 0.0, 0.0), (0.0, 900.0, 400.0, 2000.0, 0.0, 0.0)],
+               CF.uniform(CF.LOAM)):
+        m = medium_of(gfk, st, engine=engine)
+        ranges = np.array([2.0, 5.0, 10.0, 20.0])
+        freqs = np.array([5.0, 20.0, 60.0, 120.0])
+        got, status = m.bank_spectra(ranges, freqs)
+        assert (status == 0).all()
+        want, ost = oracle.bank_spectra(st, ranges, freqs)
+        assert (ost == 0).all()
+        assert rel_l2(got, want) < 1e-6
+        single = m.vertical_displacement_multi(ranges, 20.0)
+        assert np.allclose(single, got[1], rtol=1e-12, atol=0)
+
+
+def test_single_range_vertical_displacement(gfk, engine, oracle):
+    h = CF.LOAM
+    m = gfk.Medium(gfk.uniform(*h), engine=engine)
+    lam = CF.rayleigh_velocity(h) / 30.0
+    for mult in (1.5, 3.0):
+        got = m.vertical_displacement(mult * lam, 30.0)
+        want = oracle.vertical_displacement(CF.uniform(h), mult * lam, 30.0)
+        assert abs(got - want) / abs(want) < 1e-8
+
+
+def test_single_soil_full_bank_against_oracle(gfk, engine, oracle):
+    """The whole 512 x 64 bank of the single-soil workload, Dunkin, shared grid."""
+    wl = gfk.workloads.single_soil()
+    m = wl.medium(gfk.DUNKIN, engine=engine)
+    got, status = m.bank_spectra(wl.ranges, wl.freqs, wl.integration())
+    assert (status == 0).all()
+    want, ost = oracle.bank_spectra(as_tuples(wl.stack), wl.ranges, wl.freqs, samples=wl.samples, kmax=wl.kmax,
+                                    formulation=oracle.DUNKIN, omega_imag=wl.omega_imag)
+    assert (ost == 0).all()
+    assert rel_l2(got, want) < 1e-9
+
+
+def test_single_soil_reference_parity_band(gfk, engine, oracle):
+    """The reference's semantics (real frequency, Qp = 2.25 Qs, guard) on the
+    single-soil grid: bins the reference answers match the oracle's
+    restatement, the rest are refused with EGUARD as fk.go:251-266 refuses."""
+    wl = gfk.workloads.single_soil()
+    st = [(l.thickness, l.vp, l.vs, l.density, l.qs, 0.0) for l in wl.stack]
+    m = medium_of(gfk, st, engine=engine)
+    got, status = m.bank_spectra(wl.ranges, wl.freqs, wl.integration(), raise_on_error=False)
+    answered = status == 0
+    band = wl.freqs[answered]
+    assert band.max() < 170 and band.max() > 160   # 16*0.87*150/(2 pi 2) = 166 Hz
+    assert (status[~answered] == gfk._native.EGUARD).all()
+    sample = np.nonzero(answered)[0][::6]
+    want, ost = oracle.bank_spectra(st, wl.ranges, wl.freqs[sample], samples=wl.samples, kmax=wl.kmax)
+    assert (ost == 0).all()
+    assert rel_l2(got[sample], want) < 1e-6
+    # and the Dunkin solve agrees with the reference-direct one in that band
+    md = medium_of(gfk, st, formulation=gfk.DUNKIN, engine=engine)
+    gd, sd = md.bank_spectra(wl.ranges, band, wl.integration())
+    assert (sd == 0).all()
+    assert rel_l2(gd, got[answered]) < 1e-6
+
+
+def test_graded_soil_full_size_sampled_rows(gfk, engine, oracle):
+    """The 2048 x 1024 graded-soil bank on the GPU; rows at 8 frequencies
+    across the band recomputed by the oracle at the same full grid."""
+    wl = gfk.workloads.graded_soil()
+    m = wl.medium(gfk.DUNKIN, engine=engine)
+    got, status = m.bank_spectra(wl.ranges, wl.freqs, wl.integration())
+    assert (status == 0).all() and np.isfinite(got).all()
+    rows = np.linspace(0, len(wl.freqs) - 1, 8).astype(int)
+    want, ost = oracle.bank_spectra(as_tuples(wl.stack), wl.ranges, wl.freqs[rows], samples=wl.samples,
+                                    kmax=wl.kmax, formulation=oracle.DUNKIN, omega_imag=wl.omega_imag)
+    assert (ost == 0).all()
+    assert rel_l2(got[rows], want) < 1e-9
+
+
+def test_split_layer_invariance_above_the_guard(gfk, engine):
+    """stability_test.go:30-92 carried past 400 Hz: a half-space cut into
+    identical 2 m layers is the half-space, to 1e-9, on the GPU."""
+    h = CF.LOAM
+    half = gfk.Medium(gfk.uniform(*h), formulation=gfk.DUNKIN, default_q=30, engine=engine)
+    l = gfk.Layer(2.0, h[0], h[1], h[2], h[3])
+    split = gfk.Medium(gfk.Stack([l, l, gfk.Layer(0, h[0], h[1], h[2], h[3])]), formulation=gfk.DUNKIN,
+                       default_q=30, engine=engine)
+    freqs = np.array([10.0, 100.0, 400.0, 800.0, 1400.0])
+    ranges = np.array([10.0])
+    a, _ = half.bank_spectra(ranges, freqs)
+    b, _ = split.bank_spectra(ranges, freqs)
+    assert np.max(np.abs(a - b) / np.abs(a)) < 1e-9
+    ref = gfk.Medium(split.stack, engine=engine)
+    _, st = ref.bank_spectra(ranges, freqs, raise_on_error=False)
+    assert list(st) == [0, 0, gfk._native.EGUARD, gfk._native.EGUARD, gfk._native.EGUARD]
+
+
+def test_static_limit_and_boussinesq(gfk, engine):
+    h = CF.LOAM
+    m = gfk.Medium(gfk.Stack([gfk.Layer(0, h[0], h[1], h[2], 1e9)]), default_q=1e9, formulation=gfk.DUNKIN,
+                   engine=engine)
+    want = CF.boussinesq_coefficient(h)
+    u = m.surface_response(np.array([1.0, 10.0, 200.0, 4000.0]), 0.05)
+    assert np.max(np.abs(np.abs(u * np.array([1.0, 10.0, 200.0, 4000.0])) - want) / want) < 1e-5
+    mu, nu = CF.shear_modulus(h), CF.poisson_ratio(h)
+    for r in (2.0, 10.0):
+        got = m.vertical_displacement(r, 0.02, gfk.Integration(8000))
+        assert abs(abs(got) - (1 - nu) / (2 * math.pi * mu * r)) / ((1 - nu) / (2 * math.pi * mu * r)) < 0.02
+
+
+def test_linearity_in_force_scale(gfk, engine):
+    """Doubling every density doubles mu_ref and halves the response."""
+    wl = gfk.workloads.single_soil()
+    m = wl.medium(gfk.DUNKIN, engine=engine)
+    heavy = gfk.Stack(gfk.Layer(l.thickness, l.vp, l.vs, 2 * l.density, l.qs, l.qp) for l in wl.stack)
+    m2 = gfk.Medium(heavy, formulation=gfk.DUNKIN, omega_imag=wl.omega_imag, engine=engine)
+    a, _ = m.bank_spectra(wl.ranges[::16], wl.freqs[::32], wl.integration())
+    b, _ = m2.bank_spectra(wl.ranges[::16], wl.freqs[::32], wl.integration())
+    assert rel_l2(2 * b, a) < 1e-12
+
+
+def test_error_statuses(gfk, engine):
+    E = gfk._native
+    m = gfk.Medium(gfk.uniform(*CF.LOAM), engine=engine)
+    with pytest.raises(gfk.FkError) as e:
+        m.surface_response(0.0, 10.0)
+    assert e.value.status == E.EARG
+    with pytest.raises(gfk.FkError) as e:
+        m.vertical_displacement(-1.0, 10.0)
+    assert e.value.status == E.EARG
+    bad = gfk.Medium(gfk.Stack([gfk.Layer(0, 100, 200, 1700)]), engine=engine)
+    with pytest.raises(gfk.FkError) as e:
+        bad.surface_response(1.0, 10.0)
+    assert e.value.status == E.ESTACK
+    _, st = bad.bank_spectra([1.0, 2.0], [10.0, 20.0], raise_on_error=False)
+    assert (st == E.ESTACK).all()
+    nanm = gfk.Medium(gfk.Stack([gfk.Layer(1, 500, float("nan"), 1700), gfk.Layer(0, 500, 200, 1700)]),
+                      formulation=gfk.DUNKIN, engine=engine)
+    with pytest.raises(gfk.FkError) as e:
+        nanm.bank_spectra([1.0], [10.0])
+    assert e.value.status == E.ESTACK
+    with pytest.raises(gfk.FkError) as e:
+        gfk.Medium(gfk.uniform(*CF.LOAM), omega_imag=1.0, engine=engine).bank_spectra([1.0], [10.0])
+    assert e.value.status == E.EARG  # the reference formulation is real-frequency only
+    with pytest.raises(gfk.FkError) as e:
+        m.bank_spectra([], [10.0])
+    assert e.value.status == E.EARG
+    got, st = m.bank_spectra([1.0], [-5.0, 10.0], raise_on_error=False)
+    assert st[0] == E.EARG and st[1] == 0 and got[0, 0] == 0
+    # a failed call leaves the context usable
+    assert np.isfinite(m.vertical_displacement_multi([1.0, 2.0], 10.0)).all()
+
+
+def test_plan_is_deterministic_and_timed(gfk, engine):
+    wl = gfk.workloads.single_soil()
+    m = wl.medium(gfk.DUNKIN, engine=engine)
+    p = gfk.Plan(m, wl.ranges, wl.freqs, wl.integration(), engine=engine)
+    p.execute()
+    a, _ = p.download()
+    before = engine.kernel_launches()
+    p.execute()
+    b, _ = p.download()
+    assert engine.kernel_launches() - before == p.launches_per_execute()
+    assert np.array_equal(a, b)
+    prop, quad, other = p.kernel_times()
+    assert prop > 0 and quad > 0
+    ref, _ = m.bank_spectra(wl.ranges, wl.freqs, wl.integration())
+    assert np.array_equal(a, ref)
+    p.close()
+
+
+def test_build_and_write_bank(gfk, engine, tmp_path):
+    """geobank build on the GPU (cmd/geobank/main.go:51-178) round-tripped
+    through the file format."""
+    st = gfk.Stack([gfk.Layer(3.0, 400, 160, 1600), gfk.Layer(0, 900, 400, 2000)])
+    h = gfk.Header(gfk.Provenance("gfk-b200 fk (layered wavenumber integration)"), st, 2000.0, 512,
+                   gfk.RangeGrid(1.0, 10.0, 40), "vertical surface displacement per unit vertical surface point force",
+                   "m/N")
+    m = gfk.Medium(st, default_q=30, engine=engine)
+    b, spectra = gfk.build_bank(m, h, 100.0)
+    path = tmp_path / "g.bank"
+    b.write(path)
+    r = gfk.open_bank(path)
+    top = int(100.0 / (2000.0 / 512))
+    assert np.array_equal(r.data, b.data)
+    assert (r.data[:, 0] == 0).all() and (r.data[:, top + 1:] == 0).all()
+    assert np.array_equal(r.data[:, 1:top + 1, 0], spectra.T.real.astype(np.float32))
