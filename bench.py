@@ -73,47 +73,58 @@ def allmax(x, world):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """SM clock and clock-event (throttle) reasons sampled every 10 ms through
+    NVML while the timed region runs (read-only queries)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "hw_power_brake_slowdown": 0x80, "sw_power_cap": 0x4}
 
     def __init__(self, device):
         self.device = device
         self.rows = []
-        self.proc = None
+        self.stop_flag = threading.Event()
+        self.thread = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except (FileNotFoundError, OSError):
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            h = None
+            try:
+                import torch
+                prop = torch.cuda.get_device_properties(self.device)
+                bus = f"{prop.pci_domain_id:08x}:{prop.pci_bus_id:02x}:{prop.pci_device_id:02x}.0"
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self.nv, self.h = pynvml, h
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+            return
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                self.rows.append(parts)
+    def _run(self):
+        nv, h = self.nv, self.h
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((sm, reasons))
+            except Exception:
+                pass
+            time.sleep(0.01)
 
     def stop(self):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-        if not self.rows:
+        if not self.thread:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+        self.stop_flag.set()
+        self.thread.join(timeout=2)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        reasons = sorted({name for _, r in self.rows for name, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": self.max_mhz,
                 "reasons": reasons, "samples": len(self.rows)}
 
 
@@ -223,6 +234,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gfk", choices=["gfk", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--freq-stride", type=int, default=1,
+                    help="profiling only: keep every n-th frequency (a smaller case of the same kernels)")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling only: skip the e2e leg, the FP64 peak probe and the CPU baseline")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -233,6 +248,8 @@ def main():
     import __graft_entry__
     gfk = __graft_entry__.load_package()
     wl = gfk.workloads.graded_soil()
+    if args.freq_stride > 1:
+        wl.freqs = wl.freqs[::args.freq_stride].copy()
     eng = gfk.Engine(local)
     med = wl.medium(gfk.DUNKIN, engine=eng)
     plan = gfk.Plan(med, wl.ranges, wl.freqs, wl.integration(), engine=eng)
@@ -284,6 +301,11 @@ def main():
                                           ctypes.cast(status_host.data_ptr(), ctypes.POINTER(ctypes.c_int32)))
         eng.check(st)
 
+    if args.profile:
+        plan.close()
+        eng.close()
+        print(json.dumps({"profile_run": True, "ms_per_step": step_ms, "kernel_ms": [prop_ms, quad_ms, other_ms]}))
+        return
     e2e_call()
     barrier(world)
     t0 = time.perf_counter()

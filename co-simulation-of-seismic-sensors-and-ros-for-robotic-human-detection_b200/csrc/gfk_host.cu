@@ -15,11 +15,14 @@
 
 // ------------------------------------------------------------------ ctx --
 
+struct gfk_plan;
+
 struct gfk_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string last_error;
     int64_t launches = 0;
+    std::vector<gfk_plan*> plans;  // live plans, destroyed by gfk_close
 };
 
 namespace {
@@ -447,8 +450,10 @@ int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const doub
         delete p;
         return st;
     }
-    const int nchunks = (int)p->chunk_begin.size() - 1;
-    p->launches_per_exec = 2 + 3 * nchunks + (p->shared ? 1 : 0);
+    int nchunks = 0;
+    for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
+        if (p->chunk_begin[c + 1] > p->chunk_begin[c]) nchunks++;
+    p->launches_per_exec = nf > 0 ? 2 + 2 * nchunks + (p->shared ? 1 : 0) : 0;
     *out = p;
     return GFK_OK;
 }
@@ -576,6 +581,11 @@ int gfk_open(int device, gfk_ctx** out) {
 int gfk_close(gfk_ctx* ctx) {
     if (!ctx) return GFK_OK;
     cudaSetDevice(ctx->device);
+    for (gfk_plan* p : ctx->plans) {  // plans still open become invalid here
+        plan_free(p);
+        delete p;
+    }
+    ctx->plans.clear();
     if (ctx->stream) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);
@@ -603,7 +613,9 @@ int gfk_plan_create(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const
     if (!out) return GFK_EARG;
     if (!ctx) return GFK_EARG;
     cudaSetDevice(ctx->device);
-    return plan_build(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, out);
+    int st = plan_build(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, out);
+    if (!st) ctx->plans.push_back(*out);
+    return st;
 }
 
 int gfk_plan_execute(gfk_plan* p) {
@@ -644,6 +656,8 @@ int gfk_plan_kernel_times(gfk_plan* p, double* prop_ms, double* quad_ms, double*
 int gfk_plan_destroy(gfk_plan* p) {
     if (!p) return GFK_OK;
     cudaSetDevice(p->ctx->device);
+    auto& v = p->ctx->plans;
+    v.erase(std::remove(v.begin(), v.end(), p), v.end());
     plan_free(p);
     delete p;
     return GFK_OK;

@@ -9,6 +9,7 @@ internal/visco/visco.go:42-108); every computation runs in libgfk on the GPU.
 """
 import ctypes
 import math
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -240,6 +241,7 @@ class Engine:
                               "(libgfk needs a CUDA device; there is no CPU fallback)")
         self.ctx = h
         self.device = device
+        self._plans = weakref.WeakSet()
 
     def check(self, st):
         if st:
@@ -251,6 +253,8 @@ class Engine:
 
     def close(self):
         if self.ctx:
+            for p in list(self._plans):
+                p.close()
             N.lib().gfk_close(self.ctx)
             self.ctx = None
 
@@ -287,6 +291,7 @@ class Plan:
                                          opt.c(), ctypes.byref(h))
         self.engine.check(st)
         self.p = h
+        self.engine._plans.add(self)
 
     def execute(self):
         self.engine.check(N.lib().gfk_plan_execute(self.p))
@@ -316,7 +321,8 @@ class Plan:
 
     def close(self):
         if self.p:
-            N.lib().gfk_plan_destroy(self.p)
+            if self.engine.ctx:  # a closed engine has destroyed its plans already
+                N.lib().gfk_plan_destroy(self.p)
             self.p = None
 
     def __del__(self):

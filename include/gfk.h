@@ -118,8 +118,11 @@ typedef struct gfk_solve {
 /* ---- context -------------------------------------------------------------- */
 typedef struct gfk_ctx gfk_ctx;
 
-/* Creates a context on CUDA device `device`: one stream, a scratch arena. */
+/* Creates a context on CUDA device `device`: one stream; device buffers come
+ * from the device's stream-ordered memory pool, kept cached between calls. */
 int gfk_open(int device, gfk_ctx **out);
+/* Destroys the context and any of its plans still open (their handles
+ * become invalid). */
 int gfk_close(gfk_ctx *ctx);
 /* Short name of a status code. */
 const char *gfk_status_string(int status);
