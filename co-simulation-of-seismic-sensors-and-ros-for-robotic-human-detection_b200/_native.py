@@ -27,7 +27,7 @@ EXPORTS = [
     "gfk_vertical_displacement_multi", "gfk_bank_spectra",
     "gfk_plan_create", "gfk_plan_execute", "gfk_plan_result_device", "gfk_plan_download",
     "gfk_plan_launches_per_execute", "gfk_plan_kernel_times", "gfk_plan_destroy",
-    "gfk_bank_pack", "gfk_bank_write",
+    "gfk_bank_pack", "gfk_bank_write", "gfk_vertical_displacement_multi_noalloc",
 ]
 
 
@@ -96,6 +96,8 @@ def lib():
         "gfk_plan_destroy": (ctypes.c_int, [vp]),
         "gfk_bank_pack": (ctypes.c_int, [P(d), i32, i32, i32, i32, P(ctypes.c_float)]),
         "gfk_bank_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, P(ctypes.c_float), i64]),
+        "gfk_vertical_displacement_multi_noalloc": (ctypes.c_int, [P(GfkMedium), P(GfkSolve), P(d), i32, d,
+                                                                   GfkIntegration, P(d), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -8,7 +8,7 @@ PKG = pathlib.Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libgfk.so"
-SOURCES = ["gfk_kernels.cu", "gfk_host.cu"]
+SOURCES = ["gfk_kernels.cu", "gfk_host.cu", "gfk_noalloc.cu"]
 HEADERS = ["gfk_math.cuh", "gfk_solver.cuh", "gfk_kernels.cuh"]
 
 NVCC_FLAGS = [

@@ -1,0 +1,166 @@
+// gfk_noalloc.cu — a VerticalDisplacementMulti that allocates nothing.
+//
+// Some callers cannot allocate device memory at the time they need a
+// response: a process whose device memory has been claimed up front by
+// another framework's caching allocator (a cudaMalloc there fails or fights
+// that pool), and latency-bound loops, such as a sensor node producing fixed
+// chunks on a deadline, where cudaMalloc/cudaFree can synchronise the device
+// and stall every other stream. This entry point serves them: all the device
+// memory it uses is one fixed array compiled into the library, so a call does
+// no cudaMalloc, cudaFree or stream-ordered allocation, and no host heap
+// allocation either.
+//
+// The array is a file-scope __device__ buffer of kNoallocScratchBytes (4 MiB).
+// Every GPU that loads libgfk holds it until the process exits, and every call
+// on a device shares it, so calls whose GPU work overlaps — on two streams, or
+// from two host threads — race on it and must be serialised by the caller.
+// Host code may not use the array's name as a device address; the address is
+// looked up once per device with cudaGetSymbolAddress, with that device
+// current, by the first call made on it. Make that first call before any
+// stream capture begins.
+#include <cstddef>
+#include <mutex>
+
+#include "../../include/gfk.h"
+#include "gfk_kernels.cuh"
+
+namespace {
+
+constexpr size_t kNoallocScratchBytes = size_t(4) << 20;
+
+// Layout of the scratch array (offsets in bytes, each 256-aligned).
+constexpr size_t kOffLayersP = 0;                                                  // LayerP[64]
+constexpr size_t kOffLayersC = 4096;                                               // LayerC[64]
+constexpr size_t kOffScalars = kOffLayersC + 64 * sizeof(gfk::LayerC);             // per-call scalars
+constexpr size_t kOffRanges = kOffScalars + 256;                                   // double[nr]
+constexpr size_t kOffG = kOffRanges + size_t(GFK_NOALLOC_MAX_RANGES) * 8;          // cd[nr]
+constexpr size_t kOffRem = kOffG + size_t(GFK_NOALLOC_MAX_RANGES) * 16;            // cd[nk]
+static_assert(kOffRem + size_t(GFK_NOALLOC_MAX_SAMPLES) * 16 <= kNoallocScratchBytes, "scratch too small");
+static_assert(64 * sizeof(gfk::LayerP) <= kOffLayersC, "layer block too small");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+// Per-call scalars, copied into the scratch array's scalar block.
+struct Scalars {
+    double freq, dk, kfar;
+    int64_t off;
+    int nk;
+    int status;
+    cd wc2, C;
+};
+static_assert(sizeof(Scalars) <= 256, "scalar block too small");
+
+std::mutex g_setup_mu;
+void* g_scratch_addr[256] = {nullptr};  // device address of the array, per device ordinal
+
+int scratch_address(int device, unsigned char** out) {
+    if (device < 0 || device >= 256) return GFK_ECUDA;
+    std::lock_guard<std::mutex> lock(g_setup_mu);
+    if (!g_scratch_addr[device]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) return GFK_ECUDA;
+        g_scratch_addr[device] = ptr;
+    }
+    *out = static_cast<unsigned char*>(g_scratch_addr[device]);
+    return GFK_OK;
+}
+
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+
+}  // namespace
+
+extern "C" int gfk_vertical_displacement_multi_noalloc(const gfk_medium* m, const gfk_solve* s,
+                                                       const double* ranges_m, int32_t nr, double freq_hz,
+                                                       gfk_integration opt, double* out, void* stream) {
+    if (!m || !s || !out || !ranges_m) return GFK_EARG;
+    if (nr <= 0) return GFK_EARG;
+    if (nr > GFK_NOALLOC_MAX_RANGES) return GFK_ELIMIT;
+    if (s->formulation != GFK_REFERENCE_DIRECT && s->formulation != GFK_DUNKIN) return GFK_EARG;
+    if (s->quadrature != GFK_PLAIN_FP64) return GFK_EARG;
+    if (s->formulation == GFK_REFERENCE_DIRECT && s->omega_imag != 0) return GFK_EARG;
+    if (!(s->omega_imag >= 0) || !(s->omega_imag < INFINITY)) return GFK_EARG;
+    if (!m->layers || m->count <= 0) return GFK_ESTACK;
+    if (m->count > gfk::kMaxLayers) return GFK_ELIMIT;
+    // the reference's order: guard, grid, then the stack (fk.go:507-523, 280)
+    if (s->guard || s->formulation == GFK_REFERENCE_DIRECT) {
+        int st = gfk_check_layer_phase(m, freq_hz);
+        if (st) return st;
+    }
+    gfk_grid g;
+    int st = gfk_grid_for(m, ranges_m, nr, freq_hz, opt, &g);
+    if (st) return st;
+    if (!(freq_hz > 0)) return GFK_EARG;
+    st = gfk_stack_validate(m);
+    if (st) return st;
+    if (g.samples > GFK_NOALLOC_MAX_SAMPLES) return GFK_ELIMIT;
+
+    cudaStream_t strm = static_cast<cudaStream_t>(stream);
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return GFK_ECUDA;
+    unsigned char* base = nullptr;
+    if ((st = scratch_address(device, &base))) return st;
+
+    gfk::LayerP lp[gfk::kMaxLayers];
+    double mu_ref = 0, slowest = m->layers[0].vs_mps, rmin = ranges_m[0];
+    for (int i = 0; i < m->count; i++) {
+        const gfk_layer& l = m->layers[i];
+        lp[i] = gfk::LayerP{l.thickness_m, l.vp_mps, l.vs_mps, l.density_kgm3, l.qs, l.qp};
+        mu_ref = fmax(mu_ref, l.density_kgm3 * l.vs_mps * l.vs_mps);
+        slowest = fmin(slowest, l.vs_mps);
+    }
+    for (int j = 0; j < nr; j++) rmin = fmin(rmin, ranges_m[j]);
+    Scalars sc{};
+    sc.freq = freq_hz;
+    sc.dk = g.kmax / g.samples;
+    sc.kfar = fmax(200 * (kTwoPi * freq_hz / slowest), 400 / rmin);  // fk.go:515-521
+    sc.off = 0;
+    sc.nk = g.samples;
+    sc.status = 0;  // the array keeps the last call's flags: cleared here
+
+    auto* d_lp = reinterpret_cast<gfk::LayerP*>(base + kOffLayersP);
+    auto* d_lc = reinterpret_cast<gfk::LayerC*>(base + kOffLayersC);
+    unsigned char* sb = base + kOffScalars;
+    auto* d_sc = reinterpret_cast<Scalars*>(sb);
+    auto* d_freq = reinterpret_cast<double*>(sb + offsetof(Scalars, freq));
+    auto* d_dk = reinterpret_cast<double*>(sb + offsetof(Scalars, dk));
+    auto* d_kfar = reinterpret_cast<double*>(sb + offsetof(Scalars, kfar));
+    auto* d_off = reinterpret_cast<int64_t*>(sb + offsetof(Scalars, off));
+    auto* d_nk = reinterpret_cast<int*>(sb + offsetof(Scalars, nk));
+    auto* d_status = reinterpret_cast<int*>(sb + offsetof(Scalars, status));
+    auto* d_wc2 = reinterpret_cast<cd*>(sb + offsetof(Scalars, wc2));
+    auto* d_C = reinterpret_cast<cd*>(sb + offsetof(Scalars, C));
+    auto* d_r = reinterpret_cast<double*>(base + kOffRanges);
+    auto* d_G = reinterpret_cast<cd*>(base + kOffG);
+    auto* d_rem = reinterpret_cast<cd*>(base + kOffRem);
+
+    gfk::MediumP mp;
+    mp.ref_freq = m->ref_freq_hz;
+    mp.default_q = m->default_q;
+    mp.tau_sigma = m->sls_tau_sigma;
+    mp.tau_eps = m->sls_tau_eps;
+    mp.count = m->count;
+    mp.sls = (m->sls_tau_sigma > 0 && m->sls_tau_eps > 0) ? 1 : 0;
+
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    ok(cudaMemcpyAsync(d_lp, lp, sizeof(gfk::LayerP) * m->count, cudaMemcpyHostToDevice, strm));
+    ok(cudaMemcpyAsync(d_sc, &sc, sizeof sc, cudaMemcpyHostToDevice, strm));
+    ok(cudaMemcpyAsync(d_r, ranges_m, sizeof(double) * nr, cudaMemcpyHostToDevice, strm));
+    if (e != cudaSuccess) return GFK_ECUDA;
+    const int form = s->formulation;
+    gfk::launch_layer_consts(strm, d_lp, mp, d_freq, 1, s->omega_imag, mu_ref, form, d_lc, d_wc2);
+    gfk::launch_static(strm, d_lc, m->count, d_freq, d_wc2, d_kfar, 1, mu_ref, form, d_C, d_status);
+    gfk::launch_prop(strm, d_lc, m->count, d_freq, d_wc2, 1, d_nk, d_dk, d_off, g.samples, d_C, mu_ref, form, d_rem,
+                     d_status);
+    gfk::launch_quad_ragged(strm, d_rem, d_C, d_r, 1, nr, d_nk, d_dk, d_off, d_G);
+    ok(cudaGetLastError());
+    int flags = 0;
+    ok(cudaMemcpyAsync(out, d_G, sizeof(cd) * nr, cudaMemcpyDeviceToHost, strm));
+    ok(cudaMemcpyAsync(&flags, d_status, sizeof(int), cudaMemcpyDeviceToHost, strm));
+    ok(cudaStreamSynchronize(strm));
+    if (e != cudaSuccess) return GFK_ECUDA;
+    if (flags & gfk::kStSingular) return GFK_ESINGULAR;
+    if (flags & gfk::kStNonfinite) return GFK_ENONFINITE;
+    return GFK_OK;
+}

@@ -197,6 +197,29 @@ int gfk_plan_kernel_times(gfk_plan *p, double *prop_ms, double *quad_ms,
                           double *other_ms, int32_t reset);
 int gfk_plan_destroy(gfk_plan *p);
 
+/* ---- allocation-free variant --------------------------------------------- */
+/* No counterpart in the reference: a gfk_vertical_displacement_multi for
+ * callers that cannot allocate device memory when they need a response — a
+ * process whose device memory another framework's caching allocator has
+ * already claimed, or a deadline-bound loop (a sensor node emitting fixed
+ * chunks) where cudaMalloc/cudaFree can synchronise the device. It performs no
+ * device, stream-ordered or host heap allocation: its device working memory is
+ * one 4 MiB array compiled into libgfk, which every GPU that loads the library
+ * holds until exit. Limits: nr <= GFK_NOALLOC_MAX_RANGES ranges and a grid of
+ * at most GFK_NOALLOC_MAX_SAMPLES wavenumbers; larger requests return
+ * GFK_ELIMIT. Inputs and the output (nr (re, im) pairs) are host memory; the
+ * work runs on `stream` (a cudaStream_t, NULL for the default stream) of the
+ * current device and the call returns after it completes. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current; make it before any stream capture begins. All calls share
+ * the array, so calls whose GPU work overlaps race and must be serialised by
+ * the caller. Statuses as gfk_vertical_displacement_multi; no message is kept. */
+#define GFK_NOALLOC_MAX_RANGES 16384
+#define GFK_NOALLOC_MAX_SAMPLES 196608
+int gfk_vertical_displacement_multi_noalloc(const gfk_medium *m, const gfk_solve *s,
+                                            const double *ranges_m, int32_t nr, double freq_hz,
+                                            gfk_integration opt, double *out, void *stream);
+
 /* ---- bank file (internal/bank/format.go:32-46, 215-240) ------------------ */
 /* Packs an FP64 [nf][nr] result into the bank's float32 payload: range-major
  * [count][bins] (re, im) pairs with bin = first_bin + f index; bins outside
