@@ -260,6 +260,7 @@ def main():
     got, status = plan.download()
     assert (status == 0).all() and np.isfinite(got).all()
     plan.kernel_times(reset=True)
+    variant, tune_ms = plan.tuning()
 
     # --- device-resident timing -----------------------------------------
     clocks = ClockSampler(local)
@@ -304,7 +305,8 @@ def main():
     if args.profile:
         plan.close()
         eng.close()
-        print(json.dumps({"profile_run": True, "ms_per_step": step_ms, "kernel_ms": [prop_ms, quad_ms, other_ms]}))
+        print(json.dumps({"profile_run": True, "ms_per_step": step_ms, "kernel_ms": [prop_ms, quad_ms, other_ms],
+                          "prop_variant": variant, "tune_ms": tune_ms}))
         return
     e2e_call()
     barrier(world)
@@ -335,6 +337,7 @@ def main():
                 "algorithmic_flops": {"propagator": f_prop, "quadrature": f_quad},
                 "step_frac_of_fp64_roofline": roof_time / (step_ms * 1e-3),
                 "kernel_ms": {"propagator": prop_ms, "quadrature": quad_ms, "other": other_ms},
+                "propagator_launch_shape": {"chosen": variant, "tuning_ms": tune_ms},
                 "hbm_gbs_peak": peaks.get("hbm_gbs")}
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

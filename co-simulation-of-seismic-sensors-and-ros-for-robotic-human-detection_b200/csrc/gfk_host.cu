@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -207,6 +208,8 @@ struct gfk_plan {
     int* d_status = nullptr;
     int64_t rem_capacity = 0;  // complex values
     int32_t launches_per_exec = 0;
+    int prop_variant = -1;  // Dunkin launch shape; -1 until the first execute tunes it
+    std::vector<float> tune_ms;  // per variant, from the tuning run
     // timing
     std::vector<TimedSeg> segs;
     size_t seg_next = 0;
@@ -458,6 +461,57 @@ int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const doub
     return GFK_OK;
 }
 
+// Times every Dunkin launch shape on a window of up to 64 of the plan's own
+// frequencies (the middle of the band) and keeps the fastest. The window's
+// integrand rows are recomputed by the real launch afterwards.
+int tune_prop(gfk_plan* p) {
+    gfk_ctx* ctx = p->ctx;
+    cudaStream_t s = ctx->stream;
+    const int nv = gfk::prop_variant_count();
+    p->prop_variant = 0;
+    if (const char* env = getenv("GFK_PROP_VARIANT")) {
+        p->prop_variant = std::max(0, std::min(nv - 1, atoi(env)));
+        return GFK_OK;
+    }
+    if (p->solve.formulation != GFK_DUNKIN || p->nf == 0) return GFK_OK;
+    const int c0 = p->chunk_begin[0], c1 = p->chunk_begin[1];
+    const int win = std::min(64, c1 - c0);
+    if (win <= 0) return GFK_OK;
+    const int fb = c0 + (c1 - c0 - win) / 2;
+    int cmax = 0;
+    for (int f = fb; f < fb + win; f++) cmax = std::max(cmax, p->nk[f]);
+    if ((int64_t)win * cmax < 4096) return GFK_OK;  // too little work to tell shapes apart
+    cudaEvent_t a, b;
+    GFK_CUDA(ctx, cudaEventCreate(&a));
+    GFK_CUDA(ctx, cudaEventCreate(&b));
+    p->tune_ms.assign(nv, INFINITY);
+    for (int rep = 0; rep < 2; rep++)
+        for (int v = 0; v < nv; v++) {
+            cudaEventRecord(a, s);
+            gfk::launch_prop(s, p->d_lc + (size_t)fb * p->nl, p->nl, p->d_freqs + fb, p->d_wc2 + fb, win,
+                             p->d_nk + fb, p->d_dk + fb, p->d_off + fb, cmax, p->d_C + fb, p->mu_ref, GFK_DUNKIN,
+                             p->d_rem, p->d_status + fb, v);
+            cudaEventRecord(b, s);
+            ctx->launches++;
+            cudaError_t e = cudaEventSynchronize(b);
+            if (e != cudaSuccess) {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+                return fail(ctx, GFK_ECUDA, "propagator tuning: %s", cudaGetErrorString(e));
+            }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            p->tune_ms[v] = std::min(p->tune_ms[v], ms);
+        }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    int best = 0;
+    for (int v = 1; v < nv; v++)
+        if (p->tune_ms[v] < p->tune_ms[best]) best = v;
+    p->prop_variant = best;
+    return GFK_OK;
+}
+
 int plan_exec(gfk_plan* p) {
     gfk_ctx* ctx = p->ctx;
     cudaStream_t s = ctx->stream;
@@ -477,6 +531,7 @@ int plan_exec(gfk_plan* p) {
     if (p->shared) gfk::launch_j0_table(s, p->d_ranges, p->nr, p->nk[0], p->dk[0], p->d_W);
     if ((st = end_seg(p, seg))) return st;
     ctx->launches += 2 + (p->shared ? 1 : 0);
+    if (p->prop_variant < 0 && (st = tune_prop(p))) return st;
     for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++) {
         const int fb = p->chunk_begin[c], fe = p->chunk_begin[c + 1];
         const int cnf = fe - fb;
@@ -485,7 +540,8 @@ int plan_exec(gfk_plan* p) {
         for (int f = fb; f < fe; f++) cmax = std::max(cmax, p->nk[f]);
         if ((st = begin_seg(p, 0, &seg))) return st;
         gfk::launch_prop(s, p->d_lc + (size_t)fb * p->nl, p->nl, p->d_freqs + fb, p->d_wc2 + fb, cnf, p->d_nk + fb,
-                         p->d_dk + fb, p->d_off + fb, cmax, p->d_C + fb, p->mu_ref, form, p->d_rem, p->d_status + fb);
+                         p->d_dk + fb, p->d_off + fb, cmax, p->d_C + fb, p->mu_ref, form, p->d_rem, p->d_status + fb,
+                         p->prop_variant);
         if ((st = end_seg(p, seg))) return st;
         if ((st = begin_seg(p, 1, &seg))) return st;
         if (p->shared)
@@ -637,6 +693,14 @@ int gfk_plan_download(gfk_plan* p, double* out, int32_t* status_per_f) {
 }
 
 int32_t gfk_plan_launches_per_execute(const gfk_plan* p) { return p ? p->launches_per_exec : 0; }
+
+int gfk_plan_tuning(const gfk_plan* p, int32_t* variant, float* ms_per_variant, int32_t capacity) {
+    if (!p || !variant) return GFK_EARG;
+    *variant = p->prop_variant;
+    const int n = (int)p->tune_ms.size();
+    for (int i = 0; ms_per_variant && i < std::min(n, (int)capacity); i++) ms_per_variant[i] = p->tune_ms[i];
+    return n;
+}
 
 int gfk_plan_kernel_times(gfk_plan* p, double* prop_ms, double* quad_ms, double* other_ms, int32_t reset) {
     if (!p) return GFK_EARG;

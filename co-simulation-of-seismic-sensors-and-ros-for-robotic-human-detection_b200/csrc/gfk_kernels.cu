@@ -96,11 +96,14 @@ void launch_static(cudaStream_t s, const LayerC* lc, int nl, const double* freqs
 }
 
 // ------------------------------------------------------------ propagator --
+//
+// One thread per (f, k) (ILP = 1) or per (f, k, k + half-block) pair (ILP = 2,
+// two wavenumbers in lockstep). The block's layer constants are staged in
+// shared memory; every block serves one frequency. Launch shapes are template
+// parameters; the plan times them once and keeps the fastest.
 
-constexpr int kPropThreads = 128;
-
-template <int FORM>
-__global__ __launch_bounds__(kPropThreads) void k_prop(const LayerC* __restrict__ lc, int nl,
+template <int FORM, int THREADS, int MINB, int ILP>
+__global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict__ lc, int nl,
                                                        const double* __restrict__ freqs, const cd* __restrict__ wc2,
                                                        const int* __restrict__ nk, const double* __restrict__ dk,
                                                        const int64_t* __restrict__ off, const cd* __restrict__ C,
@@ -110,34 +113,76 @@ __global__ __launch_bounds__(kPropThreads) void k_prop(const LayerC* __restrict_
     for (int l = threadIdx.x; l < nl; l += blockDim.x) s_lc[l] = lc[(size_t)f * nl + l];
     __syncthreads();
     const int n = nk[f];
-    const int i = blockIdx.x * kPropThreads + threadIdx.x + 1;
-    if (i > n) return;
-    const double k = (double)i * dk[f];
-    cd u;
+    const double d = dk[f];
+    const cd c = C[f];
+    const int i0 = blockIdx.x * (THREADS * ILP) + threadIdx.x + 1;
+    if (i0 > n) return;
+    cd* row = rem + off[f];
+    int bad = 0;
     if (FORM == 0) {
         bool ok;
-        u = direct_u(s_lc, nl, kTwoPi * freqs[f], k, mu_ref, ok);
-        if (!ok) atomicOr(status + f, kStSingular);
+        const double k = (double)i0 * d;
+        cd u = direct_u(s_lc, nl, kTwoPi * freqs[f], k, mu_ref, ok);
+        if (!ok) bad |= kStSingular;
+        cd r = k * u - c;
+        if (!finite_cd(r)) { bad |= kStNonfinite; r = mk(0.0); }
+        row[i0 - 1] = r;
+    } else if (ILP == 1) {
+        const double k = (double)i0 * d;
+        cd r = k * dunkin_u(s_lc, nl, wc2[f], k, mu_ref) - c;
+        if (!finite_cd(r)) { bad |= kStNonfinite; r = mk(0.0); }
+        row[i0 - 1] = r;
     } else {
-        u = dunkin_u(s_lc, nl, wc2[f], k, mu_ref);
+        const int i1 = i0 + THREADS;
+        const bool has1 = i1 <= n;
+        const double k0 = (double)i0 * d;
+        const double k1 = has1 ? (double)i1 * d : k0;
+        cd u0, u1;
+        dunkin_u2(s_lc, nl, wc2[f], k0, k1, mu_ref, u0, u1);
+        cd r0 = k0 * u0 - c;
+        if (!finite_cd(r0)) { bad |= kStNonfinite; r0 = mk(0.0); }
+        row[i0 - 1] = r0;
+        if (has1) {
+            cd r1 = k1 * u1 - c;
+            if (!finite_cd(r1)) { bad |= kStNonfinite; r1 = mk(0.0); }
+            row[i1 - 1] = r1;
+        }
     }
-    cd r = k * u - C[f];
-    if (!finite_cd(r)) {
-        atomicOr(status + f, kStNonfinite);
-        r = mk(0.0);
-    }
-    rem[off[f] + (i - 1)] = r;
+    if (bad) atomicOr(status + f, bad);
 }
+
+namespace {
+struct PropVariant {
+    void (*fn)(const LayerC*, int, const double*, const cd*, const int*, const double*, const int64_t*, const cd*,
+               double, cd*, int*);
+    int threads, ilp;
+};
+const PropVariant kDunkinVariants[] = {
+    {k_prop<1, 128, 4, 1>, 128, 1},  // <= 128 registers, 16 warps/SM
+    {k_prop<1, 128, 5, 1>, 128, 1},  // <= 96 registers, 20 warps/SM
+    {k_prop<1, 128, 6, 1>, 128, 1},  // <= 80 registers, 24 warps/SM
+    {k_prop<1, 128, 2, 2>, 128, 2},  // two wavenumbers in lockstep, 8 warps/SM
+    {k_prop<1, 64, 4, 2>, 64, 2},
+    {k_prop<1, 256, 2, 1>, 256, 1},
+};
+}  // namespace
+
+int prop_variant_count() { return (int)(sizeof(kDunkinVariants) / sizeof(kDunkinVariants[0])); }
 
 void launch_prop(cudaStream_t s, const LayerC* lc, int nl, const double* freqs, const cd* wc2, int nf,
                  const int* nk, const double* dk, const int64_t* off, int max_nk, const cd* C, double mu_ref,
-                 int formulation, cd* rem, int* status) {
+                 int formulation, cd* rem, int* status, int variant) {
     if (nf <= 0 || max_nk <= 0) return;
-    dim3 grid((max_nk + kPropThreads - 1) / kPropThreads, nf);
-    if (formulation == 0)
-        k_prop<0><<<grid, kPropThreads, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status);
-    else
-        k_prop<1><<<grid, kPropThreads, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status);
+    if (formulation == 0) {
+        dim3 grid((max_nk + 127) / 128, nf);
+        k_prop<0, 128, 1, 1><<<grid, 128, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status);
+        return;
+    }
+    if (variant < 0 || variant >= prop_variant_count()) variant = 0;
+    const PropVariant& v = kDunkinVariants[variant];
+    const int per_block = v.threads * v.ilp;
+    dim3 grid((max_nk + per_block - 1) / per_block, nf);
+    v.fn<<<grid, v.threads, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status);
 }
 
 // -------------------------------------------------------------- J0 table --

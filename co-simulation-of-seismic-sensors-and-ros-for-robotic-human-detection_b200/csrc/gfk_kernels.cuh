@@ -15,9 +15,11 @@ void launch_static(cudaStream_t s, const LayerC* lc, int nl, const double* freqs
                    const double* kfar, int nf, double mu_ref, int formulation, cd* C, int* status);
 
 // rem[off[f] + i - 1] = k_i u(k_i, f) - C_f for i = 1..nk[f], k_i = i dk[f].
+// `variant` picks one of prop_variant_count() launch shapes of the Dunkin kernel.
 void launch_prop(cudaStream_t s, const LayerC* lc, int nl, const double* freqs, const cd* wc2, int nf,
                  const int* nk, const double* dk, const int64_t* off, int max_nk, const cd* C,
-                 double mu_ref, int formulation, cd* rem, int* status);
+                 double mu_ref, int formulation, cd* rem, int* status, int variant = 0);
+int prop_variant_count();
 
 // W[(i-1) nr + j] = w_i J0(k_i r_j) dk, w = 1/2 at i = nk.
 void launch_j0_table(cudaStream_t s, const double* ranges, int nr, int nk, double dk, double* W);

@@ -75,6 +75,56 @@ GFK_HD cd cexpm1_(cd z) {
     return cd{em * c - 2.0 * sh * sh, (em + 1.0) * s};
 }
 
+// Reciprocal and reciprocal square root, correctly rounded / within 1 ulp on
+// the device; the host versions exist so the solver can be compiled and checked
+// on the CPU.
+GFK_HD double rcp_(double x) {
+#ifdef __CUDA_ARCH__
+    return __drcp_rn(x);
+#else
+    return 1.0 / x;
+#endif
+}
+GFK_HD double rsqrt_(double x) {
+#ifdef __CUDA_ARCH__
+    return rsqrt(x);
+#else
+    return 1.0 / sqrt(x);
+#endif
+}
+
+// 1/b = conj(b)/|b|^2 with one real reciprocal. For the moderate magnitudes of
+// the solver's quantities (|b| within 1e-150..1e150) this is accurate to a few
+// ulp and much cheaper than Smith's division.
+GFK_HD cd crcp_(cd b) {
+    const double t = rcp_(fma(b.re, b.re, b.im * b.im));
+    return cd{b.re * t, -b.im * t};
+}
+GFK_HD cd cdiv_fast(cd a, cd b) { return a * crcp_(b); }
+
+// Principal square root from one sqrt and one rsqrt: with r = |z|,
+// s = (|x| + r)/2 and t = sqrt(s): (t, y/2t) for x >= 0, (|y|/2t, copysign(t, y))
+// otherwise.
+GFK_HD cd csqrt_fast(cd z) {
+    const double r = sqrt(fma(z.re, z.re, z.im * z.im));
+    const double s = 0.5 * (fabs(z.re) + r);
+    if (s == 0.0) return cd{0.0, z.im};
+    const double ti = rsqrt_(s);
+    const double t = s * ti;
+    const double h = 0.5 * ti;
+    if (z.re >= 0.0) return cd{t, z.im * h};
+    return cd{fabs(z.im) * h, copysign(t, z.im)};
+}
+
+// 2^e as a double, built from its bits (|e| < 1000).
+GFK_HD double pow2i(int e) {
+#ifdef __CUDA_ARCH__
+    return __hiloint2double((e + 1023) << 20, 0);
+#else
+    return ldexp(1.0, e);
+#endif
+}
+
 // log(z) = log|z| + i arg z.
 GFK_HD cd clog_(cd z) { return cd{log(hypot(z.re, z.im)), atan2(z.im, z.re)}; }
 

@@ -83,30 +83,39 @@ GFK_HD cd complex_velocity(const MediumP& m, double v, double q, double f, doubl
 // and every other common scale cancel in the surface ratio M_12/M_23.
 
 struct Terms {
-    cd ra, rb, ea, eb, mup, u1, x2, r2;
+    cd ra, rb, ea, eb, ieb, mup, u1, x2, r2;
 };
 
-__device__ __forceinline__ Terms layer_terms(const LayerC& L, cd c2) {
+GFK_HD Terms layer_terms(const LayerC& L, cd c2) {
     Terms t;
     t.ea = c2 * L.c[0];
     t.eb = c2 * L.c[1];
     const cd kap = L.c[2];
     t.mup = L.c[3];
-    t.ra = csqrt_(1.0 - t.ea);  // principal root: Re >= 0, the decaying branch
-    t.rb = csqrt_(1.0 - t.eb);
+    t.ra = csqrt_fast(1.0 - t.ea);  // principal root: Re >= 0, the decaying branch
+    t.rb = csqrt_fast(1.0 - t.eb);
     const cd ra = t.ra, rb = t.rb, ea = t.ea, eb = t.eb;
     const cd rarb = ra * rb;
     const cd rb2p1 = 1.0 + rb * rb;
     if (cnorm1(eb) < 0.35) {
-        // small c: the O(eb) numerators written without cancellation
-        t.u1 = (kap + 1.0 - ea) / (1.0 + rarb);
+        // small c: the O(eb) numerators written without cancellation; the four
+        // denominators share one reciprocal
+        const cd d1 = 1.0 + rarb;
         const cd s = ra + rb;
+        const cd d2 = s * s;
+        const cd d3 = rb2p1 * rb2p1 + 4.0 * rarb;
+        const cd d12 = d1 * d2, d34 = d3 * eb;
+        const cd ip = crcp_(d12 * d34);
+        const cd i12 = d34 * ip, i34 = d12 * ip;  // 1/(d1 d2), 1/(d3 eb)
         const cd omk = 1.0 - kap;
-        t.x2 = (eb * omk * omk) / (s * s) + kap;
+        t.u1 = (kap + 1.0 - ea) * (d2 * i12);
+        t.x2 = (eb * omk * omk) * (d1 * i12) + kap;
         const cd num = 16.0 * (kap - 1.0) + eb * (24.0 - 16.0 * kap + eb * (eb - 8.0));
-        t.r2 = num / (rb2p1 * rb2p1 + 4.0 * rarb);
+        t.r2 = num * (eb * i34);
+        t.ieb = d3 * i34;
     } else {
-        const cd ieb = 1.0 / eb;
+        const cd ieb = crcp_(eb);
+        t.ieb = ieb;
         t.u1 = (1.0 - rarb) * ieb;
         t.x2 = (rb2p1 - 2.0 * rarb) * ieb;
         t.r2 = (rb2p1 * rb2p1 - 4.0 * rarb) * ieb;
@@ -115,7 +124,7 @@ __device__ __forceinline__ Terms layer_terms(const LayerC& L, cd c2) {
 }
 
 // pd ^ g: minors of a layer's two downward-decaying solutions.
-__device__ __forceinline__ void decaying_minors(const Terms& t, cd m[6]) {
+GFK_HD void decaying_minors(const Terms& t, cd m[6]) {
     const cd mu = t.mup;
     m[0] = -t.u1;
     m[1] = -(mu * t.x2);
@@ -126,7 +135,7 @@ __device__ __forceinline__ void decaying_minors(const Terms& t, cd m[6]) {
 }
 
 // m <- C(exp(-A zeta)) m up to a scalar: one layer, bottom to top.
-__device__ __forceinline__ void dunkin_layer_up(const Terms& t, double zeta, cd m[6]) {
+GFK_HD void dunkin_layer_up(const Terms& t, double zeta, cd m[6]) {
     const cd ra = t.ra, rb = t.rb, mu = t.mup, u1 = t.u1, x2 = t.x2, r2 = t.r2;
     const cd rarb = ra * rb;
     const cd tt = mu * (1.0 + rb * rb);
@@ -150,15 +159,18 @@ __device__ __forceinline__ void dunkin_layer_up(const Terms& t, double zeta, cd 
     // y = Q D
     const cd y0 = D5, y1 = -D4, y2 = D3, y3 = D2, y4 = -D1, y5 = D0;
     // exp(-T zeta) compound over exp((ra + rb) zeta): 1, a 4x4 Kronecker block, (EaEb)^2
-    const cd Ea = cexp_(-(ra * zeta));
     const cd Eb = cexp_(-(rb * zeta));
-    const cd delta = (t.eb - t.ea) / (ra + rb);  // ra - rb, cancellation-free
+    const cd delta = (t.eb - t.ea) * crcp_(ra + rb);  // ra - rb, cancellation-free
     const cd dz = delta * zeta;
-    cd W;  // tau (Eb - Ea)/(ra - rb) = rb (Eb - Ea)/eb
+    cd Ea, W;  // W = tau (Eb - Ea)/(ra - rb) = rb (Eb - Ea)/eb
     if (cnorm1(dz) < 0.5) {
-        W = (rb * (Eb * (-1.0) * cexpm1_(-dz))) / t.eb;  // Eb - Ea = -Eb expm1(-delta zeta)
+        const cd em1 = cexpm1_(-dz);  // Ea = Eb exp(-dz), Eb - Ea = -Eb expm1(-dz)
+        const cd e = Eb * em1;
+        Ea = Eb + e;
+        W = (rb * (-e)) * t.ieb;
     } else {
-        W = (rb * (Eb - Ea)) / t.eb;
+        Ea = cexp_(-(ra * zeta));
+        W = (rb * (Eb - Ea)) * t.ieb;
     }
     const cd EaEb = Ea * Eb;
     const cd z0 = y0;
@@ -181,16 +193,16 @@ __device__ __forceinline__ void dunkin_layer_up(const Terms& t, double zeta, cd 
 #pragma unroll
     for (int i = 0; i < 6; i++) mx = fmax(mx, cnorm1(m[i]));
     if (mx > 0.0 && mx < INFINITY) {
-        int e = ilogb(mx);
+        const double sc = pow2i(-ilogb(mx));
 #pragma unroll
-        for (int i = 0; i < 6; i++) m[i] = cldexp(m[i], -e);
+        for (int i = 0; i < 6; i++) m[i] = m[i] * sc;
     }
 }
 
 // Surface vertical displacement per newton (fk.go:276-327) by minor
 // propagation: u_z = i b4 M_12/M_23 with b4 = -i/(2 pi mu_ref k).
-__device__ __forceinline__ cd dunkin_u(const LayerC* L, int n, cd wc2, double k, double mu_ref) {
-    const cd c2 = wc2 / (k * k);
+GFK_HD cd dunkin_u(const LayerC* L, int n, cd wc2, double k, double mu_ref) {
+    const cd c2 = wc2 * (1.0 / (k * k));
     cd m[6];
     {
         Terms t = layer_terms(L[n - 1], c2);
@@ -201,6 +213,28 @@ __device__ __forceinline__ cd dunkin_u(const LayerC* L, int n, cd wc2, double k,
         dunkin_layer_up(t, k * L[i].h, m);
     }
     return m[3] / ((kTwoPi * mu_ref * k) * m[5]);
+}
+
+// Two wavenumbers of one frequency in lockstep through the layers: two
+// independent dependency chains per thread, for latency hiding at low occupancy.
+GFK_HD void dunkin_u2(const LayerC* L, int n, cd wc2, double k0, double k1, double mu_ref, cd& u0, cd& u1) {
+    const cd c20 = wc2 * (1.0 / (k0 * k0));
+    const cd c21 = wc2 * (1.0 / (k1 * k1));
+    cd m0[6], m1[6];
+    {
+        Terms t0 = layer_terms(L[n - 1], c20);
+        Terms t1 = layer_terms(L[n - 1], c21);
+        decaying_minors(t0, m0);
+        decaying_minors(t1, m1);
+    }
+    for (int i = n - 2; i >= 0; i--) {
+        Terms t0 = layer_terms(L[i], c20);
+        Terms t1 = layer_terms(L[i], c21);
+        dunkin_layer_up(t0, k0 * L[i].h, m0);
+        dunkin_layer_up(t1, k1 * L[i].h, m1);
+    }
+    u0 = m0[3] / ((kTwoPi * mu_ref * k0) * m0[5]);
+    u1 = m1[3] / ((kTwoPi * mu_ref * k1) * m1[5]);
 }
 
 // ------------------------------------------------------ reference direct --

@@ -312,6 +312,13 @@ class Plan:
     def launches_per_execute(self):
         return int(N.lib().gfk_plan_launches_per_execute(self.p))
 
+    def tuning(self):
+        """(chosen propagator launch shape, ms per shape) from the first execute."""
+        v = ctypes.c_int32()
+        ms = (ctypes.c_float * 16)()
+        n = N.lib().gfk_plan_tuning(self.p, ctypes.byref(v), ms, 16)
+        return int(v.value), [float(ms[i]) for i in range(max(n, 0))]
+
     def kernel_times(self, reset=False):
         """(propagator, quadrature, other) ms per execute, CUDA-event timed."""
         a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()

@@ -188,8 +188,15 @@ int gfk_plan_execute(gfk_plan *p);
 int gfk_plan_result_device(gfk_plan *p, const double **d_out);
 /* Copies the result (and per-frequency status) of the last execute to the host. */
 int gfk_plan_download(gfk_plan *p, double *out, int32_t *status_per_f);
-/* Number of kernel launches one execute performs. */
+/* Number of kernel launches one execute performs (after the first, which
+ * also runs the propagator tuning below). */
 int32_t gfk_plan_launches_per_execute(const gfk_plan *p);
+/* The plan's first execute times each launch shape of the Dunkin propagator
+ * (threads per block, blocks per SM, wavenumbers per thread) on a window of
+ * its own frequencies and keeps the fastest; the environment variable
+ * GFK_PROP_VARIANT=<index> forces one instead. Writes the chosen index and up
+ * to `capacity` measured times (ms); returns the number of shapes. */
+int gfk_plan_tuning(const gfk_plan *p, int32_t *variant, float *ms_per_variant, int32_t capacity);
 /* Average duration in ms of the dominant kernel (the quadrature or the
  * propagator, whichever took longer) over the executes since the last reset,
  * timed with CUDA events on the plan's stream; name receives its label. */
