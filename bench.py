@@ -236,6 +236,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--freq-stride", type=int, default=1,
                     help="profiling only: keep every n-th frequency (a smaller case of the same kernels)")
+    ap.add_argument("--quadrature", default="split", choices=["split", "fp64"],
+                    help="split: exact int8-slice tensor-core sum (default); fp64: the plain FP64 sum")
     ap.add_argument("--profile", action="store_true",
                     help="profiling only: skip the e2e leg, the FP64 peak probe and the CPU baseline")
     args = ap.parse_args()
@@ -251,7 +253,8 @@ def main():
     if args.freq_stride > 1:
         wl.freqs = wl.freqs[::args.freq_stride].copy()
     eng = gfk.Engine(local)
-    med = wl.medium(gfk.DUNKIN, engine=eng)
+    quad = gfk.PLAIN_FP64 if args.quadrature == "fp64" else gfk.SPLIT_INT8
+    med = wl.medium(gfk.DUNKIN, engine=eng, quadrature=quad)
     plan = gfk.Plan(med, wl.ranges, wl.freqs, wl.integration(), engine=eng)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -319,6 +322,29 @@ def main():
     h2d = nl * 48 + len(r) * 8 + len(f) * (8 + 8 + 8 + 4 + 8)
     d2h = len(f) * len(r) * 16 + len(f) * 4
 
+    # --- the plain FP64 path on the same bank: accuracy bar and speed ratio ---
+    plain_leg = None
+    if quad == gfk.SPLIT_INT8:
+        mp = wl.medium(gfk.DUNKIN, engine=eng)
+        pp = gfk.Plan(mp, wl.ranges, wl.freqs, wl.integration(), engine=eng)
+        for _ in range(max(args.warmup, 1)):
+            pp.execute()
+        ref, rst = pp.download()
+        rel = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        per_bin = float(np.max(np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)))
+        pp.kernel_times(reset=True)
+        for _ in range(args.steps):
+            flush.fill_(1)
+            pp.execute()
+        torch.cuda.synchronize()
+        pprop, pquad, pother = pp.kernel_times(reset=True)
+        pms = allmax(pprop + pquad + pother, world)
+        plain_leg = {"value": cells_all / (pms * 1e-3), "unit": UNIT, "ms_per_step": pms,
+                     "kernel_ms": {"propagator": pprop, "quadrature": pquad, "other": pother},
+                     "split_over_plain": (cells_all / (step_ms * 1e-3)) / (cells_all / (pms * 1e-3)),
+                     "relL2_split_vs_fp64": rel, "max_bin_relL2_split_vs_fp64": per_bin}
+        pp.close()
+
     # --- roofline of the dominant kernel --------------------------------
     peaks = measured_peaks()
     fp64_peak = fp64_gemm_peak(torch)
@@ -328,7 +354,8 @@ def main():
     if prop_ms >= quad_ms:
         dom, ach = "k_prop (Dunkin propagator)", f_prop / (prop_ms * 1e-3) / 1e12
     else:
-        dom, ach = "k_quad_gemm (FP64 wavenumber sum)", f_quad / (quad_ms * 1e-3) / 1e12
+        dom, ach = ("k_quad_gemm (FP64 wavenumber sum)" if quad == gfk.PLAIN_FP64 else
+                    "k_quad_tc (tensor-core wavenumber sum)"), f_quad / (quad_ms * 1e-3) / 1e12
     roof_time = (f_prop + f_quad) / (fp64_peak * 1e12)
     roofline = {"bound": "fp64", "kernel": dom, "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": ach / fp64_peak, "traffic": None,
@@ -338,6 +365,11 @@ def main():
                 "step_frac_of_fp64_roofline": roof_time / (step_ms * 1e-3),
                 "kernel_ms": {"propagator": prop_ms, "quadrature": quad_ms, "other": other_ms},
                 "propagator_launch_shape": {"chosen": variant, "tuning_ms": tune_ms},
+                "quadrature": {"path": "split int8 slices on tcgen05 (10 slice GEMMs)" if quad == gfk.SPLIT_INT8
+                               else "plain FP64", "ms": quad_ms,
+                               "useful_tflops": f_quad / (quad_ms * 1e-3) / 1e12,
+                               "int8_tops_executed": (10 * 2 * 2 * len(f) * len(r) * wl.samples) / (quad_ms * 1e-3) / 1e12
+                               if quad == gfk.SPLIT_INT8 else None},
                 "hbm_gbs_peak": peaks.get("hbm_gbs")}
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -347,7 +379,9 @@ def main():
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": dict(config_of(wl, "Dunkin formulation, FP64 propagators and FP64 quadrature"),
+               "config": dict(config_of(wl, "Dunkin formulation, FP64 propagators; " +
+                                        ("wavenumber sum as exact int8 slices on the tcgen05 tensor cores, FP64 "
+                                         "recombination" if quad == gfk.SPLIT_INT8 else "FP64 wavenumber sum")),
                               parallelism=f"replicas{world}" if world > 1 else "single"),
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                        "ms_per_step": e2e_s * 1e3},
@@ -355,6 +389,8 @@ def main():
                "wall_s_timed_region": wall}
         if cb:
             out["cpu_baseline"] = cb
+        if plain_leg:
+            out["plain_fp64"] = plain_leg
         print(json.dumps(out))
     plan.close()
     eng.close()

@@ -8,8 +8,21 @@ PKG = pathlib.Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libgfk.so"
-SOURCES = ["gfk_kernels.cu", "gfk_host.cu", "gfk_noalloc.cu"]
+SOURCES = ["gfk_kernels.cu", "gfk_quad_tc.cu", "gfk_host.cu", "gfk_noalloc.cu"]
 HEADERS = ["gfk_math.cuh", "gfk_solver.cuh", "gfk_kernels.cuh"]
+
+
+def cutlass_include():
+    """CuTe/CUTLASS headers (used for the UMMA descriptor bitfield definitions)."""
+    import site
+    cands = [os.environ.get("GFK_CUTLASS_INCLUDE")]
+    for sp in site.getsitepackages() + [site.getusersitepackages()]:
+        cands.append(os.path.join(sp, "flashinfer", "data", "cutlass", "include"))
+    for c in cands:
+        if c and pathlib.Path(c, "cute", "arch", "mma_sm100_desc.hpp").exists():
+            return c
+    raise RuntimeError("CuTe headers (cute/arch/mma_sm100_desc.hpp) not found; set GFK_CUTLASS_INCLUDE")
+
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -39,7 +52,7 @@ def build(force=False, verbose=False):
         return LIB
     LIB_DIR.mkdir(exist_ok=True)
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", str(tmp), *[str(CSRC / s) for s in SOURCES]]
+    cmd = [nvcc(), *NVCC_FLAGS, "-I", cutlass_include(), "-o", str(tmp), *[str(CSRC / s) for s in SOURCES]]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

@@ -207,6 +207,12 @@ struct gfk_plan {
     cd *d_wc2 = nullptr, *d_C = nullptr, *d_rem = nullptr, *d_G = nullptr;
     int* d_status = nullptr;
     int64_t rem_capacity = 0;  // complex values
+    // split (tensor-core) quadrature
+    bool tc = false;
+    int Mp = 0, Np = 0, Kp = 0, col_exp = 0;
+    int8_t *d_A = nullptr, *d_B = nullptr;
+    int* d_rowexp = nullptr;
+    unsigned long long* d_rowmax = nullptr;
     int32_t launches_per_exec = 0;
     int prop_variant = -1;  // Dunkin launch shape; -1 until the first execute tunes it
     std::vector<float> tune_ms;  // per variant, from the tuning run
@@ -225,8 +231,9 @@ const int64_t kDefaultRemBudget = int64_t(4) << 30;  // bytes of integrand per c
 void plan_free(gfk_plan* p) {
     if (!p) return;
     cudaStream_t s = p->ctx ? p->ctx->stream : nullptr;
-    void* ptrs[] = {p->d_layers, p->d_freqs, p->d_ranges, p->d_dk,  p->d_kfar, p->d_W, p->d_nk,
-                    p->d_off,    p->d_lc,    p->d_wc2,    p->d_C,   p->d_rem,  p->d_G, p->d_status};
+    void* ptrs[] = {p->d_layers, p->d_freqs, p->d_ranges, p->d_dk, p->d_kfar, p->d_W,      p->d_nk,
+                    p->d_off,    p->d_lc,    p->d_wc2,    p->d_C,  p->d_rem,  p->d_G,      p->d_status,
+                    p->d_A,      p->d_B,     p->d_rowexp, p->d_rowmax};
     for (void* q : ptrs)
         if (q) cudaFreeAsync(q, s);
     for (auto& sg : p->segs) {
@@ -304,8 +311,8 @@ int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const doub
     if (!s) return fail(ctx, GFK_EARG, "solve options missing");
     if (s->formulation != GFK_REFERENCE_DIRECT && s->formulation != GFK_DUNKIN)
         return fail(ctx, GFK_EARG, "unknown formulation %d", s->formulation);
-    if (s->quadrature != GFK_PLAIN_FP64)
-        return fail(ctx, GFK_EARG, "quadrature %d is not available in this build", s->quadrature);
+    if (s->quadrature != GFK_PLAIN_FP64 && s->quadrature != GFK_SPLIT_INT8)
+        return fail(ctx, GFK_EARG, "unknown quadrature %d", s->quadrature);
     if (s->formulation == GFK_REFERENCE_DIRECT && s->omega_imag != 0)
         return fail(ctx, GFK_EARG, "the reference formulation evaluates at real frequencies; omega_imag must be 0");
     if (!(s->omega_imag >= 0) || !std::isfinite(s->omega_imag))
@@ -391,6 +398,22 @@ int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const doub
     ctx->last_error = first_msg;
     p->total_k = total;
     p->shared = shared && g_n > 0;
+    if (s->quadrature == GFK_SPLIT_INT8) {
+        if (nf > 0 && g_n > 0 && !p->shared) {
+            std::string m = "the split quadrature needs one wavenumber grid for every frequency "
+                            "(a fixed Integration.kmax and samples)";
+            plan_free(p);
+            delete p;
+            return fail(ctx, GFK_EARG, "%s", m.c_str());
+        }
+        if (g_n > 65536) {
+            plan_free(p);
+            delete p;
+            return fail(ctx, GFK_ELIMIT, "the split quadrature's exact s32 sums allow at most 65536 wavenumbers, got %d",
+                        g_n);
+        }
+        p->tc = p->shared;
+    }
     // frequency chunks bounded by the integrand budget
     const int64_t budget = kDefaultRemBudget / (int64_t)sizeof(cd);
     int64_t acc = 0, cap = 0;
@@ -423,7 +446,22 @@ int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const doub
     if (!st) st = dalloc(ctx, &p->d_G, nfa * nr);
     if (!st) st = dalloc(ctx, &p->d_status, nfa);
     if (!st) st = dalloc(ctx, &p->d_rem, (size_t)std::max<int64_t>(cap, 1));
-    if (!st && p->shared) st = dalloc(ctx, &p->d_W, (size_t)g_n * nr);
+    if (!st && p->shared && !p->tc) st = dalloc(ctx, &p->d_W, (size_t)g_n * nr);
+    if (!st && p->tc) {
+        int max_cnf = 0;
+        for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
+            max_cnf = std::max(max_cnf, p->chunk_begin[c + 1] - p->chunk_begin[c]);
+        p->Mp = (2 * max_cnf + 127) / 128 * 128;
+        p->Np = (nr + 127) / 128 * 128;
+        p->Kp = (g_n + 63) / 64 * 64;
+        p->col_exp = gfk::tc_col_exp(g_kmax / g_n);
+        st = dalloc(ctx, &p->d_A, (size_t)4 * p->Mp * p->Kp);
+        if (!st) st = dalloc(ctx, &p->d_B, (size_t)4 * p->Np * p->Kp);
+        if (!st) st = dalloc(ctx, &p->d_rowexp, (size_t)p->Mp);
+        if (!st) st = dalloc(ctx, &p->d_rowmax, (size_t)2 * max_cnf);
+        if (!st && cudaMemsetAsync(p->d_A, 0, (size_t)4 * p->Mp * p->Kp, ctx->stream) != cudaSuccess)
+            st = fail(ctx, GFK_ECUDA, "clearing the slice planes failed");
+    }
     if (st) {
         plan_free(p);
         delete p;
@@ -456,7 +494,7 @@ int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const doub
     int nchunks = 0;
     for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
         if (p->chunk_begin[c + 1] > p->chunk_begin[c]) nchunks++;
-    p->launches_per_exec = nf > 0 ? 2 + 2 * nchunks + (p->shared ? 1 : 0) : 0;
+    p->launches_per_exec = nf > 0 ? (p->tc ? 3 + 3 * nchunks : 2 + 2 * nchunks + (p->shared ? 1 : 0)) : 0;
     *out = p;
     return GFK_OK;
 }
@@ -528,7 +566,10 @@ int plan_exec(gfk_plan* p) {
     gfk::launch_layer_consts(s, p->d_layers, medium_params(&p->med), p->d_freqs, nf, p->solve.omega_imag, p->mu_ref,
                              form, p->d_lc, p->d_wc2);
     gfk::launch_static(s, p->d_lc, p->nl, p->d_freqs, p->d_wc2, p->d_kfar, nf, p->mu_ref, form, p->d_C, p->d_status);
-    if (p->shared) gfk::launch_j0_table(s, p->d_ranges, p->nr, p->nk[0], p->dk[0], p->d_W);
+    if (p->tc)
+        gfk::launch_j0_slices(s, p->d_ranges, p->nr, p->nk[0], p->Kp, p->Np, p->dk[0], p->col_exp, p->d_B);
+    else if (p->shared)
+        gfk::launch_j0_table(s, p->d_ranges, p->nr, p->nk[0], p->dk[0], p->d_W);
     if ((st = end_seg(p, seg))) return st;
     ctx->launches += 2 + (p->shared ? 1 : 0);
     if (p->prop_variant < 0 && (st = tune_prop(p))) return st;
@@ -538,13 +579,21 @@ int plan_exec(gfk_plan* p) {
         if (cnf <= 0) continue;
         int cmax = 0;
         for (int f = fb; f < fe; f++) cmax = std::max(cmax, p->nk[f]);
+        if (p->tc) GFK_CUDA(ctx, cudaMemsetAsync(p->d_rowmax, 0, sizeof(unsigned long long) * 2 * cnf, s));
         if ((st = begin_seg(p, 0, &seg))) return st;
         gfk::launch_prop(s, p->d_lc + (size_t)fb * p->nl, p->nl, p->d_freqs + fb, p->d_wc2 + fb, cnf, p->d_nk + fb,
                          p->d_dk + fb, p->d_off + fb, cmax, p->d_C + fb, p->mu_ref, form, p->d_rem, p->d_status + fb,
-                         p->prop_variant);
+                         p->prop_variant, p->tc ? p->d_rowmax : nullptr);
         if ((st = end_seg(p, seg))) return st;
         if ((st = begin_seg(p, 1, &seg))) return st;
-        if (p->shared)
+        if (p->tc) {
+            gfk::launch_slice_rem(s, p->d_rem, p->nk[0], p->Kp, p->Mp, cnf, p->d_rowmax, p->d_rowexp, p->d_A);
+            if (gfk::launch_quad_tc(s, p->d_A, p->d_B, 2 * cnf, p->nr, p->Mp, p->Np, p->Kp, p->d_rowexp, p->col_exp,
+                                    p->d_C + fb, p->d_ranges, p->dk[0], p->d_G + (size_t)fb * p->nr,
+                                    p->d_status + fb))
+                return fail(ctx, GFK_ECUDA, "tensor-core quadrature launch setup failed");
+            ctx->launches += 1;
+        } else if (p->shared)
             gfk::launch_quad_gemm(s, p->d_rem, p->d_W, p->d_C + fb, p->d_ranges, cnf, p->nk[0], p->nr, p->dk[0],
                                   p->d_G + (size_t)fb * p->nr);
         else
@@ -576,6 +625,9 @@ int plan_download(gfk_plan* p, double* out, int32_t* status) {
             st = GFK_ESINGULAR;
             if (first == GFK_OK)
                 msg = "fk: layer propagator or surface system is singular at f=" + std::to_string(p->freqs[f]);
+        } else if (!st && (dst[f] & gfk::kStTimeout)) {
+            st = GFK_ETIMEOUT;
+            if (first == GFK_OK) msg = "a device-side wait in the tensor-core quadrature timed out";
         } else if (!st && (dst[f] & gfk::kStNonfinite)) {
             st = GFK_ENONFINITE;
             if (first == GFK_OK) msg = "fk: non-finite response at f=" + std::to_string(p->freqs[f]);

@@ -107,7 +107,8 @@ __global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict
                                                        const double* __restrict__ freqs, const cd* __restrict__ wc2,
                                                        const int* __restrict__ nk, const double* __restrict__ dk,
                                                        const int64_t* __restrict__ off, const cd* __restrict__ C,
-                                                       double mu_ref, cd* __restrict__ rem, int* __restrict__ status) {
+                                                       double mu_ref, cd* __restrict__ rem, int* __restrict__ status,
+                                                       unsigned long long* __restrict__ rowmax) {
     __shared__ LayerC s_lc[kMaxLayers];
     const int f = blockIdx.y;
     for (int l = threadIdx.x; l < nl; l += blockDim.x) s_lc[l] = lc[(size_t)f * nl + l];
@@ -116,45 +117,62 @@ __global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict
     const double d = dk[f];
     const cd c = C[f];
     const int i0 = blockIdx.x * (THREADS * ILP) + threadIdx.x + 1;
-    if (i0 > n) return;
     cd* row = rem + off[f];
     int bad = 0;
-    if (FORM == 0) {
-        bool ok;
-        const double k = (double)i0 * d;
-        cd u = direct_u(s_lc, nl, kTwoPi * freqs[f], k, mu_ref, ok);
-        if (!ok) bad |= kStSingular;
-        cd r = k * u - c;
-        if (!finite_cd(r)) { bad |= kStNonfinite; r = mk(0.0); }
-        row[i0 - 1] = r;
-    } else if (ILP == 1) {
-        const double k = (double)i0 * d;
-        cd r = k * dunkin_u(s_lc, nl, wc2[f], k, mu_ref) - c;
-        if (!finite_cd(r)) { bad |= kStNonfinite; r = mk(0.0); }
-        row[i0 - 1] = r;
-    } else {
-        const int i1 = i0 + THREADS;
-        const bool has1 = i1 <= n;
-        const double k0 = (double)i0 * d;
-        const double k1 = has1 ? (double)i1 * d : k0;
-        cd u0, u1;
-        dunkin_u2(s_lc, nl, wc2[f], k0, k1, mu_ref, u0, u1);
-        cd r0 = k0 * u0 - c;
-        if (!finite_cd(r0)) { bad |= kStNonfinite; r0 = mk(0.0); }
-        row[i0 - 1] = r0;
-        if (has1) {
-            cd r1 = k1 * u1 - c;
-            if (!finite_cd(r1)) { bad |= kStNonfinite; r1 = mk(0.0); }
-            row[i1 - 1] = r1;
+    double mre = 0.0, mim = 0.0;
+    if (i0 <= n) {
+        if (FORM == 0) {
+            bool ok;
+            const double k = (double)i0 * d;
+            cd u = direct_u(s_lc, nl, kTwoPi * freqs[f], k, mu_ref, ok);
+            if (!ok) bad |= kStSingular;
+            cd r = k * u - c;
+            if (!finite_cd(r)) { bad |= kStNonfinite; r = mk(0.0); }
+            row[i0 - 1] = r;
+            mre = fabs(r.re); mim = fabs(r.im);
+        } else if (ILP == 1) {
+            const double k = (double)i0 * d;
+            cd r = k * dunkin_u(s_lc, nl, wc2[f], k, mu_ref) - c;
+            if (!finite_cd(r)) { bad |= kStNonfinite; r = mk(0.0); }
+            row[i0 - 1] = r;
+            mre = fabs(r.re); mim = fabs(r.im);
+        } else {
+            const int i1 = i0 + THREADS;
+            const bool has1 = i1 <= n;
+            const double k0 = (double)i0 * d;
+            const double k1 = has1 ? (double)i1 * d : k0;
+            cd u0, u1;
+            dunkin_u2(s_lc, nl, wc2[f], k0, k1, mu_ref, u0, u1);
+            cd r0 = k0 * u0 - c;
+            if (!finite_cd(r0)) { bad |= kStNonfinite; r0 = mk(0.0); }
+            row[i0 - 1] = r0;
+            mre = fabs(r0.re); mim = fabs(r0.im);
+            if (has1) {
+                cd r1 = k1 * u1 - c;
+                if (!finite_cd(r1)) { bad |= kStNonfinite; r1 = mk(0.0); }
+                row[i1 - 1] = r1;
+                mre = fmax(mre, fabs(r1.re)); mim = fmax(mim, fabs(r1.im));
+            }
+        }
+        if (bad) atomicOr(status + f, bad);
+    }
+    if (rowmax) {  // per-row maxima for the integer slicing of the tensor-core sum
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mre = fmax(mre, __shfl_xor_sync(0xffffffffu, mre, o));
+            mim = fmax(mim, __shfl_xor_sync(0xffffffffu, mim, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMax(rowmax + 2 * f, (unsigned long long)__double_as_longlong(mre));
+            atomicMax(rowmax + 2 * f + 1, (unsigned long long)__double_as_longlong(mim));
         }
     }
-    if (bad) atomicOr(status + f, bad);
 }
 
 namespace {
 struct PropVariant {
     void (*fn)(const LayerC*, int, const double*, const cd*, const int*, const double*, const int64_t*, const cd*,
-               double, cd*, int*);
+               double, cd*, int*, unsigned long long*);
     int threads, ilp;
 };
 const PropVariant kDunkinVariants[] = {
@@ -171,18 +189,18 @@ int prop_variant_count() { return (int)(sizeof(kDunkinVariants) / sizeof(kDunkin
 
 void launch_prop(cudaStream_t s, const LayerC* lc, int nl, const double* freqs, const cd* wc2, int nf,
                  const int* nk, const double* dk, const int64_t* off, int max_nk, const cd* C, double mu_ref,
-                 int formulation, cd* rem, int* status, int variant) {
+                 int formulation, cd* rem, int* status, int variant, unsigned long long* rowmax) {
     if (nf <= 0 || max_nk <= 0) return;
     if (formulation == 0) {
         dim3 grid((max_nk + 127) / 128, nf);
-        k_prop<0, 128, 1, 1><<<grid, 128, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status);
+        k_prop<0, 128, 1, 1><<<grid, 128, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status, rowmax);
         return;
     }
     if (variant < 0 || variant >= prop_variant_count()) variant = 0;
     const PropVariant& v = kDunkinVariants[variant];
     const int per_block = v.threads * v.ilp;
     dim3 grid((max_nk + per_block - 1) / per_block, nf);
-    v.fn<<<grid, v.threads, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status);
+    v.fn<<<grid, v.threads, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status, rowmax);
 }
 
 // -------------------------------------------------------------- J0 table --

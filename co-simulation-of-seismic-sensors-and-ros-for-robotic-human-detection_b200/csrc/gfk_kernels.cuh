@@ -6,7 +6,7 @@
 namespace gfk {
 
 // Device status bits, mapped to gfk_status by the host.
-enum : int { kStSingular = 1, kStNonfinite = 2 };
+enum : int { kStSingular = 1, kStNonfinite = 2, kStTimeout = 4 };
 
 void launch_layer_consts(cudaStream_t s, const LayerP* layers, MediumP med, const double* freqs, int nf,
                          double wi, double mu_ref, int formulation, LayerC* lc, cd* wc2);
@@ -18,8 +18,20 @@ void launch_static(cudaStream_t s, const LayerC* lc, int nl, const double* freqs
 // `variant` picks one of prop_variant_count() launch shapes of the Dunkin kernel.
 void launch_prop(cudaStream_t s, const LayerC* lc, int nl, const double* freqs, const cd* wc2, int nf,
                  const int* nk, const double* dk, const int64_t* off, int max_nk, const cd* C,
-                 double mu_ref, int formulation, cd* rem, int* status, int variant = 0);
+                 double mu_ref, int formulation, cd* rem, int* status, int variant = 0,
+                 unsigned long long* rowmax = nullptr);
 int prop_variant_count();
+
+// Tensor-core quadrature (gfk_quad_tc.cu): exact int8 slices of the integrand
+// rows and of the Hankel weights, tcgen05 kind::i8 GEMM, FP64 recombination.
+// rowmax[2f + p] holds the bits of max_k |part p of rem[f][k]| (set by launch_prop).
+int tc_col_exp(double dk);
+void launch_j0_slices(cudaStream_t s, const double* ranges, int nr, int nk, int Kp, int Np, double dk, int col_exp,
+                      int8_t* B);
+void launch_slice_rem(cudaStream_t s, const cd* rem, int nk, int Kp, int Mp, int nf, const unsigned long long* rowmax,
+                      int* row_exp, int8_t* A);
+int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int N, int Mp, int Np, int Kp,
+                   const int* row_exp, int col_exp, const cd* C, const double* ranges, double dk, cd* G, int* status);
 
 // W[(i-1) nr + j] = w_i J0(k_i r_j) dk, w = 1/2 at i = nk.
 void launch_j0_table(cudaStream_t s, const double* ranges, int nr, int nk, double dk, double* W);

@@ -1,0 +1,449 @@
+// gfk_quad_tc.cu — the shared-grid wavenumber sum on the tcgen05 tensor cores.
+//
+// G[f][r] = head + sum_k REM[f][k] W[k][r] is a complex-by-real GEMM
+// (M = 2 nf real rows, N = nr ranges, K = nk wavenumbers). The sum cancels
+// heavily (|G| is 40-400x below sum |terms| typically, 1e5x at worst on the
+// graded-soil workload), so it needs ~28 significant bits end to end. It is
+// computed with exact integer slices (the Ozaki splitting): each operand row
+// (REM) / column (W) is scaled by a power of two into (-1, 1) and written as
+// four signed 7-bit digits,
+//     a = 2^e_a sum_s a_s 2^-7(s+1),   b = 2^e_b sum_t b_t 2^-7(t+1),
+// the ten digit products with s + t <= 3 run as int8 x int8 -> s32 tensor-core
+// MMAs (tcgen05.mma kind::i8), accumulated EXACTLY in TMEM per level s + t, and
+// the four level sums are recombined in FP64 in the epilogue:
+//     sum_k a b = 2^(e_a+e_b) sum_l acc_l 2^-7(l+2) + O(2^-28) relative.
+// No FP32 rounding enters, so no compensated summation is needed.
+//
+// Kernel shape: one CTA per 128 x 128 output tile, 6 warps:
+//   warp 0  TMA producer (one lane): per 64-byte K block, 4 A-slice and 4
+//           B-slice tiles (SWIZZLE_64B, 8 KB each) into a 3-stage ring;
+//   warp 1  allocates 512 TMEM columns (4 levels x 128 s32 columns) and one
+//           lane issues the MMAs (M = 128, N = 128, K = 32 per instruction);
+//   warps 2-5 epilogue: tcgen05.ld the 4 levels, recombine, add the static
+//           head term, write FP64.
+// Every mbarrier wait is bounded (~1 s of SM clock); a timeout sets a status
+// bit, stops issuing, drains what is in flight and frees TMEM before exit.
+// No TMA multicast is used anywhere.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cute/arch/mma_sm100_desc.hpp>
+
+#include "gfk_kernels.cuh"
+
+namespace gfk {
+namespace tc {
+
+constexpr int BM = 128, BN = 128, BK = 64;  // BK in int8 elements (bytes)
+constexpr int S = 4;                        // slices per operand
+constexpr int STAGES = 3;
+constexpr int TILE = BM * BK;               // 8192 bytes, A and B tiles alike
+constexpr int STAGE_BYTES = 2 * S * TILE;   // 65536
+constexpr int TMEM_COLS = S * BN;           // 512: one 128-column s32 accumulator per level
+constexpr int THREADS = 192;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr long long kWaitCycles = 1LL << 31;  // bound on any single wait
+
+static_assert(BN == BM, "A and B tiles share one size");
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase of the given parity to complete; false after ~1 s.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+    if (mbar_try_wait(b, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(b, parity))
+        if (clock64() - t0 > kWaitCycles) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(addr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: K-major operand, 64-byte rows written by
+// TMA with SWIZZLE_64B, 8-row groups 512 bytes apart (SBO), Blackwell
+// descriptor version 1. Field layout from cute::UMMA::SmemDescriptor.
+__device__ __forceinline__ uint64_t sdesc_k_sw64(uint32_t saddr) {
+    cute::UMMA::SmemDescriptor d;
+    d.desc_ = 0;
+    d.start_address_ = static_cast<uint16_t>(saddr >> 4);
+    d.leading_byte_offset_ = 1;
+    d.stride_byte_offset_ = 512 >> 4;
+    d.version_ = 1;
+    d.base_offset_ = 0;
+    d.lbo_mode_ = 0;
+    d.layout_type_ = static_cast<uint8_t>(cute::UMMA::LayoutType::SWIZZLE_64B);
+    return d.desc_;
+}
+
+// Instruction descriptor: s8 x s8 -> s32, both K-major, M = 128, N = 128.
+__host__ __device__ inline uint32_t idesc_i8_128x128() {
+    cute::UMMA::InstrDescriptor id;
+    id.desc_ = 0;
+    id.c_format_ = 2;  // S32
+    id.a_format_ = 1;  // signed 8-bit
+    id.b_format_ = 1;
+    id.a_major_ = 0;   // K-major
+    id.b_major_ = 0;
+    id.n_dim_ = BN >> 3;
+    id.m_dim_ = BM >> 4;
+    return id.desc_;
+}
+
+struct Args {
+    int M, N;           // valid real rows (2 nf) and ranges
+    int Mp, Np, Kp;     // padded extents of the slice planes
+    const int* row_exp; // [M] power-of-two exponent of each real row
+    int col_exp;        // exponent shared by every W column
+    const cd* C;        // [nf] static coefficients
+    const double* ranges;
+    double dk;
+    cd* G;              // [nf][N]
+    int* status;        // [nf] status bits
+};
+
+__global__ void __launch_bounds__(THREADS, 1)
+    k_quad_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Args a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* accf = empty + STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int nkb = a.Kp / BK;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < STAGES; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(accf, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int issued = 0;
+            for (int kb = 0; kb < nkb; kb++) {
+                const int st = kb % STAGES;
+                const uint32_t ph = (kb / STAGES) & 1;
+                if (!mbar_wait(&empty[st], ph ^ 1)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                if (*(volatile int*)abort_flag) break;
+                mbar_expect_tx(&full[st], STAGE_BYTES);
+                uint8_t* base = smem + st * STAGE_BYTES;
+#pragma unroll
+                for (int s = 0; s < S; s++) tma_load_2d(base + s * TILE, &tmA, &full[st], kb * BK, s * a.Mp + m0);
+#pragma unroll
+                for (int t = 0; t < S; t++)
+                    tma_load_2d(base + (S + t) * TILE, &tmB, &full[st], kb * BK, t * a.Np + n0);
+                issued = kb + 1;
+            }
+            // drain: the last loads of each stage land before the CTA may exit
+            for (int kb = issued - 1; kb >= 0 && kb >= issued - STAGES; kb--)
+                if (!mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1)) *abort_flag = 1;
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = idesc_i8_128x128();
+            bool init[S] = {false, false, false, false};
+            for (int kb = 0; kb < nkb; kb++) {
+                const int st = kb % STAGES;
+                if (!mbar_wait(&full[st], (kb / STAGES) & 1)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                if (*(volatile int*)abort_flag) break;
+                tc_fence_after();
+                const uint32_t base = smem_u32(smem + st * STAGE_BYTES);
+#pragma unroll
+                for (int lvl = 0; lvl < S; lvl++) {
+#pragma unroll
+                    for (int s = 0; s <= lvl; s++) {
+                        const int t = lvl - s;
+#pragma unroll
+                        for (int kk = 0; kk < BK / 32; kk++) {
+                            const uint64_t da = sdesc_k_sw64(base + s * TILE + kk * 32);
+                            const uint64_t db = sdesc_k_sw64(base + (S + t) * TILE + kk * 32);
+                            tc_mma_i8(tmem + lvl * BN, da, db, idesc, init[lvl] ? 1u : 0u);
+                            init[lvl] = true;
+                        }
+                    }
+                }
+                tc_commit(&empty[st]);  // frees the stage once these MMAs have read it
+            }
+            tc_commit(accf);  // arrives when every MMA issued above has completed
+        }
+    } else {
+        // epilogue: warps 2..5 cover TMEM lane quarters 2, 3, 0, 1
+        const bool ok = mbar_wait(accf, 0);
+        tc_fence_after();
+        const int q = warp & 3;
+        const int row = m0 + q * 32 + lane;
+        const bool row_ok = ok && row < a.M && !*(volatile int*)abort_flag;
+        const int f = row >> 1, part = row & 1;
+        double rscale = 0.0;
+        cd c = mk(0.0);
+        if (row_ok) {
+            rscale = ldexp(1.0, a.row_exp[row] + a.col_exp);
+            c = a.C[f];
+        }
+        const double cpart = part ? c.im : c.re;
+#pragma unroll 1
+        for (int j = 0; j < BN / 32; j++) {
+            uint32_t v0[32], v1[32], v2[32], v3[32];
+            const uint32_t lane_addr = tmem + (static_cast<uint32_t>(q * 32) << 16) + j * 32;
+            tmem_ld32(lane_addr + 0 * BN, v0);
+            tmem_ld32(lane_addr + 1 * BN, v1);
+            tmem_ld32(lane_addr + 2 * BN, v2);
+            tmem_ld32(lane_addr + 3 * BN, v3);
+            tmem_wait_ld();
+            if (row_ok) {
+#pragma unroll
+                for (int cc = 0; cc < 32; cc++) {
+                    const int n = n0 + j * 32 + cc;
+                    if (n < a.N) {
+                        const double acc = (double)(int)v0[cc] * 0x1p-14 + (double)(int)v1[cc] * 0x1p-21 +
+                                           (double)(int)v2[cc] * 0x1p-28 + (double)(int)v3[cc] * 0x1p-35;
+                        const double head = cpart / a.ranges[n] - (0.5 * a.dk) * cpart;  // fk.go:529-532
+                        double* out = reinterpret_cast<double*>(a.G + (size_t)f * a.N + n);
+                        out[part] = head + acc * rscale;
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (threadIdx.x == 0 && *(volatile int*)abort_flag) {
+        const int r0 = m0 >> 1;
+        for (int f = r0; f < r0 + BM / 2 && 2 * f < a.M; f++) atomicOr(a.status + f, kStTimeout);
+    }
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+}
+
+// ------------------------------------------------------------- slicing --
+
+// Four signed 7-bit digits of x in (-1, 1) scaled by 128: x*128 = d0 + d1/128 + ...
+__device__ __forceinline__ void digits4(double x128, int8_t d[4]) {
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        const double q = rint(x128);
+        d[s] = static_cast<int8_t>(q);
+        x128 = (x128 - q) * 128.0;
+    }
+}
+
+// Integrand rows: rows 2f (re) and 2f+1 (im) of the A slice planes [4][Mp][Kp].
+// 16 consecutive wavenumbers per thread, one 16-byte store per slice and part.
+__global__ void k_slice_rem(const cd* __restrict__ rem, int nk, int Kp, int Mp, int nf,
+                            const unsigned long long* __restrict__ rowmax, int* __restrict__ row_exp,
+                            int8_t* __restrict__ A) {
+    const int f = blockIdx.y;
+    const int k0 = (blockIdx.x * blockDim.x + threadIdx.x) * 16;
+    if (f >= nf || k0 >= Kp) return;
+    int e[2];
+    double sc[2];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        const double mx = __longlong_as_double((long long)rowmax[2 * f + p]);
+        e[p] = mx > 0 ? ilogb(mx * (128.0 / 127.0)) + 1 : 0;  // 2^e >= mx*128/127
+        sc[p] = ldexp(128.0, -e[p]);
+    }
+    if (k0 == 0 && threadIdx.x == 0) {
+        row_exp[2 * f] = e[0];
+        row_exp[2 * f + 1] = e[1];
+    }
+    alignas(16) int8_t out[2][4][16];
+#pragma unroll 4
+    for (int i = 0; i < 16; i++) {
+        const int k = k0 + i;
+        const cd v = k < nk ? rem[(size_t)f * nk + k] : mk(0.0);
+        int8_t d[4];
+        digits4(v.re * sc[0], d);
+#pragma unroll
+        for (int s = 0; s < 4; s++) out[0][s][i] = d[s];
+        digits4(v.im * sc[1], d);
+#pragma unroll
+        for (int s = 0; s < 4; s++) out[1][s][i] = d[s];
+    }
+#pragma unroll
+    for (int p = 0; p < 2; p++)
+#pragma unroll
+        for (int s = 0; s < 4; s++)
+            *reinterpret_cast<int4*>(A + ((size_t)s * Mp + 2 * f + p) * Kp + k0) =
+                *reinterpret_cast<const int4*>(out[p][s]);
+}
+
+// Hankel weights w_i J0(k_i r_j) dk (fk.go:540-546), transposed to [range][k]
+// and sliced with the shared column exponent: |w J0 dk| <= dk always.
+__global__ void k_j0_slices(const double* __restrict__ ranges, int nr, int nk, int Kp, int Np, double dk,
+                            int col_exp, int8_t* __restrict__ B) {
+    const int n = blockIdx.y;
+    const int k0 = (blockIdx.x * blockDim.x + threadIdx.x) * 16;
+    if (n >= Np || k0 >= Kp) return;
+    const double sc = ldexp(128.0, -col_exp);
+    const double r = n < nr ? ranges[n] : 0.0;
+    alignas(16) int8_t out[4][16];
+#pragma unroll 4
+    for (int q = 0; q < 16; q++) {
+        const int i = k0 + q + 1;  // wavenumber index, k_i = i dk
+        double wv = 0.0;
+        if (n < nr && i <= nk) {
+            const double k = (double)i * dk;
+            const double w = i == nk ? 0.5 : 1.0;
+            wv = (w * j0(k * r)) * dk;
+        }
+        int8_t d[4];
+        digits4(wv * sc, d);
+#pragma unroll
+        for (int s = 0; s < 4; s++) out[s][q] = d[s];
+    }
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+        *reinterpret_cast<int4*>(B + ((size_t)s * Np + n) * Kp + k0) = *reinterpret_cast<const int4*>(out[s]);
+}
+
+}  // namespace tc
+
+// ------------------------------------------------------------------ host --
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// A [planes*rows_p][Kp] int8 plane stack; box = 128 rows x 64 bytes, SWIZZLE_64B.
+bool make_map(CUtensorMap* map, const int8_t* base, int rows_total, int Kp) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows_total};
+    cuuint64_t strides[1] = {(cuuint64_t)Kp};
+    cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)tc::BM};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+}  // namespace
+
+int tc_col_exp(double dk) { return ilogb(dk * (128.0 / 127.0)) + 1; }
+
+void launch_j0_slices(cudaStream_t s, const double* ranges, int nr, int nk, int Kp, int Np, double dk, int col_exp,
+                      int8_t* B) {
+    dim3 grid((Kp / 16 + 127) / 128, Np);
+    tc::k_j0_slices<<<grid, 128, 0, s>>>(ranges, nr, nk, Kp, Np, dk, col_exp, B);
+}
+
+void launch_slice_rem(cudaStream_t s, const cd* rem, int nk, int Kp, int Mp, int nf, const unsigned long long* rowmax,
+                      int* row_exp, int8_t* A) {
+    dim3 grid((Kp / 16 + 127) / 128, nf);
+    tc::k_slice_rem<<<grid, 128, 0, s>>>(rem, nk, Kp, Mp, nf, rowmax, row_exp, A);
+}
+
+int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int N, int Mp, int Np, int Kp,
+                   const int* row_exp, int col_exp, const cd* C, const double* ranges, double dk, cd* G, int* status) {
+    if (Mp % tc::BM || Np % tc::BN || Kp % tc::BK || M > Mp || N > Np) return 1;
+    CUtensorMap ta, tb;
+    if (!make_map(&ta, A, tc::S * Mp, Kp) || !make_map(&tb, B, tc::S * Np, Kp)) return 2;
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(tc::k_quad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES) !=
+            cudaSuccess)
+            return 3;
+        attr_set = true;
+    }
+    tc::Args a{M, N, Mp, Np, Kp, row_exp, col_exp, C, ranges, dk, G, status};
+    dim3 grid(Np / tc::BN, Mp / tc::BM);
+    tc::k_quad_tc<<<grid, tc::THREADS, tc::SMEM_BYTES, s>>>(ta, tb, a);
+    return 0;
+}
+
+}  // namespace gfk

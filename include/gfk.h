@@ -61,8 +61,13 @@ enum gfk_formulation {
 
 enum gfk_quadrature {
     GFK_PLAIN_FP64 = 0,    /* FP64 wavenumber sum on the FP64 pipe */
-    GFK_SPLIT_INT8 = 1     /* shared-grid sum as an exact-integer-sliced tensor-core GEMM
-                              (tcgen05 kind::i8, s32 accumulate), FP64 recombination */
+    GFK_SPLIT_INT8 = 1     /* shared-grid sum as an exact-integer-sliced tensor-core GEMM:
+                              each integrand row and Hankel-weight column is scaled by a
+                              power of two and cut into four signed 7-bit digits; the ten
+                              digit products of weight >= 2^-28 run as tcgen05 kind::i8
+                              MMAs with exact s32 accumulation and are recombined in FP64.
+                              Needs one wavenumber grid for all frequencies, <= 65536
+                              wavenumbers. */
 };
 
 /* ---- medium --------------------------------------------------------------- */

@@ -241,3 +241,43 @@ def test_build_and_write_bank(gfk, engine, tmp_path):
     assert np.array_equal(r.data, b.data)
     assert (r.data[:, 0] == 0).all() and (r.data[:, top + 1:] == 0).all()
     assert np.array_equal(r.data[:, 1:top + 1, 0], spectra.T.real.astype(np.float32))
+
+
+@pytest.mark.parametrize("name", ["single_soil", "graded_soil"])
+def test_split_quadrature_against_fp64(gfk, engine, name):
+    """The tensor-core (exact int8 slice) wavenumber sum against the FP64 one on
+    the same integrand: rel-L2 <= 1e-6 over the whole bank, the bar the
+    split-precision path is held to."""
+    wl = getattr(gfk.workloads, name)()
+    plain = wl.medium(gfk.DUNKIN, engine=engine)
+    split = wl.medium(gfk.DUNKIN, engine=engine, quadrature=gfk.SPLIT_INT8)
+    a, sa = plain.bank_spectra(wl.ranges, wl.freqs, wl.integration())
+    b, sb = split.bank_spectra(wl.ranges, wl.freqs, wl.integration())
+    assert (sa == 0).all() and (sb == 0).all()
+    rel = rel_l2(b, a)
+    assert rel < 1e-6, rel
+    # every bin, not just the aggregate
+    per_bin = np.linalg.norm(b - a, axis=1) / np.linalg.norm(a, axis=1)
+    assert per_bin.max() < 1e-5, per_bin.max()
+
+
+def test_split_quadrature_ragged_shapes(gfk, engine, oracle):
+    """Sizes that are not multiples of the 128 x 128 x 64 tiles."""
+    wl = gfk.workloads.single_soil()
+    ranges = wl.ranges[:45] * 1.5
+    freqs = wl.freqs[3:70:2]
+    opt = gfk.Integration(1000, 0.0, wl.kmax)
+    split = wl.medium(gfk.DUNKIN, engine=engine, quadrature=gfk.SPLIT_INT8)
+    got, st = split.bank_spectra(ranges, freqs, opt)
+    assert (st == 0).all()
+    want, ost = oracle.bank_spectra(as_tuples(wl.stack), ranges, freqs, samples=1000, kmax=wl.kmax,
+                                    formulation=oracle.DUNKIN, omega_imag=wl.omega_imag)
+    assert rel_l2(got, want) < 1e-6
+
+
+def test_split_quadrature_refuses_per_frequency_grids(gfk, engine):
+    m = gfk.Medium(gfk.uniform(500, 200, 1700, 25), formulation=gfk.DUNKIN, quadrature=gfk.SPLIT_INT8,
+                   engine=engine)
+    with pytest.raises(gfk.FkError) as e:
+        m.bank_spectra([1.0, 2.0], [10.0, 20.0])
+    assert e.value.status == gfk._native.EARG
