@@ -24,6 +24,11 @@ struct gfk_ctx {
     std::string last_error;
     int64_t launches = 0;
     std::vector<gfk_plan*> plans;  // live plans, destroyed by gfk_close
+    // propagator launch shape chosen by tuning, per (layer count, wavenumber count)
+    struct Tuned {
+        int nl, nk, variant;
+    };
+    std::vector<Tuned> tuned;
 };
 
 namespace {
@@ -512,6 +517,11 @@ int tune_prop(gfk_plan* p) {
         return GFK_OK;
     }
     if (p->solve.formulation != GFK_DUNKIN || p->nf == 0) return GFK_OK;
+    for (const auto& t : ctx->tuned)
+        if (t.nl == p->nl && t.nk == p->max_nk) {
+            p->prop_variant = t.variant;
+            return GFK_OK;
+        }
     const int c0 = p->chunk_begin[0], c1 = p->chunk_begin[1];
     const int win = std::min(64, c1 - c0);
     if (win <= 0) return GFK_OK;
@@ -547,6 +557,7 @@ int tune_prop(gfk_plan* p) {
     for (int v = 1; v < nv; v++)
         if (p->tune_ms[v] < p->tune_ms[best]) best = v;
     p->prop_variant = best;
+    ctx->tuned.push_back({p->nl, p->max_nk, best});
     return GFK_OK;
 }
 

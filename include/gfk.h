@@ -198,8 +198,9 @@ int gfk_plan_download(gfk_plan *p, double *out, int32_t *status_per_f);
 int32_t gfk_plan_launches_per_execute(const gfk_plan *p);
 /* The plan's first execute times each launch shape of the Dunkin propagator
  * (threads per block, blocks per SM, wavenumbers per thread) on a window of
- * its own frequencies and keeps the fastest; the environment variable
- * GFK_PROP_VARIANT=<index> forces one instead. Writes the chosen index and up
+ * its own frequencies and keeps the fastest; the context remembers the choice
+ * per (layer count, wavenumber count) for later plans and calls. The
+ * environment variable GFK_PROP_VARIANT=<index> forces one instead. Writes the chosen index and up
  * to `capacity` measured times (ms); returns the number of shapes. */
 int gfk_plan_tuning(const gfk_plan *p, int32_t *variant, float *ms_per_variant, int32_t capacity);
 /* Average duration in ms of the dominant kernel (the quadrature or the
