@@ -6,11 +6,11 @@ in include/gfk.h). There is no CPU fallback.
 """
 from . import _native
 from ._native import DUNKIN, PLAIN_FP64, REFERENCE_DIRECT, SPLIT_INT8
-from .fk import (Engine, FkError, Grid, Integration, Layer, MAX_LAYER_PHASE, Medium, Plan, SLS, Stack,
+from .fk import (Batch, Engine, FkError, Grid, Integration, Layer, MAX_LAYER_PHASE, Medium, Plan, SLS, Stack,
                  default_engine, uniform)
 from .bank import (Bank, Header, Provenance, RangeGrid, build_bank, open_bank, range_nyquist)
 from . import workloads
 
-__all__ = ["Engine", "FkError", "Grid", "Integration", "Layer", "MAX_LAYER_PHASE", "Medium", "Plan", "SLS",
+__all__ = ["Batch", "Engine", "FkError", "Grid", "Integration", "Layer", "MAX_LAYER_PHASE", "Medium", "Plan", "SLS",
            "Stack", "default_engine", "uniform", "Bank", "Header", "Provenance", "RangeGrid", "build_bank",
            "open_bank", "range_nyquist", "workloads", "DUNKIN", "REFERENCE_DIRECT", "PLAIN_FP64", "SPLIT_INT8"]

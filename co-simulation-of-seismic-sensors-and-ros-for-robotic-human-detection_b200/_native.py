@@ -27,6 +27,7 @@ EXPORTS = [
     "gfk_vertical_displacement_multi", "gfk_bank_spectra",
     "gfk_plan_create", "gfk_plan_execute", "gfk_plan_result_device", "gfk_plan_download",
     "gfk_plan_launches_per_execute", "gfk_plan_tuning", "gfk_plan_kernel_times", "gfk_plan_destroy",
+    "gfk_plan_use_graph", "gfk_batch_create",
     "gfk_bank_pack", "gfk_bank_write", "gfk_vertical_displacement_multi_noalloc",
 ]
 
@@ -95,6 +96,9 @@ def lib():
         "gfk_plan_tuning": (ctypes.c_int, [vp, P(i32), P(ctypes.c_float), i32]),
         "gfk_plan_kernel_times": (ctypes.c_int, [vp, P(d), P(d), P(d), i32]),
         "gfk_plan_destroy": (ctypes.c_int, [vp]),
+        "gfk_plan_use_graph": (ctypes.c_int, [vp, i32]),
+        "gfk_batch_create": (ctypes.c_int, [vp, P(GfkMedium), i32, P(P(d)), P(i32), P(GfkSolve), P(d), i32,
+                                            GfkIntegration, P(vp)]),
         "gfk_bank_pack": (ctypes.c_int, [P(d), i32, i32, i32, i32, P(ctypes.c_float)]),
         "gfk_bank_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, P(ctypes.c_float), i64]),
         "gfk_vertical_displacement_multi_noalloc": (ctypes.c_int, [P(GfkMedium), P(GfkSolve), P(d), i32, d,

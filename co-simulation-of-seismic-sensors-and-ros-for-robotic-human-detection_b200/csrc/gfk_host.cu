@@ -164,7 +164,7 @@ int grid_for(gfk_ctx* ctx, const gfk_medium* m, const double* ranges, int nr, do
 }
 
 gfk::MediumP medium_params(const gfk_medium* m) {
-    gfk::MediumP p;
+    gfk::MediumP p{};
     p.ref_freq = m->ref_freq_hz;
     p.default_q = m->default_q;
     p.tau_sigma = m->sls_tau_sigma;
@@ -177,41 +177,45 @@ gfk::MediumP medium_params(const gfk_medium* m) {
 }  // namespace
 
 // ---------------------------------------------------------------- plans --
+//
+// A plan is a fixed set of bank rows — (medium, frequency) pairs, one or many
+// media — over one range list, with its device buffers. Rows are ordered
+// medium by medium, each medium's frequencies in the caller's order.
 
 // How a plan sets its wavenumber grid per frequency.
 enum GridMode { kGridMulti = 0, kGridSingle = 1 };
 
 struct TimedSeg {
-    int kind;  // 0 prop, 1 quad, 2 other
+    int kind;  // 0 prop, 1 quad, 2 other, 3 whole graph
     cudaEvent_t a, b;
     bool pending;
 };
 
 struct gfk_plan {
     gfk_ctx* ctx = nullptr;
-    std::vector<gfk_layer> layers;
-    gfk_medium med{};
     gfk_solve solve{};
-    std::vector<double> ranges, freqs;
-    std::vector<int32_t> host_status;  // per f, set on the host (guard, args)
-    std::vector<int> nk;
-    std::vector<double> dk, kfar;
-    std::vector<int64_t> off;
+    std::vector<double> ranges;
+    int nsoil = 0, nf = 0, nr = 0, max_nk = 0, max_nl = 0;
+    // host tables
+    std::vector<gfk::LayerP> lp;
+    std::vector<gfk::MediumP> media;
+    std::vector<gfk::FreqDesc> fd;  // integrand offsets relative to each row's chunk
+    std::vector<double> freqs;
+    std::vector<int32_t> host_status;  // per row, set on the host (guard, arguments, stack)
     bool shared = false;
-    double mu_ref = 0;
-    int nf = 0, nr = 0, nl = 0, max_nk = 0;
-    int64_t total_k = 0;
-    // chunks over frequency: [f_begin, f_end) with REM offset base
-    std::vector<int> chunk_begin;
+    double g_kmax = 0;
+    int g_n = 0;
+    std::vector<int> chunk_begin;  // row chunks [chunk_begin[c], chunk_begin[c+1])
+    std::vector<int> chunk_max_nk;
+    int64_t rem_capacity = 0;  // complex values
     // device
-    gfk::LayerP* d_layers = nullptr;
-    double *d_freqs = nullptr, *d_ranges = nullptr, *d_dk = nullptr, *d_kfar = nullptr, *d_W = nullptr;
-    int* d_nk = nullptr;
-    int64_t* d_off = nullptr;
+    gfk::LayerP* d_lp = nullptr;
+    gfk::MediumP* d_media = nullptr;
+    gfk::FreqDesc* d_fd = nullptr;
+    double *d_ranges = nullptr, *d_W = nullptr;
     gfk::LayerC* d_lc = nullptr;
     cd *d_wc2 = nullptr, *d_C = nullptr, *d_rem = nullptr, *d_G = nullptr;
     int* d_status = nullptr;
-    int64_t rem_capacity = 0;  // complex values
     // split (tensor-core) quadrature
     bool tc = false;
     int Mp = 0, Np = 0, Kp = 0, col_exp = 0;
@@ -219,12 +223,15 @@ struct gfk_plan {
     int* d_rowexp = nullptr;
     unsigned long long* d_rowmax = nullptr;
     int32_t launches_per_exec = 0;
-    int prop_variant = -1;  // Dunkin launch shape; -1 until the first execute tunes it
+    int prop_variant = -1;       // Dunkin launch shape; -1 until the first execute tunes it
     std::vector<float> tune_ms;  // per variant, from the tuning run
+    // CUDA graph of one whole execute
+    bool use_graph = false;
+    cudaGraphExec_t gexec = nullptr;
     // timing
     std::vector<TimedSeg> segs;
     size_t seg_next = 0;
-    double acc_ms[3] = {0, 0, 0};
+    double acc_ms[4] = {0, 0, 0, 0};
     int acc_execs = 0;
     bool executed = false;
 };
@@ -232,13 +239,15 @@ struct gfk_plan {
 namespace {
 
 const int64_t kDefaultRemBudget = int64_t(4) << 30;  // bytes of integrand per chunk
+const int kMaxChunkRows = 65535;                       // grid.y of the per-row kernels
 
 void plan_free(gfk_plan* p) {
     if (!p) return;
     cudaStream_t s = p->ctx ? p->ctx->stream : nullptr;
-    void* ptrs[] = {p->d_layers, p->d_freqs, p->d_ranges, p->d_dk, p->d_kfar, p->d_W,      p->d_nk,
-                    p->d_off,    p->d_lc,    p->d_wc2,    p->d_C,  p->d_rem,  p->d_G,      p->d_status,
-                    p->d_A,      p->d_B,     p->d_rowexp, p->d_rowmax};
+    if (p->gexec) cudaGraphExecDestroy(p->gexec);
+    void* ptrs[] = {p->d_lp,  p->d_media, p->d_fd, p->d_ranges, p->d_W, p->d_lc,     p->d_wc2,
+                    p->d_C,   p->d_rem,   p->d_G,  p->d_status, p->d_A, p->d_B,      p->d_rowexp,
+                    p->d_rowmax};
     for (void* q : ptrs)
         if (q) cudaFreeAsync(q, s);
     for (auto& sg : p->segs) {
@@ -309,8 +318,14 @@ int flush_segs(gfk_plan* p) {
     return GFK_OK;
 }
 
-int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const double* ranges, int32_t nr,
-               const double* freqs, int32_t nf, gfk_integration opt, GridMode mode, gfk_plan** out) {
+struct SoilIn {
+    const gfk_medium* m;
+    const double* freqs;
+    int nf;
+};
+
+int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s, const double* ranges, int32_t nr,
+               gfk_integration opt, GridMode mode, gfk_plan** out) {
     *out = nullptr;
     if (!ctx) return GFK_EARG;
     if (!s) return fail(ctx, GFK_EARG, "solve options missing");
@@ -322,94 +337,133 @@ int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const doub
         return fail(ctx, GFK_EARG, "the reference formulation evaluates at real frequencies; omega_imag must be 0");
     if (!(s->omega_imag >= 0) || !std::isfinite(s->omega_imag))
         return fail(ctx, GFK_EARG, "omega_imag must be finite and non-negative, got %g", s->omega_imag);
-    if (nf < 0 || nr < 0 || (nf > 0 && !freqs)) return fail(ctx, GFK_EARG, "fk: bad frequency list");
+    if (nsoil <= 0 || !soils) return fail(ctx, GFK_EARG, "no media given");
     if (nr <= 0 || !ranges) return fail(ctx, GFK_EARG, "fk: no ranges given");
     for (int j = 0; j < nr; j++)
         if (!(ranges[j] > 0)) return fail(ctx, GFK_EARG, "fk: range must be positive, got %g m", ranges[j]);
-    if (!m || !m->layers || m->count <= 0) return fail(ctx, GFK_ESTACK, "layer: a stack needs at least a half-space");
-    if (m->count > gfk::kMaxLayers)
-        return fail(ctx, GFK_ELIMIT, "layer: %d layers, this build handles at most %d", m->count, gfk::kMaxLayers);
+    int64_t nf_total = 0;
+    for (int i = 0; i < nsoil; i++) {
+        if (soils[i].nf < 0 || (soils[i].nf > 0 && !soils[i].freqs)) return fail(ctx, GFK_EARG, "fk: bad frequency list");
+        nf_total += soils[i].nf;
+    }
+    if (nf_total > INT32_MAX / 2) return fail(ctx, GFK_ELIMIT, "too many bank rows (%lld)", (long long)nf_total);
+    if (nsoil == 1) {  // a single medium's stack errors fail the call, as the Go calls do
+        const gfk_medium* m = soils[0].m;
+        if (!m || !m->layers || m->count <= 0)
+            return fail(ctx, GFK_ESTACK, "layer: a stack needs at least a half-space");
+        if (m->count > gfk::kMaxLayers)
+            return fail(ctx, GFK_ELIMIT, "layer: %d layers, this build handles at most %d", m->count, gfk::kMaxLayers);
+    }
 
     gfk_plan* p = new gfk_plan();
     p->ctx = ctx;
-    p->layers.assign(m->layers, m->layers + m->count);
-    p->med = *m;
-    p->med.layers = p->layers.data();
     p->solve = *s;
     p->ranges.assign(ranges, ranges + nr);
-    p->freqs.assign(freqs, freqs + nf);
-    p->nf = nf;
+    p->nsoil = nsoil;
+    p->nf = (int)nf_total;
     p->nr = nr;
-    p->nl = m->count;
     const bool guard = s->guard || s->formulation == GFK_REFERENCE_DIRECT;
-    const int stack_status = validate(ctx, &p->med);
-    const std::string stack_msg = ctx->last_error;
-    p->mu_ref = stack_status ? 0.0 : reference_modulus(&p->med);
     double rmin = INFINITY;
     for (double r : p->ranges) rmin = std::min(rmin, r);
-    const double slowest = slowest_vs(&p->med);
-    p->host_status.assign(nf, GFK_OK);
-    p->nk.assign(nf, 0);
-    p->dk.assign(nf, 0.0);
-    p->kfar.assign(nf, 0.0);
-    p->off.assign(nf, 0);
+    p->host_status.assign(p->nf, GFK_OK);
+    p->fd.assign(p->nf, gfk::FreqDesc{});
+    p->freqs.assign(p->nf, 0.0);
     std::string first_msg;
-    int64_t total = 0;
+    int64_t lc_total = 0;
     double g_kmax = -1;
     int g_n = -1;
     bool shared = true;
-    for (int f = 0; f < nf; f++) {
-        const double fr = p->freqs[f];
-        int st = GFK_OK;
-        if (guard) st = check_layer_phase(ctx, &p->med, fr);
-        gfk_grid g{0, 0, 0};
-        if (!st) {
-            if (mode == kGridMulti) {
-                st = grid_for(ctx, &p->med, p->ranges.data(), nr, fr, opt, &g);
-            } else {  // Medium.VerticalDisplacement's own rule (fk.go:407-421)
-                const double kbody = kTwoPi * fr / slowest;
-                const double kmf = opt.kmax_factor > 0 ? opt.kmax_factor : 30;
-                g.kmax = std::max(opt.kmax > 0 ? opt.kmax : kmf * kbody, 40 / p->ranges[0]);
-                g.samples = opt.samples > 0 ? opt.samples : 20000;
+    int row = 0;
+    for (int si = 0; si < nsoil; si++) {
+        const gfk_medium* m = soils[si].m;
+        gfk::MediumP mp{};
+        int stack_status = GFK_OK;
+        std::string stack_msg;
+        if (!m || !m->layers || m->count <= 0) {
+            stack_status = fail(ctx, GFK_ESTACK, "layer: a stack needs at least a half-space");
+        } else if (m->count > gfk::kMaxLayers) {
+            stack_status = fail(ctx, GFK_ELIMIT, "layer: %d layers, this build handles at most %d", m->count,
+                                gfk::kMaxLayers);
+        } else {
+            stack_status = validate(ctx, m);
+        }
+        stack_msg = ctx->last_error;
+        double slowest = 1.0;
+        if (stack_status == GFK_OK) {
+            mp = medium_params(m);
+            mp.mu_ref = reference_modulus(m);
+            mp.lp_off = (int)p->lp.size();
+            for (int i = 0; i < m->count; i++) {
+                const gfk_layer& l = m->layers[i];
+                p->lp.push_back(gfk::LayerP{l.thickness_m, l.vp_mps, l.vs_mps, l.density_kgm3, l.qs, l.qp});
             }
+            slowest = slowest_vs(m);
+            p->max_nl = std::max(p->max_nl, m->count);
+        } else {
+            mp.count = 0;  // an invalid medium never reaches the device
         }
-        if (!st && !(fr > 0))
-            st = fail(ctx, GFK_EARG, "fk: wavenumber and frequency must be positive, got %g and %g",
-                      std::max(200 * kTwoPi * fr / slowest, 400 / rmin), fr);
-        if (!st && stack_status) {
-            st = stack_status;
-            ctx->last_error = stack_msg;
-        }
-        if (st) {
-            p->host_status[f] = st;
-            if (first_msg.empty()) first_msg = ctx->last_error;
-            shared = false;
-            continue;
-        }
-        const double kbody = kTwoPi * fr / slowest;
-        p->kfar[f] = std::max(200 * kbody, 400 / rmin);
-        p->nk[f] = g.samples;
-        p->dk[f] = g.kmax / g.samples;
-        p->off[f] = total;
-        total += g.samples;
-        p->max_nk = std::max(p->max_nk, g.samples);
-        if (g_n < 0) {
-            g_n = g.samples;
-            g_kmax = g.kmax;
-        } else if (g_n != g.samples || g_kmax != g.kmax) {
-            shared = false;
+        p->media.push_back(mp);
+        for (int fi = 0; fi < soils[si].nf; fi++, row++) {
+            const double fr = soils[si].freqs[fi];
+            p->freqs[row] = fr;
+            gfk::FreqDesc& d = p->fd[row];
+            d.freq = fr;
+            d.soil = si;
+            d.lc_off = lc_total;
+            int st = GFK_OK;
+            if (stack_status != GFK_OK && stack_status != GFK_ESTACK) {
+                st = stack_status;
+                ctx->last_error = stack_msg;
+            }
+            if (!st && guard && m && m->layers && m->count > 0) st = check_layer_phase(ctx, m, fr);
+            gfk_grid g{0, 0, 0};
+            if (!st && m && m->layers && m->count > 0) {
+                if (mode == kGridMulti) {
+                    st = grid_for(ctx, m, p->ranges.data(), nr, fr, opt, &g);
+                } else {  // Medium.VerticalDisplacement's own rule (fk.go:407-421)
+                    const double kbody = kTwoPi * fr / slowest;
+                    const double kmf = opt.kmax_factor > 0 ? opt.kmax_factor : 30;
+                    g.kmax = std::max(opt.kmax > 0 ? opt.kmax : kmf * kbody, 40 / p->ranges[0]);
+                    g.samples = opt.samples > 0 ? opt.samples : 20000;
+                }
+            }
+            if (!st && !(fr > 0))
+                st = fail(ctx, GFK_EARG, "fk: wavenumber and frequency must be positive, got %g and %g",
+                          std::max(200 * kTwoPi * fr / slowest, 400 / rmin), fr);
+            if (!st && stack_status) {
+                st = stack_status;
+                ctx->last_error = stack_msg;
+            }
+            if (st) {
+                p->host_status[row] = st;
+                if (first_msg.empty()) first_msg = ctx->last_error;
+                shared = false;
+                continue;  // kfar = 0: no device work for this row
+            }
+            lc_total += m->count;
+            const double kbody = kTwoPi * fr / slowest;
+            d.kfar = std::max(200 * kbody, 400 / rmin);
+            d.nk = g.samples;
+            d.dk = g.kmax / g.samples;
+            p->max_nk = std::max(p->max_nk, g.samples);
+            if (g_n < 0) {
+                g_n = g.samples;
+                g_kmax = g.kmax;
+            } else if (g_n != g.samples || g_kmax != g.kmax) {
+                shared = false;
+            }
         }
     }
     ctx->last_error = first_msg;
-    p->total_k = total;
     p->shared = shared && g_n > 0;
+    p->g_n = std::max(g_n, 0);
+    p->g_kmax = g_kmax;
     if (s->quadrature == GFK_SPLIT_INT8) {
-        if (nf > 0 && g_n > 0 && !p->shared) {
-            std::string m = "the split quadrature needs one wavenumber grid for every frequency "
-                            "(a fixed Integration.kmax and samples)";
+        if (p->nf > 0 && g_n > 0 && !p->shared) {
             plan_free(p);
             delete p;
-            return fail(ctx, GFK_EARG, "%s", m.c_str());
+            return fail(ctx, GFK_EARG, "the split quadrature needs one wavenumber grid for every frequency "
+                                       "(a fixed Integration.kmax and samples)");
         }
         if (g_n > 65536) {
             plan_free(p);
@@ -419,33 +473,39 @@ int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const doub
         }
         p->tc = p->shared;
     }
-    // frequency chunks bounded by the integrand budget
+    // row chunks bounded by the integrand budget and the grid limit
     const int64_t budget = kDefaultRemBudget / (int64_t)sizeof(cd);
     int64_t acc = 0, cap = 0;
+    int rows_in = 0, cmax = 0;
     p->chunk_begin.push_back(0);
-    for (int f = 0; f < nf; f++) {
-        if (acc > 0 && acc + p->nk[f] > budget) {
+    for (int f = 0; f < p->nf; f++) {
+        const int nk = p->fd[f].kfar > 0 ? p->fd[f].nk : 0;
+        if (rows_in > 0 && (acc + nk > budget || rows_in >= kMaxChunkRows)) {
             p->chunk_begin.push_back(f);
+            p->chunk_max_nk.push_back(cmax);
             cap = std::max(cap, acc);
             acc = 0;
+            rows_in = 0;
+            cmax = 0;
         }
-        acc += p->nk[f];
+        p->fd[f].off = acc;
+        acc += nk;
+        rows_in++;
+        cmax = std::max(cmax, nk);
     }
     cap = std::max(cap, acc);
-    p->chunk_begin.push_back(nf);
+    p->chunk_begin.push_back(p->nf);
+    p->chunk_max_nk.push_back(cmax);
     p->rem_capacity = cap;
 
     // device buffers
     int st = GFK_OK;
-    const size_t nfa = std::max(nf, 1);
-    if (!st) st = dalloc(ctx, &p->d_layers, p->nl);
-    if (!st) st = dalloc(ctx, &p->d_freqs, nfa);
+    const size_t nfa = std::max(p->nf, 1);
+    if (!st) st = dalloc(ctx, &p->d_lp, std::max<size_t>(p->lp.size(), 1));
+    if (!st) st = dalloc(ctx, &p->d_media, (size_t)nsoil);
+    if (!st) st = dalloc(ctx, &p->d_fd, nfa);
     if (!st) st = dalloc(ctx, &p->d_ranges, nr);
-    if (!st) st = dalloc(ctx, &p->d_dk, nfa);
-    if (!st) st = dalloc(ctx, &p->d_kfar, nfa);
-    if (!st) st = dalloc(ctx, &p->d_nk, nfa);
-    if (!st) st = dalloc(ctx, &p->d_off, nfa);
-    if (!st) st = dalloc(ctx, &p->d_lc, nfa * p->nl);
+    if (!st) st = dalloc(ctx, &p->d_lc, (size_t)std::max<int64_t>(lc_total, 1));
     if (!st) st = dalloc(ctx, &p->d_wc2, nfa);
     if (!st) st = dalloc(ctx, &p->d_C, nfa);
     if (!st) st = dalloc(ctx, &p->d_G, nfa * nr);
@@ -467,30 +527,12 @@ int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const doub
         if (!st && cudaMemsetAsync(p->d_A, 0, (size_t)4 * p->Mp * p->Kp, ctx->stream) != cudaSuccess)
             st = fail(ctx, GFK_ECUDA, "clearing the slice planes failed");
     }
-    if (st) {
-        plan_free(p);
-        delete p;
-        return st;
-    }
-    std::vector<gfk::LayerP> lp(p->nl);
-    for (int i = 0; i < p->nl; i++) {
-        const gfk_layer& l = p->layers[i];
-        lp[i] = gfk::LayerP{l.thickness_m, l.vp_mps, l.vs_mps, l.density_kgm3, l.qs, l.qp};
-    }
-    // offsets are relative to their chunk's start
-    std::vector<int64_t> roff(nf);
-    for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++) {
-        const int fb = p->chunk_begin[c], fe = p->chunk_begin[c + 1];
-        const int64_t base = fb < nf ? p->off[fb] : 0;
-        for (int f = fb; f < fe; f++) roff[f] = p->off[f] - base;
-    }
-    if (!st) st = h2d(ctx, p->d_layers, lp.data(), lp.size());
-    if (!st) st = h2d(ctx, p->d_freqs, p->freqs.data(), nf);
+    if (!st) st = h2d(ctx, p->d_lp, p->lp.data(), p->lp.size());
+    if (!st) st = h2d(ctx, p->d_media, p->media.data(), p->media.size());
+    if (!st) st = h2d(ctx, p->d_fd, p->fd.data(), p->fd.size());
     if (!st) st = h2d(ctx, p->d_ranges, p->ranges.data(), nr);
-    if (!st) st = h2d(ctx, p->d_dk, p->dk.data(), nf);
-    if (!st) st = h2d(ctx, p->d_kfar, p->kfar.data(), nf);
-    if (!st) st = h2d(ctx, p->d_nk, p->nk.data(), nf);
-    if (!st) st = h2d(ctx, p->d_off, roff.data(), nf);
+    if (!st && cudaStreamSynchronize(ctx->stream) != cudaSuccess)  // host tables may be freed by the caller
+        st = fail(ctx, GFK_ECUDA, "plan upload failed");
     if (st) {
         plan_free(p);
         delete p;
@@ -499,14 +541,14 @@ int plan_build(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const doub
     int nchunks = 0;
     for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
         if (p->chunk_begin[c + 1] > p->chunk_begin[c]) nchunks++;
-    p->launches_per_exec = nf > 0 ? (p->tc ? 3 + 3 * nchunks : 2 + 2 * nchunks + (p->shared ? 1 : 0)) : 0;
+    p->launches_per_exec = p->nf > 0 ? (p->tc ? 3 + 3 * nchunks : 2 + 2 * nchunks + (p->shared ? 1 : 0)) : 0;
     *out = p;
     return GFK_OK;
 }
 
-// Times every Dunkin launch shape on a window of up to 64 of the plan's own
-// frequencies (the middle of the band) and keeps the fastest. The window's
-// integrand rows are recomputed by the real launch afterwards.
+// Times every Dunkin launch shape on a window of up to 64 rows of the first
+// chunk (its middle) and keeps the fastest. The window's integrand rows are
+// recomputed by the real launch afterwards.
 int tune_prop(gfk_plan* p) {
     gfk_ctx* ctx = p->ctx;
     cudaStream_t s = ctx->stream;
@@ -518,7 +560,7 @@ int tune_prop(gfk_plan* p) {
     }
     if (p->solve.formulation != GFK_DUNKIN || p->nf == 0) return GFK_OK;
     for (const auto& t : ctx->tuned)
-        if (t.nl == p->nl && t.nk == p->max_nk) {
+        if (t.nl == p->max_nl && t.nk == p->max_nk) {
             p->prop_variant = t.variant;
             return GFK_OK;
         }
@@ -527,7 +569,7 @@ int tune_prop(gfk_plan* p) {
     if (win <= 0) return GFK_OK;
     const int fb = c0 + (c1 - c0 - win) / 2;
     int cmax = 0;
-    for (int f = fb; f < fb + win; f++) cmax = std::max(cmax, p->nk[f]);
+    for (int f = fb; f < fb + win; f++) cmax = std::max(cmax, p->fd[f].kfar > 0 ? p->fd[f].nk : 0);
     if ((int64_t)win * cmax < 4096) return GFK_OK;  // too little work to tell shapes apart
     cudaEvent_t a, b;
     GFK_CUDA(ctx, cudaEventCreate(&a));
@@ -536,9 +578,8 @@ int tune_prop(gfk_plan* p) {
     for (int rep = 0; rep < 2; rep++)
         for (int v = 0; v < nv; v++) {
             cudaEventRecord(a, s);
-            gfk::launch_prop(s, p->d_lc + (size_t)fb * p->nl, p->nl, p->d_freqs + fb, p->d_wc2 + fb, win,
-                             p->d_nk + fb, p->d_dk + fb, p->d_off + fb, cmax, p->d_C + fb, p->mu_ref, GFK_DUNKIN,
-                             p->d_rem, p->d_status + fb, v);
+            gfk::launch_prop(s, p->d_lc, p->d_media, p->d_fd + fb, p->d_wc2 + fb, win, cmax, p->d_C + fb,
+                             GFK_DUNKIN, p->d_rem, p->d_status + fb, v);
             cudaEventRecord(b, s);
             ctx->launches++;
             cudaError_t e = cudaEventSynchronize(b);
@@ -557,63 +598,91 @@ int tune_prop(gfk_plan* p) {
     for (int v = 1; v < nv; v++)
         if (p->tune_ms[v] < p->tune_ms[best]) best = v;
     p->prop_variant = best;
-    ctx->tuned.push_back({p->nl, p->max_nk, best});
+    ctx->tuned.push_back({p->max_nl, p->max_nk, best});
+    return GFK_OK;
+}
+
+// Enqueues one whole execute on the context's stream. `timed` records the
+// per-kernel-class event segments (not inside a graph capture).
+int plan_enqueue(gfk_plan* p, bool timed) {
+    gfk_ctx* ctx = p->ctx;
+    cudaStream_t s = ctx->stream;
+    const int nf = p->nf;
+    const int form = p->solve.formulation;
+    int st = GFK_OK;
+    size_t seg = 0;
+    GFK_CUDA(ctx, cudaMemsetAsync(p->d_status, 0, sizeof(int) * nf, s));
+    if (timed && (st = begin_seg(p, 2, &seg))) return st;
+    gfk::launch_layer_consts(s, p->d_lp, p->d_media, p->d_fd, nf, p->solve.omega_imag, form, p->d_lc, p->d_wc2);
+    gfk::launch_static(s, p->d_lc, p->d_media, p->d_fd, p->d_wc2, nf, form, p->d_C, p->d_status);
+    if (p->tc)
+        gfk::launch_j0_slices(s, p->d_ranges, p->nr, p->g_n, p->Kp, p->Np, p->g_kmax / p->g_n, p->col_exp, p->d_B);
+    else if (p->shared)
+        gfk::launch_j0_table(s, p->d_ranges, p->nr, p->g_n, p->g_kmax / p->g_n, p->d_W);
+    if (timed && (st = end_seg(p, seg))) return st;
+    ctx->launches += 2 + (p->shared ? 1 : 0);
+    if (timed && p->prop_variant < 0 && (st = tune_prop(p))) return st;
+    const double dk = p->shared ? p->g_kmax / p->g_n : 0.0;
+    for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++) {
+        const int fb = p->chunk_begin[c], fe = p->chunk_begin[c + 1];
+        const int cnf = fe - fb;
+        if (cnf <= 0) continue;
+        const int cmax = p->chunk_max_nk[c];
+        if (p->tc) GFK_CUDA(ctx, cudaMemsetAsync(p->d_rowmax, 0, sizeof(unsigned long long) * 2 * cnf, s));
+        if (timed && (st = begin_seg(p, 0, &seg))) return st;
+        gfk::launch_prop(s, p->d_lc, p->d_media, p->d_fd + fb, p->d_wc2 + fb, cnf, cmax, p->d_C + fb, form, p->d_rem,
+                         p->d_status + fb, std::max(p->prop_variant, 0), p->tc ? p->d_rowmax : nullptr);
+        if (timed && (st = end_seg(p, seg))) return st;
+        if (timed && (st = begin_seg(p, 1, &seg))) return st;
+        if (p->tc) {
+            gfk::launch_slice_rem(s, p->d_rem, p->g_n, p->Kp, p->Mp, cnf, p->d_rowmax, p->d_rowexp, p->d_A);
+            if (gfk::launch_quad_tc(s, p->d_A, p->d_B, 2 * cnf, p->nr, p->Mp, p->Np, p->Kp, p->d_rowexp, p->col_exp,
+                                    p->d_C + fb, p->d_ranges, dk, p->d_G + (size_t)fb * p->nr, p->d_status + fb))
+                return fail(ctx, GFK_ECUDA, "tensor-core quadrature launch setup failed");
+            ctx->launches += 1;
+        } else if (p->shared) {
+            gfk::launch_quad_gemm(s, p->d_rem, p->d_W, p->d_C + fb, p->d_ranges, cnf, p->g_n, p->nr, dk,
+                                  p->d_G + (size_t)fb * p->nr);
+        } else {
+            gfk::launch_quad_ragged(s, p->d_rem, p->d_C + fb, p->d_ranges, cnf, p->nr, p->d_fd + fb,
+                                    p->d_G + (size_t)fb * p->nr);
+        }
+        if (timed && (st = end_seg(p, seg))) return st;
+        ctx->launches += 2;
+    }
+    GFK_CUDA(ctx, cudaGetLastError());
     return GFK_OK;
 }
 
 int plan_exec(gfk_plan* p) {
     gfk_ctx* ctx = p->ctx;
-    cudaStream_t s = ctx->stream;
-    const int nf = p->nf;
-    if (nf == 0) {
+    if (p->nf == 0) {
         p->executed = true;
         return GFK_OK;
     }
-    const int form = p->solve.formulation;
-    GFK_CUDA(ctx, cudaMemsetAsync(p->d_status, 0, sizeof(int) * nf, s));
-    size_t seg;
-    int st = begin_seg(p, 2, &seg);
-    if (st) return st;
-    gfk::launch_layer_consts(s, p->d_layers, medium_params(&p->med), p->d_freqs, nf, p->solve.omega_imag, p->mu_ref,
-                             form, p->d_lc, p->d_wc2);
-    gfk::launch_static(s, p->d_lc, p->nl, p->d_freqs, p->d_wc2, p->d_kfar, nf, p->mu_ref, form, p->d_C, p->d_status);
-    if (p->tc)
-        gfk::launch_j0_slices(s, p->d_ranges, p->nr, p->nk[0], p->Kp, p->Np, p->dk[0], p->col_exp, p->d_B);
-    else if (p->shared)
-        gfk::launch_j0_table(s, p->d_ranges, p->nr, p->nk[0], p->dk[0], p->d_W);
-    if ((st = end_seg(p, seg))) return st;
-    ctx->launches += 2 + (p->shared ? 1 : 0);
-    if (p->prop_variant < 0 && (st = tune_prop(p))) return st;
-    for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++) {
-        const int fb = p->chunk_begin[c], fe = p->chunk_begin[c + 1];
-        const int cnf = fe - fb;
-        if (cnf <= 0) continue;
-        int cmax = 0;
-        for (int f = fb; f < fe; f++) cmax = std::max(cmax, p->nk[f]);
-        if (p->tc) GFK_CUDA(ctx, cudaMemsetAsync(p->d_rowmax, 0, sizeof(unsigned long long) * 2 * cnf, s));
-        if ((st = begin_seg(p, 0, &seg))) return st;
-        gfk::launch_prop(s, p->d_lc + (size_t)fb * p->nl, p->nl, p->d_freqs + fb, p->d_wc2 + fb, cnf, p->d_nk + fb,
-                         p->d_dk + fb, p->d_off + fb, cmax, p->d_C + fb, p->mu_ref, form, p->d_rem, p->d_status + fb,
-                         p->prop_variant, p->tc ? p->d_rowmax : nullptr);
+    int st = GFK_OK;
+    if (p->use_graph && p->executed && p->prop_variant >= 0) {
+        if (!p->gexec) {  // capture one whole execute, once
+            const int64_t before = ctx->launches;
+            cudaGraph_t g = nullptr;
+            GFK_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            st = plan_enqueue(p, false);
+            cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+            if (!st && e != cudaSuccess) st = fail(ctx, GFK_ECUDA, "graph capture: %s", cudaGetErrorString(e));
+            if (!st && cudaGraphInstantiate(&p->gexec, g, 0) != cudaSuccess)
+                st = fail(ctx, GFK_ECUDA, "graph instantiation failed");
+            if (g) cudaGraphDestroy(g);
+            ctx->launches = before;  // capturing launches nothing
+            if (st) return st;
+        }
+        size_t seg;
+        if ((st = begin_seg(p, 3, &seg))) return st;
+        GFK_CUDA(ctx, cudaGraphLaunch(p->gexec, ctx->stream));
         if ((st = end_seg(p, seg))) return st;
-        if ((st = begin_seg(p, 1, &seg))) return st;
-        if (p->tc) {
-            gfk::launch_slice_rem(s, p->d_rem, p->nk[0], p->Kp, p->Mp, cnf, p->d_rowmax, p->d_rowexp, p->d_A);
-            if (gfk::launch_quad_tc(s, p->d_A, p->d_B, 2 * cnf, p->nr, p->Mp, p->Np, p->Kp, p->d_rowexp, p->col_exp,
-                                    p->d_C + fb, p->d_ranges, p->dk[0], p->d_G + (size_t)fb * p->nr,
-                                    p->d_status + fb))
-                return fail(ctx, GFK_ECUDA, "tensor-core quadrature launch setup failed");
-            ctx->launches += 1;
-        } else if (p->shared)
-            gfk::launch_quad_gemm(s, p->d_rem, p->d_W, p->d_C + fb, p->d_ranges, cnf, p->nk[0], p->nr, p->dk[0],
-                                  p->d_G + (size_t)fb * p->nr);
-        else
-            gfk::launch_quad_ragged(s, p->d_rem, p->d_C + fb, p->d_ranges, cnf, p->nr, p->d_nk + fb, p->d_dk + fb,
-                                    p->d_off + fb, p->d_G + (size_t)fb * p->nr);
-        if ((st = end_seg(p, seg))) return st;
-        ctx->launches += 2;
+        ctx->launches += p->launches_per_exec;
+    } else {
+        if ((st = plan_enqueue(p, true))) return st;
     }
-    GFK_CUDA(ctx, cudaGetLastError());
     p->acc_execs++;
     p->executed = true;
     return GFK_OK;
@@ -649,6 +718,12 @@ int plan_download(gfk_plan* p, double* out, int32_t* status) {
     }
     if (first) ctx->last_error = msg;
     return first;
+}
+
+int plan_one(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const double* ranges, int32_t nr,
+             const double* freqs, int32_t nf, gfk_integration opt, GridMode mode, gfk_plan** out) {
+    SoilIn si{m, freqs, nf};
+    return plan_build(ctx, &si, 1, s, ranges, nr, opt, mode, out);
 }
 
 }  // namespace
@@ -732,7 +807,7 @@ int gfk_plan_create(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const
     if (!out) return GFK_EARG;
     if (!ctx) return GFK_EARG;
     cudaSetDevice(ctx->device);
-    int st = plan_build(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, out);
+    int st = plan_one(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, out);
     if (!st) ctx->plans.push_back(*out);
     return st;
 }
@@ -772,12 +847,35 @@ int gfk_plan_kernel_times(gfk_plan* p, double* prop_ms, double* quad_ms, double*
     const double n = p->acc_execs > 0 ? p->acc_execs : 1;
     if (prop_ms) *prop_ms = p->acc_ms[0] / n;
     if (quad_ms) *quad_ms = p->acc_ms[1] / n;
-    if (other_ms) *other_ms = p->acc_ms[2] / n;
+    if (other_ms) *other_ms = (p->acc_ms[2] + p->acc_ms[3]) / n;
     if (reset) {
-        p->acc_ms[0] = p->acc_ms[1] = p->acc_ms[2] = 0;
+        p->acc_ms[0] = p->acc_ms[1] = p->acc_ms[2] = p->acc_ms[3] = 0;
         p->acc_execs = 0;
     }
     return GFK_OK;
+}
+
+int gfk_plan_use_graph(gfk_plan* p, int32_t enable) {
+    if (!p) return GFK_EARG;
+    p->use_graph = enable != 0;
+    if (!p->use_graph && p->gexec) {
+        cudaGraphExecDestroy(p->gexec);
+        p->gexec = nullptr;
+    }
+    return GFK_OK;
+}
+
+int gfk_batch_create(gfk_ctx* ctx, const gfk_medium* media, int32_t nsoil, const double* const* freqs_hz,
+                     const int32_t* nf, const gfk_solve* s, const double* ranges_m, int32_t nr, gfk_integration opt,
+                     gfk_plan** out) {
+    if (!ctx || !out) return GFK_EARG;
+    if (nsoil <= 0 || !media || !freqs_hz || !nf) return fail(ctx, GFK_EARG, "no media given");
+    cudaSetDevice(ctx->device);
+    std::vector<SoilIn> soils(nsoil);
+    for (int i = 0; i < nsoil; i++) soils[i] = SoilIn{&media[i], freqs_hz[i], nf[i]};
+    int st = plan_build(ctx, soils.data(), nsoil, s, ranges_m, nr, opt, kGridMulti, out);
+    if (!st) ctx->plans.push_back(*out);
+    return st;
 }
 
 int gfk_plan_destroy(gfk_plan* p) {
@@ -795,7 +893,7 @@ int gfk_bank_spectra(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, cons
     if (!ctx) return GFK_EARG;
     cudaSetDevice(ctx->device);
     gfk_plan* p = nullptr;
-    int st = plan_build(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, &p);
+    int st = plan_one(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, &p);
     if (st) return st;
     st = plan_exec(p);
     if (!st) st = plan_download(p, out, status_per_f);
@@ -819,10 +917,11 @@ int gfk_vertical_displacement(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve
     if (!(freq_hz > 0)) return fail(ctx, GFK_EARG, "fk: frequency must be positive, got %g Hz", freq_hz);
     cudaSetDevice(ctx->device);
     gfk_plan* p = nullptr;
-    int st = plan_build(ctx, m, s, &range_m, 1, &freq_hz, 1, opt, kGridSingle, &p);
+    int st = plan_one(ctx, m, s, &range_m, 1, &freq_hz, 1, opt, kGridSingle, &p);
     if (st) return st;
     // a single range always takes the per-frequency (sequential-sum) quadrature
     p->shared = false;
+    p->tc = false;
     st = plan_exec(p);
     int32_t fst = 0;
     if (!st) st = plan_download(p, out, &fst);
@@ -889,12 +988,25 @@ extern "C" int gfk_surface_response(gfk_ctx* ctx, const gfk_medium* m, const gfk
         const gfk_layer& l = m->layers[i];
         lp[i] = gfk::LayerP{l.thickness_m, l.vp_mps, l.vs_mps, l.density_kgm3, l.qs, l.qp};
     }
+    gfk::MediumP mp = medium_params(m);
+    mp.mu_ref = mu_ref;
+    mp.lp_off = 0;
+    std::vector<gfk::FreqDesc> fds(nf);
+    for (int f = 0; f < nf; f++) {
+        fds[f] = gfk::FreqDesc{};
+        fds[f].freq = uf[f];
+        fds[f].lc_off = (int64_t)f * nl;
+    }
     gfk::LayerP* d_layers = nullptr;
+    gfk::MediumP* d_media = nullptr;
+    gfk::FreqDesc* d_fd = nullptr;
     double *d_f = nullptr, *d_k = nullptr;
     int *d_fidx = nullptr, *d_status = nullptr;
     gfk::LayerC* d_lc = nullptr;
     cd *d_wc2 = nullptr, *d_out = nullptr;
     st = dalloc(ctx, &d_layers, nl);
+    if (!st) st = dalloc(ctx, &d_media, 1);
+    if (!st) st = dalloc(ctx, &d_fd, nf);
     if (!st) st = dalloc(ctx, &d_f, nf);
     if (!st) st = dalloc(ctx, &d_k, n);
     if (!st) st = dalloc(ctx, &d_fidx, n);
@@ -903,14 +1015,15 @@ extern "C" int gfk_surface_response(gfk_ctx* ctx, const gfk_medium* m, const gfk
     if (!st) st = dalloc(ctx, &d_wc2, nf);
     if (!st) st = dalloc(ctx, &d_out, n);
     if (!st) st = h2d(ctx, d_layers, lp.data(), nl);
+    if (!st) st = h2d(ctx, d_media, &mp, 1);
+    if (!st) st = h2d(ctx, d_fd, fds.data(), nf);
     if (!st) st = h2d(ctx, d_f, uf.data(), nf);
     if (!st) st = h2d(ctx, d_k, k, n);
     if (!st) st = h2d(ctx, d_fidx, fidx.data(), n);
     int hstat = 0;
     if (!st) {
         cudaMemsetAsync(d_status, 0, sizeof(int), ctx->stream);
-        gfk::launch_layer_consts(ctx->stream, d_layers, medium_params(m), d_f, nf, s->omega_imag, mu_ref,
-                                 s->formulation, d_lc, d_wc2);
+        gfk::launch_layer_consts(ctx->stream, d_layers, d_media, d_fd, nf, s->omega_imag, s->formulation, d_lc, d_wc2);
         gfk::k_pairs<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
             d_lc, nl, d_f, d_wc2, d_fidx, d_k, n, mu_ref, s->formulation, d_out, d_status);
         ctx->launches += 2;
@@ -923,9 +1036,10 @@ extern "C" int gfk_surface_response(gfk_ctx* ctx, const gfk_medium* m, const gfk
         cudaError_t e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) st = fail(ctx, GFK_ECUDA, "surface response: %s", cudaGetErrorString(e));
     }
-    void* ptrs[] = {d_layers, d_f, d_k, d_fidx, d_status, d_lc, d_wc2, d_out};
+    void* ptrs[] = {d_layers, d_media, d_fd, d_f, d_k, d_fidx, d_status, d_lc, d_wc2, d_out};
     for (void* q : ptrs)
         if (q) cudaFreeAsync(q, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);  // the host tables above are freed on return
     if (st) return st;
     if (hstat & gfk::kStSingular)
         return fail(ctx, GFK_ESINGULAR, "fk: layer propagator or surface system is singular");

@@ -16,71 +16,73 @@ namespace gfk {
 
 // ------------------------------------------------------------ constants --
 
-__global__ void k_layer_consts(const LayerP* __restrict__ layers, MediumP med, const double* __restrict__ freqs,
-                               int nf, double wi, double mu_ref, int formulation, LayerC* __restrict__ lc,
-                               cd* __restrict__ wc2) {
-    const int nl = med.count;
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= nf * nl) return;
-    const int f = idx / nl, l = idx - f * nl;
-    const double fr = freqs[f];
-    const LayerP L = layers[l];
-    const double q = q_of(med, L);
-    LayerC out;
-    if (formulation == 0) {
-        // Medium.propsOf (fk.go:119-128): Qp = 2.25 Qs, real frequency
-        const cd a = complex_velocity(med, L.vp, 2.25 * q, fr, 0.0);
-        const cd b = complex_velocity(med, L.vs, q, fr, 0.0);
-        out.c[0] = a;
-        out.c[1] = b;
-        out.c[2] = (L.rho * b) * b;
-        out.c[3] = mk(L.rho);
-    } else {
-        const double qp = L.qp > 0 ? L.qp : 2.25 * q;
-        const cd a = complex_velocity(med, L.vp, qp, fr, wi);
-        const cd b = complex_velocity(med, L.vs, q, fr, wi);
-        const cd a2 = a * a, b2 = b * b;
-        out.c[0] = 1.0 / a2;
-        out.c[1] = 1.0 / b2;
-        out.c[2] = b2 / a2;
-        out.c[3] = (L.rho * b2) / mu_ref;
+__global__ void k_layer_consts(const LayerP* __restrict__ lp, const MediumP* __restrict__ media,
+                               const FreqDesc* __restrict__ fd, int nf, double wi, int formulation,
+                               LayerC* __restrict__ lc, cd* __restrict__ wc2) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const FreqDesc d = fd[f];
+    const MediumP med = media[d.soil];
+    const double fr = d.freq;
+    for (int l = 0; l < med.count; l++) {
+        const LayerP L = lp[med.lp_off + l];
+        const double q = q_of(med, L);
+        LayerC out;
+        if (formulation == 0) {
+            // Medium.propsOf (fk.go:119-128): Qp = 2.25 Qs, real frequency
+            const cd a = complex_velocity(med, L.vp, 2.25 * q, fr, 0.0);
+            const cd b = complex_velocity(med, L.vs, q, fr, 0.0);
+            out.c[0] = a;
+            out.c[1] = b;
+            out.c[2] = (L.rho * b) * b;
+            out.c[3] = mk(L.rho);
+        } else {
+            const double qp = L.qp > 0 ? L.qp : 2.25 * q;
+            const cd a = complex_velocity(med, L.vp, qp, fr, wi);
+            const cd b = complex_velocity(med, L.vs, q, fr, wi);
+            const cd a2 = a * a, b2 = b * b;
+            out.c[0] = 1.0 / a2;
+            out.c[1] = 1.0 / b2;
+            out.c[2] = b2 / a2;
+            out.c[3] = (L.rho * b2) / med.mu_ref;
+        }
+        out.h = L.h;
+        out.pad = 0.0;
+        lc[d.lc_off + l] = out;
     }
-    out.h = L.h;
-    out.pad = 0.0;
-    lc[idx] = out;
-    if (l == 0) {
-        const cd wc = mk(kTwoPi * fr, -wi);
-        wc2[f] = wc * wc;
-    }
+    const cd wc = mk(kTwoPi * fr, -wi);
+    wc2[f] = wc * wc;
 }
 
-void launch_layer_consts(cudaStream_t s, const LayerP* layers, MediumP med, const double* freqs, int nf,
-                         double wi, double mu_ref, int formulation, LayerC* lc, cd* wc2) {
-    const int n = nf * med.count;
-    k_layer_consts<<<(n + 127) / 128, 128, 0, s>>>(layers, med, freqs, nf, wi, mu_ref, formulation, lc, wc2);
+void launch_layer_consts(cudaStream_t s, const LayerP* lp, const MediumP* media, const FreqDesc* fd, int nf,
+                         double wi, int formulation, LayerC* lc, cd* wc2) {
+    if (nf <= 0) return;
+    k_layer_consts<<<(nf + 127) / 128, 128, 0, s>>>(lp, media, fd, nf, wi, formulation, lc, wc2);
 }
 
 __device__ __forceinline__ bool finite_cd(cd a) { return isfinite(a.re) && isfinite(a.im); }
 
 // ------------------------------------------------------ static coefficient --
 
-__global__ void k_static(const LayerC* __restrict__ lc, int nl, const double* __restrict__ freqs,
-                         const cd* __restrict__ wc2, const double* __restrict__ kfar, int nf, double mu_ref,
-                         int formulation, cd* __restrict__ C, int* __restrict__ status) {
+__global__ void k_static(const LayerC* __restrict__ lc, const MediumP* __restrict__ media,
+                         const FreqDesc* __restrict__ fd, const cd* __restrict__ wc2, int nf, int formulation,
+                         cd* __restrict__ C, int* __restrict__ status) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nf) return;
-    const double k = kfar[f];
+    const FreqDesc d = fd[f];
+    const double k = d.kfar;
     if (!(k > 0)) {
         C[f] = mk(0.0);
         return;
     }
+    const MediumP med = media[d.soil];
     cd u;
     if (formulation == 0) {
         bool ok;
-        u = direct_u(lc + (size_t)f * nl, nl, kTwoPi * freqs[f], k, mu_ref, ok);
+        u = direct_u(lc + d.lc_off, med.count, kTwoPi * d.freq, k, med.mu_ref, ok);
         if (!ok) atomicOr(status + f, kStSingular);
     } else {
-        u = dunkin_u(lc + (size_t)f * nl, nl, wc2[f], k, mu_ref);
+        u = dunkin_u(lc + d.lc_off, med.count, wc2[f], k, med.mu_ref);
     }
     cd c = k * u;
     if (!finite_cd(c)) {
@@ -90,9 +92,10 @@ __global__ void k_static(const LayerC* __restrict__ lc, int nl, const double* __
     C[f] = c;
 }
 
-void launch_static(cudaStream_t s, const LayerC* lc, int nl, const double* freqs, const cd* wc2,
-                   const double* kfar, int nf, double mu_ref, int formulation, cd* C, int* status) {
-    k_static<<<(nf + 63) / 64, 64, 0, s>>>(lc, nl, freqs, wc2, kfar, nf, mu_ref, formulation, C, status);
+void launch_static(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2, int nf,
+                   int formulation, cd* C, int* status) {
+    if (nf <= 0) return;
+    k_static<<<(nf + 63) / 64, 64, 0, s>>>(lc, media, fd, wc2, nf, formulation, C, status);
 }
 
 // ------------------------------------------------------------ propagator --
@@ -103,28 +106,32 @@ void launch_static(cudaStream_t s, const LayerC* lc, int nl, const double* freqs
 // parameters; the plan times them once and keeps the fastest.
 
 template <int FORM, int THREADS, int MINB, int ILP>
-__global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict__ lc, int nl,
-                                                       const double* __restrict__ freqs, const cd* __restrict__ wc2,
-                                                       const int* __restrict__ nk, const double* __restrict__ dk,
-                                                       const int64_t* __restrict__ off, const cd* __restrict__ C,
-                                                       double mu_ref, cd* __restrict__ rem, int* __restrict__ status,
+__global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict__ lc,
+                                                       const MediumP* __restrict__ media,
+                                                       const FreqDesc* __restrict__ fd, const cd* __restrict__ wc2,
+                                                       const cd* __restrict__ C, cd* __restrict__ rem,
+                                                       int* __restrict__ status,
                                                        unsigned long long* __restrict__ rowmax) {
     __shared__ LayerC s_lc[kMaxLayers];
     const int f = blockIdx.y;
-    for (int l = threadIdx.x; l < nl; l += blockDim.x) s_lc[l] = lc[(size_t)f * nl + l];
+    const FreqDesc fdesc = fd[f];
+    const MediumP med = media[fdesc.soil];
+    const int nl = med.count;
+    const double mu_ref = med.mu_ref;
+    for (int l = threadIdx.x; l < nl; l += blockDim.x) s_lc[l] = lc[fdesc.lc_off + l];
     __syncthreads();
-    const int n = nk[f];
-    const double d = dk[f];
+    const int n = fdesc.kfar > 0 ? fdesc.nk : 0;
+    const double d = fdesc.dk;
     const cd c = C[f];
     const int i0 = blockIdx.x * (THREADS * ILP) + threadIdx.x + 1;
-    cd* row = rem + off[f];
+    cd* row = rem + fdesc.off;
     int bad = 0;
     double mre = 0.0, mim = 0.0;
     if (i0 <= n) {
         if (FORM == 0) {
             bool ok;
             const double k = (double)i0 * d;
-            cd u = direct_u(s_lc, nl, kTwoPi * freqs[f], k, mu_ref, ok);
+            cd u = direct_u(s_lc, nl, kTwoPi * fdesc.freq, k, mu_ref, ok);
             if (!ok) bad |= kStSingular;
             cd r = k * u - c;
             if (!finite_cd(r)) { bad |= kStNonfinite; r = mk(0.0); }
@@ -171,8 +178,7 @@ __global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict
 
 namespace {
 struct PropVariant {
-    void (*fn)(const LayerC*, int, const double*, const cd*, const int*, const double*, const int64_t*, const cd*,
-               double, cd*, int*, unsigned long long*);
+    void (*fn)(const LayerC*, const MediumP*, const FreqDesc*, const cd*, const cd*, cd*, int*, unsigned long long*);
     int threads, ilp;
 };
 const PropVariant kDunkinVariants[] = {
@@ -187,20 +193,20 @@ const PropVariant kDunkinVariants[] = {
 
 int prop_variant_count() { return (int)(sizeof(kDunkinVariants) / sizeof(kDunkinVariants[0])); }
 
-void launch_prop(cudaStream_t s, const LayerC* lc, int nl, const double* freqs, const cd* wc2, int nf,
-                 const int* nk, const double* dk, const int64_t* off, int max_nk, const cd* C, double mu_ref,
-                 int formulation, cd* rem, int* status, int variant, unsigned long long* rowmax) {
+void launch_prop(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2, int nf,
+                 int max_nk, const cd* C, int formulation, cd* rem, int* status, int variant,
+                 unsigned long long* rowmax) {
     if (nf <= 0 || max_nk <= 0) return;
     if (formulation == 0) {
         dim3 grid((max_nk + 127) / 128, nf);
-        k_prop<0, 128, 1, 1><<<grid, 128, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status, rowmax);
+        k_prop<0, 128, 1, 1><<<grid, 128, 0, s>>>(lc, media, fd, wc2, C, rem, status, rowmax);
         return;
     }
     if (variant < 0 || variant >= prop_variant_count()) variant = 0;
     const PropVariant& v = kDunkinVariants[variant];
     const int per_block = v.threads * v.ilp;
     dim3 grid((max_nk + per_block - 1) / per_block, nf);
-    v.fn<<<grid, v.threads, 0, s>>>(lc, nl, freqs, wc2, nk, dk, off, C, mu_ref, rem, status, rowmax);
+    v.fn<<<grid, v.threads, 0, s>>>(lc, media, fd, wc2, C, rem, status, rowmax);
 }
 
 // -------------------------------------------------------------- J0 table --
@@ -323,17 +329,17 @@ void launch_quad_gemm(cudaStream_t s, const cd* rem, const double* W, const cd* 
 
 __global__ __launch_bounds__(128) void k_quad_ragged(const cd* __restrict__ rem, const cd* __restrict__ C,
                                                      const double* __restrict__ ranges, int nf, int nr,
-                                                     const int* __restrict__ nk, const double* __restrict__ dk,
-                                                     const int64_t* __restrict__ off, cd* __restrict__ G) {
+                                                     const FreqDesc* __restrict__ fd, cd* __restrict__ G) {
     const int f = blockIdx.y;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nr) return;
-    const int n = nk[f];
-    const double d = dk[f];
+    const FreqDesc fdesc = fd[f];
+    const int n = fdesc.kfar > 0 ? fdesc.nk : 0;
+    const double d = fdesc.dk;
     const double r = ranges[j];
     const cd c = C[f];
     cd acc = c / r - (0.5 * d) * c;
-    const cd* row = rem + off[f];
+    const cd* row = rem + fdesc.off;
     for (int i = 1; i <= n; i++) {
         const double k = (double)i * d;
         const double w = i == n ? 0.5 : 1.0;
@@ -346,9 +352,10 @@ __global__ __launch_bounds__(128) void k_quad_ragged(const cd* __restrict__ rem,
 }
 
 void launch_quad_ragged(cudaStream_t s, const cd* rem, const cd* C, const double* ranges, int nf, int nr,
-                        const int* nk, const double* dk, const int64_t* off, cd* G) {
+                        const FreqDesc* fd, cd* G) {
+    if (nf <= 0) return;
     dim3 grid((nr + 127) / 128, nf);
-    k_quad_ragged<<<grid, 128, 0, s>>>(rem, C, ranges, nf, nr, nk, dk, off, G);
+    k_quad_ragged<<<grid, 128, 0, s>>>(rem, C, ranges, nf, nr, fd, G);
 }
 
 // ------------------------------------------------------------ bank pack --

@@ -8,17 +8,20 @@ namespace gfk {
 // Device status bits, mapped to gfk_status by the host.
 enum : int { kStSingular = 1, kStNonfinite = 2, kStTimeout = 4 };
 
-void launch_layer_consts(cudaStream_t s, const LayerP* layers, MediumP med, const double* freqs, int nf,
-                         double wi, double mu_ref, int formulation, LayerC* lc, cd* wc2);
+// Every kernel below serves nf rows described by fd[0..nf); a row's medium is
+// media[fd[f].soil], whose layers are lp[media[..].lp_off ..].
 
-void launch_static(cudaStream_t s, const LayerC* lc, int nl, const double* freqs, const cd* wc2,
-                   const double* kfar, int nf, double mu_ref, int formulation, cd* C, int* status);
+// lc[fd[f].lc_off + l] for every layer of the row's medium, and wc2[f].
+void launch_layer_consts(cudaStream_t s, const LayerP* lp, const MediumP* media, const FreqDesc* fd, int nf,
+                         double wi, int formulation, LayerC* lc, cd* wc2);
 
-// rem[off[f] + i - 1] = k_i u(k_i, f) - C_f for i = 1..nk[f], k_i = i dk[f].
+void launch_static(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2, int nf,
+                   int formulation, cd* C, int* status);
+
+// rem[fd[f].off + i - 1] = k_i u(k_i, f) - C_f for i = 1..nk, k_i = i dk.
 // `variant` picks one of prop_variant_count() launch shapes of the Dunkin kernel.
-void launch_prop(cudaStream_t s, const LayerC* lc, int nl, const double* freqs, const cd* wc2, int nf,
-                 const int* nk, const double* dk, const int64_t* off, int max_nk, const cd* C,
-                 double mu_ref, int formulation, cd* rem, int* status, int variant = 0,
+void launch_prop(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2, int nf,
+                 int max_nk, const cd* C, int formulation, cd* rem, int* status, int variant = 0,
                  unsigned long long* rowmax = nullptr);
 int prop_variant_count();
 
@@ -42,7 +45,7 @@ void launch_quad_gemm(cudaStream_t s, const cd* rem, const double* W, const cd* 
 
 // Per-frequency grids: the same sum with J0 evaluated in the loop.
 void launch_quad_ragged(cudaStream_t s, const cd* rem, const cd* C, const double* ranges, int nf, int nr,
-                        const int* nk, const double* dk, const int64_t* off, cd* G);
+                        const FreqDesc* fd, cd* G);
 
 void launch_bank_pack(cudaStream_t s, const cd* G, int nf, int nr, int first_bin, int bins, float* payload);
 

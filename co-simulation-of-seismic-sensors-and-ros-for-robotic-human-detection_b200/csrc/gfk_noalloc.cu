@@ -31,7 +31,7 @@ constexpr size_t kNoallocScratchBytes = size_t(4) << 20;
 // Layout of the scratch array (offsets in bytes, each 256-aligned).
 constexpr size_t kOffLayersP = 0;                                                  // LayerP[64]
 constexpr size_t kOffLayersC = 4096;                                               // LayerC[64]
-constexpr size_t kOffScalars = kOffLayersC + 64 * sizeof(gfk::LayerC);             // per-call scalars
+constexpr size_t kOffScalars = kOffLayersC + 64 * sizeof(gfk::LayerC);             // medium, row, scalars
 constexpr size_t kOffRanges = kOffScalars + 256;                                   // double[nr]
 constexpr size_t kOffG = kOffRanges + size_t(GFK_NOALLOC_MAX_RANGES) * 8;          // cd[nr]
 constexpr size_t kOffRem = kOffG + size_t(GFK_NOALLOC_MAX_RANGES) * 16;            // cd[nk]
@@ -40,15 +40,16 @@ static_assert(64 * sizeof(gfk::LayerP) <= kOffLayersC, "layer block too small");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
 
-// Per-call scalars, copied into the scratch array's scalar block.
+// Per-call values, copied into the scratch array's scalar block.
 struct Scalars {
-    double freq, dk, kfar;
-    int64_t off;
-    int nk;
+    gfk::MediumP medium;
+    gfk::FreqDesc row;
     int status;
+    int pad;
     cd wc2, C;
 };
 static_assert(sizeof(Scalars) <= 256, "scalar block too small");
+static_assert(offsetof(Scalars, row) % 8 == 0 && offsetof(Scalars, wc2) % 8 == 0, "alignment");
 
 std::mutex g_setup_mu;
 void* g_scratch_addr[256] = {nullptr};  // device address of the array, per device ordinal
@@ -111,36 +112,35 @@ extern "C" int gfk_vertical_displacement_multi_noalloc(const gfk_medium* m, cons
     }
     for (int j = 0; j < nr; j++) rmin = fmin(rmin, ranges_m[j]);
     Scalars sc{};
-    sc.freq = freq_hz;
-    sc.dk = g.kmax / g.samples;
-    sc.kfar = fmax(200 * (kTwoPi * freq_hz / slowest), 400 / rmin);  // fk.go:515-521
-    sc.off = 0;
-    sc.nk = g.samples;
+    sc.medium.ref_freq = m->ref_freq_hz;
+    sc.medium.default_q = m->default_q;
+    sc.medium.tau_sigma = m->sls_tau_sigma;
+    sc.medium.tau_eps = m->sls_tau_eps;
+    sc.medium.mu_ref = mu_ref;
+    sc.medium.count = m->count;
+    sc.medium.sls = (m->sls_tau_sigma > 0 && m->sls_tau_eps > 0) ? 1 : 0;
+    sc.medium.lp_off = 0;
+    sc.row.freq = freq_hz;
+    sc.row.dk = g.kmax / g.samples;
+    sc.row.kfar = fmax(200 * (kTwoPi * freq_hz / slowest), 400 / rmin);  // fk.go:515-521
+    sc.row.off = 0;
+    sc.row.lc_off = 0;
+    sc.row.nk = g.samples;
+    sc.row.soil = 0;
     sc.status = 0;  // the array keeps the last call's flags: cleared here
 
     auto* d_lp = reinterpret_cast<gfk::LayerP*>(base + kOffLayersP);
     auto* d_lc = reinterpret_cast<gfk::LayerC*>(base + kOffLayersC);
     unsigned char* sb = base + kOffScalars;
     auto* d_sc = reinterpret_cast<Scalars*>(sb);
-    auto* d_freq = reinterpret_cast<double*>(sb + offsetof(Scalars, freq));
-    auto* d_dk = reinterpret_cast<double*>(sb + offsetof(Scalars, dk));
-    auto* d_kfar = reinterpret_cast<double*>(sb + offsetof(Scalars, kfar));
-    auto* d_off = reinterpret_cast<int64_t*>(sb + offsetof(Scalars, off));
-    auto* d_nk = reinterpret_cast<int*>(sb + offsetof(Scalars, nk));
+    auto* d_medium = reinterpret_cast<gfk::MediumP*>(sb + offsetof(Scalars, medium));
+    auto* d_row = reinterpret_cast<gfk::FreqDesc*>(sb + offsetof(Scalars, row));
     auto* d_status = reinterpret_cast<int*>(sb + offsetof(Scalars, status));
     auto* d_wc2 = reinterpret_cast<cd*>(sb + offsetof(Scalars, wc2));
     auto* d_C = reinterpret_cast<cd*>(sb + offsetof(Scalars, C));
     auto* d_r = reinterpret_cast<double*>(base + kOffRanges);
     auto* d_G = reinterpret_cast<cd*>(base + kOffG);
     auto* d_rem = reinterpret_cast<cd*>(base + kOffRem);
-
-    gfk::MediumP mp;
-    mp.ref_freq = m->ref_freq_hz;
-    mp.default_q = m->default_q;
-    mp.tau_sigma = m->sls_tau_sigma;
-    mp.tau_eps = m->sls_tau_eps;
-    mp.count = m->count;
-    mp.sls = (m->sls_tau_sigma > 0 && m->sls_tau_eps > 0) ? 1 : 0;
 
     cudaError_t e = cudaSuccess;
     auto ok = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
@@ -149,11 +149,10 @@ extern "C" int gfk_vertical_displacement_multi_noalloc(const gfk_medium* m, cons
     ok(cudaMemcpyAsync(d_r, ranges_m, sizeof(double) * nr, cudaMemcpyHostToDevice, strm));
     if (e != cudaSuccess) return GFK_ECUDA;
     const int form = s->formulation;
-    gfk::launch_layer_consts(strm, d_lp, mp, d_freq, 1, s->omega_imag, mu_ref, form, d_lc, d_wc2);
-    gfk::launch_static(strm, d_lc, m->count, d_freq, d_wc2, d_kfar, 1, mu_ref, form, d_C, d_status);
-    gfk::launch_prop(strm, d_lc, m->count, d_freq, d_wc2, 1, d_nk, d_dk, d_off, g.samples, d_C, mu_ref, form, d_rem,
-                     d_status);
-    gfk::launch_quad_ragged(strm, d_rem, d_C, d_r, 1, nr, d_nk, d_dk, d_off, d_G);
+    gfk::launch_layer_consts(strm, d_lp, d_medium, d_row, 1, s->omega_imag, form, d_lc, d_wc2);
+    gfk::launch_static(strm, d_lc, d_medium, d_row, d_wc2, 1, form, d_C, d_status);
+    gfk::launch_prop(strm, d_lc, d_medium, d_row, d_wc2, 1, g.samples, d_C, form, d_rem, d_status);
+    gfk::launch_quad_ragged(strm, d_rem, d_C, d_r, 1, nr, d_row, d_G);
     ok(cudaGetLastError());
     int flags = 0;
     ok(cudaMemcpyAsync(out, d_G, sizeof(cd) * nr, cudaMemcpyDeviceToHost, strm));

@@ -31,9 +31,25 @@ struct LayerP {
     double h, vp, vs, rho, qs, qp;
 };
 
+// One medium of a plan: fk.Medium's defaults plus what the kernels derive.
 struct MediumP {
     double ref_freq, default_q, tau_sigma, tau_eps;
-    int count, sls;
+    double mu_ref;  // max rho Vs^2 (fk.go:216-222)
+    int count;      // stack entries, the last one the half-space
+    int sls;        // nonzero: SLS relaxation replaces constant Q
+    int lp_off;     // first layer in the plan's LayerP table
+    int pad;
+};
+
+// One frequency of a plan (a bank row).
+struct FreqDesc {
+    double freq;     // Hz
+    double dk;       // wavenumber step; k_i = i dk, i = 1..nk
+    double kfar;     // k of the static coefficient (fk.go:515-521); 0 skips the row
+    int64_t off;     // integrand row offset within its chunk
+    int64_t lc_off;  // first of the row's layer constants
+    int nk;          // wavenumber samples
+    int soil;        // index into the medium table
 };
 
 GFK_HD double q_of(const MediumP& m, const LayerP& l) {  // fk.go:67-75

@@ -280,6 +280,7 @@ class Plan:
     recomputes everything on the device per execute()."""
 
     def __init__(self, medium, ranges, freqs, opt=None, engine=None):
+        self.p = None
         self.engine = engine or medium.engine or default_engine()
         self.ranges = np.ascontiguousarray(ranges, dtype=np.float64)
         self.freqs = np.ascontiguousarray(freqs, dtype=np.float64)
@@ -292,6 +293,10 @@ class Plan:
         self.engine.check(st)
         self.p = h
         self.engine._plans.add(self)
+
+    def use_graph(self, enable=True):
+        """From the next execute on, run each execute as one captured CUDA graph."""
+        self.engine.check(N.lib().gfk_plan_use_graph(self.p, 1 if enable else 0))
 
     def execute(self):
         self.engine.check(N.lib().gfk_plan_execute(self.p))
@@ -337,6 +342,41 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+class Batch(Plan):
+    """gfk_batch_create: one plan over many media, each with its own
+    frequencies, sharing ranges, integration and solve options (taken from
+    the first medium). Rows are ordered medium by medium."""
+
+    def __init__(self, media, freqs_per_medium, ranges, opt=None, engine=None):
+        self.p = None
+        media = list(media)
+        if not media:
+            raise FkError(N.EARG, "no media given")
+        self.engine = engine or media[0].engine or default_engine()
+        self.ranges = np.ascontiguousarray(ranges, dtype=np.float64)
+        self._freqs = [np.ascontiguousarray(f, dtype=np.float64) for f in freqs_per_medium]
+        if len(self._freqs) != len(media):
+            raise FkError(N.EARG, "one frequency list per medium")
+        self.freqs = np.concatenate(self._freqs) if self._freqs else np.zeros(0)
+        self.counts = np.array([len(f) for f in self._freqs], dtype=np.int64)
+        opt = opt or Integration()
+        holders = [_c_medium(m) for m in media]
+        arr = (N.GfkMedium * len(media))(*[h.c for h in holders])
+        fptrs = (ctypes.POINTER(ctypes.c_double) * len(media))(*[_dp(f) for f in self._freqs])
+        nfs = (ctypes.c_int32 * len(media))(*[len(f) for f in self._freqs])
+        h = ctypes.c_void_p()
+        st = N.lib().gfk_batch_create(self.engine.ctx, arr, len(media), fptrs, nfs, ctypes.byref(media[0]._solve()),
+                                      _dp(self.ranges), len(self.ranges), opt.c(), ctypes.byref(h))
+        del holders
+        self.engine.check(st)
+        self.p = h
+        self.engine._plans.add(self)
+
+    def split(self, rows):
+        """Splits a [sum nf, ...] result into one array per medium."""
+        return np.split(rows, np.cumsum(self.counts)[:-1])
 
 
 # ----------------------------------------------------------------- plumbing --

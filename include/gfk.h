@@ -209,6 +209,20 @@ int gfk_plan_tuning(const gfk_plan *p, int32_t *variant, float *ms_per_variant, 
 int gfk_plan_kernel_times(gfk_plan *p, double *prop_ms, double *quad_ms,
                           double *other_ms, int32_t reset);
 int gfk_plan_destroy(gfk_plan *p);
+/* enable != 0: from the second execute on, the whole execute (every launch of
+ * every row chunk) is one CUDA graph, captured once and relaunched. */
+int gfk_plan_use_graph(gfk_plan *p, int32_t enable);
+
+/* A plan over many media at once — the batched form of cmd/geobank's loop
+ * (cmd/geobank/main.go:133-167) across soils: medium i contributes the rows
+ * (medium i, freqs_hz[i][0..nf[i])). Rows are ordered medium by medium; the
+ * result of gfk_plan_download is [sum nf][nr] (re, im) pairs in that order,
+ * with per-row status. A medium that fails validation marks its rows and
+ * takes no device work. All media share the ranges and the integration. */
+int gfk_batch_create(gfk_ctx *ctx, const gfk_medium *media, int32_t nsoil,
+                     const double *const *freqs_hz, const int32_t *nf,
+                     const gfk_solve *s, const double *ranges_m, int32_t nr,
+                     gfk_integration opt, gfk_plan **out);
 
 /* ---- allocation-free variant --------------------------------------------- */
 /* No counterpart in the reference: a gfk_vertical_displacement_multi for

@@ -281,3 +281,53 @@ def test_split_quadrature_refuses_per_frequency_grids(gfk, engine):
     with pytest.raises(gfk.FkError) as e:
         m.bank_spectra([1.0, 2.0], [10.0, 20.0])
     assert e.value.status == gfk._native.EARG
+
+
+def test_batch_of_uneven_soils_matches_single_plans(gfk, engine, oracle):
+    """Media with different layer counts and frequency lists in one batch give
+    the rows each medium gives on its own; a medium that fails validation
+    marks only its own rows."""
+    soils, ranges, nk, kmax = gfk.workloads.batched_soils(count=6, seed=11)
+    ranges = ranges[::4]
+    opt = gfk.Integration(2048, 0.0, kmax)
+    media, freqs = [], []
+    for st, fr in soils:
+        media.append(gfk.Medium(st, formulation=gfk.DUNKIN, omega_imag=1.5, engine=engine))
+        freqs.append(fr[::97])
+    bad = gfk.Medium(gfk.Stack([gfk.Layer(0, 100, 200, 1700)]), formulation=gfk.DUNKIN, omega_imag=1.5,
+                     engine=engine)
+    media.insert(2, bad)
+    freqs.insert(2, np.array([10.0, 20.0]))
+    for quad in (gfk.PLAIN_FP64, gfk.SPLIT_INT8):
+        for m in media:
+            m.quadrature = quad
+        b = gfk.Batch(media, freqs, ranges, opt, engine=engine)
+        b.execute()
+        got, status = b.download(raise_on_error=False)
+        parts, stats = b.split(got), b.split(status)
+        assert (stats[2] == gfk._native.ESTACK).all()
+        for i, (m, fr) in enumerate(zip(media, freqs)):
+            if i == 2:
+                continue
+            assert (stats[i] == 0).all()
+            want, _ = m.bank_spectra(ranges, fr, opt)
+            assert rel_l2(parts[i], want) < 1e-12
+        st0 = soils[0][0]
+        w0, _ = oracle.bank_spectra(as_tuples(st0), ranges, freqs[0], samples=2048, kmax=kmax,
+                                    formulation=oracle.DUNKIN, omega_imag=1.5)
+        assert rel_l2(parts[0], w0) < 1e-6
+        b.close()
+
+
+def test_graph_execute_matches_stream_execute(gfk, engine):
+    wl = gfk.workloads.single_soil()
+    m = wl.medium(gfk.DUNKIN, engine=engine, quadrature=gfk.SPLIT_INT8)
+    p = gfk.Plan(m, wl.ranges, wl.freqs, wl.integration(), engine=engine)
+    p.execute()
+    a, _ = p.download()
+    p.use_graph(True)
+    p.execute()  # captures
+    p.execute()  # relaunches
+    b, _ = p.download()
+    assert np.array_equal(a, b)
+    p.close()
