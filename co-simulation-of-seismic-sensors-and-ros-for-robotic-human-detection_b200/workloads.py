@@ -111,3 +111,20 @@ def batched_soils(count=4096, seed=20240611):
     ranges = np.arange(1, 129, dtype=np.float64)
     kmax = 2.5 * 2 * math.pi * 500.0 / 80.0
     return soils, ranges, 8192, kmax
+
+
+def shard(units, rank, world):
+    """The units (e.g. (stack, freqs) soils) one rank of `world` builds:
+    greedy longest-processing-time assignment on the cost rows x layers, so
+    ranks finish together; deterministic, every rank computes the same split."""
+    if world <= 1:
+        return list(units)
+    cost = [len(fr) * len(st) for st, fr in units]
+    order = sorted(range(len(units)), key=lambda i: (-cost[i], i))
+    load = [0] * world
+    owner = [0] * len(units)
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[i] = r
+        load[r] += cost[i]
+    return [u for i, u in enumerate(units) if owner[i] == rank]
