@@ -437,7 +437,6 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
             if (st) {
                 p->host_status[row] = st;
                 if (first_msg.empty()) first_msg = ctx->last_error;
-                shared = false;
                 continue;  // kfar = 0: no device work for this row
             }
             lc_total += m->count;
@@ -473,13 +472,14 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
         }
         p->tc = p->shared;
     }
-    // row chunks bounded by the integrand budget and the grid limit
+    // row chunks bounded by the integrand budget and the grid limit; on a shared
+    // grid every row keeps its dense slot (row x Nk), failed rows included
     const int64_t budget = kDefaultRemBudget / (int64_t)sizeof(cd);
     int64_t acc = 0, cap = 0;
     int rows_in = 0, cmax = 0;
     p->chunk_begin.push_back(0);
     for (int f = 0; f < p->nf; f++) {
-        const int nk = p->fd[f].kfar > 0 ? p->fd[f].nk : 0;
+        const int nk = p->shared ? p->g_n : (p->fd[f].kfar > 0 ? p->fd[f].nk : 0);
         if (rows_in > 0 && (acc + nk > budget || rows_in >= kMaxChunkRows)) {
             p->chunk_begin.push_back(f);
             p->chunk_max_nk.push_back(cmax);

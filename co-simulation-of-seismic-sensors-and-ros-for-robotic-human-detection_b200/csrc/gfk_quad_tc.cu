@@ -332,11 +332,14 @@ __global__ void k_slice_rem(const cd* __restrict__ rem, int nk, int Kp, int Mp, 
         row_exp[2 * f] = e[0];
         row_exp[2 * f + 1] = e[1];
     }
+    // a row with no device work (its maximum stayed 0) slices to zeros
+    // without reading its integrand slot
+    const bool live = rowmax[2 * f] != 0 || rowmax[2 * f + 1] != 0;
     alignas(16) int8_t out[2][4][16];
 #pragma unroll 4
     for (int i = 0; i < 16; i++) {
         const int k = k0 + i;
-        const cd v = k < nk ? rem[(size_t)f * nk + k] : mk(0.0);
+        const cd v = (live && k < nk) ? rem[(size_t)f * nk + k] : mk(0.0);
         int8_t d[4];
         digits4(v.re * sc[0], d);
 #pragma unroll
