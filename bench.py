@@ -299,6 +299,32 @@ def run_batched(args, gfk, torch, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_sobol(args, gfk, torch, rank, world, local):
+    """The all-plain Sobol run: N(d+2) soils, each through the GPU f-k solve at
+    10 m (512 bins, 8192 wavenumbers), traces, metrics, indices. One step is
+    the whole run; ranks would split the soils (weak scaling in soils)."""
+    S = gfk.sobol
+    eng = gfk.Engine(local)
+    t0 = time.perf_counter()
+    res = S.run_plain(eng, n=args.sobol_n, seed=0)
+    wall = time.perf_counter() - t0
+    eng.close()
+    if rank == 0:
+        cells = res.seconds["rows"]
+        out = {"metric": METRIC, "value": cells / res.seconds["solve_gpu"], "unit": UNIT, "n_gpus": world,
+               "steps": 1, "warmup": 0, "ms_per_step": 1e3 * res.seconds["solve_gpu"], "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": f"sobol plain: Saltelli N={args.sobol_n}, d=8 soil parameters, "
+                                      f"{res.seconds['soils']} soils x 512 bins at 10 m, 8192 wavenumbers, "
+                                      "75 kg footstep through an SM-24-like geophone (10 Hz, 0.7)",
+                          "soils": res.seconds["soils"], "rows": cells},
+               "e2e": {"value": cells / wall, "unit": UNIT, "s_per_run": wall,
+                       "h2d_bytes_per_step": res.seconds["soils"] * 3 * 48, "d2h_bytes_per_step": cells * 16},
+               "sobol": {"S1": res.s1, "ST": res.st,
+                         "seconds": {k: v for k, v in res.seconds.items() if k not in ("rows", "soils")}}}
+        print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -308,8 +334,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--freq-stride", type=int, default=1,
                     help="profiling only: keep every n-th frequency (a smaller case of the same kernels)")
-    ap.add_argument("--workload", default="graded", choices=["graded", "batched"],
-                    help="graded: the 10-layer graded soil (default); batched: seeded uneven soils")
+    ap.add_argument("--workload", default="graded", choices=["graded", "batched", "sobol"],
+                    help="graded: the 10-layer graded soil (default); batched: seeded uneven soils; "
+                         "sobol: the all-plain Sobol run")
+    ap.add_argument("--sobol-n", type=int, default=16384, help="sobol workload: Saltelli base size N")
     ap.add_argument("--soils", type=int, default=4096, help="batched workload: number of soils")
     ap.add_argument("--quadrature", default="split", choices=["split", "fp64"],
                     help="split: exact int8-slice tensor-core sum (default); fp64: the plain FP64 sum")
@@ -326,6 +354,8 @@ def main():
     gfk = __graft_entry__.load_package()
     if args.workload == "batched":
         return run_batched(args, gfk, torch, rank, world, local)
+    if args.workload == "sobol":
+        return run_sobol(args, gfk, torch, rank, world, local)
     wl = gfk.workloads.graded_soil()
     if args.freq_stride > 1:
         wl.freqs = wl.freqs[::args.freq_stride].copy()

@@ -10,7 +10,8 @@ from .fk import (Batch, Engine, FkError, Grid, Integration, Layer, MAX_LAYER_PHA
                  default_engine, uniform)
 from .bank import (Bank, Header, Provenance, RangeGrid, build_bank, open_bank, range_nyquist)
 from . import workloads
+from . import sobol
 
 __all__ = ["Batch", "Engine", "FkError", "Grid", "Integration", "Layer", "MAX_LAYER_PHASE", "Medium", "Plan", "SLS",
            "Stack", "default_engine", "uniform", "Bank", "Header", "Provenance", "RangeGrid", "build_bank",
-           "open_bank", "range_nyquist", "workloads", "DUNKIN", "REFERENCE_DIRECT", "PLAIN_FP64", "SPLIT_INT8"]
+           "open_bank", "range_nyquist", "workloads", "sobol", "DUNKIN", "REFERENCE_DIRECT", "PLAIN_FP64", "SPLIT_INT8"]

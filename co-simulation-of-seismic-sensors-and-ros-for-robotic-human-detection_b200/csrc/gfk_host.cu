@@ -216,6 +216,9 @@ struct gfk_plan {
     gfk::LayerC* d_lc = nullptr;
     cd *d_wc2 = nullptr, *d_C = nullptr, *d_rem = nullptr, *d_G = nullptr;
     int* d_status = nullptr;
+    // fused propagator + sum for a few ranges (no integrand in HBM)
+    bool fused = false;
+    cd* d_partial = nullptr;
     // split (tensor-core) quadrature
     bool tc = false;
     int Mp = 0, Np = 0, Kp = 0, col_exp = 0;
@@ -247,7 +250,7 @@ void plan_free(gfk_plan* p) {
     if (p->gexec) cudaGraphExecDestroy(p->gexec);
     void* ptrs[] = {p->d_lp,  p->d_media, p->d_fd, p->d_ranges, p->d_W, p->d_lc,     p->d_wc2,
                     p->d_C,   p->d_rem,   p->d_G,  p->d_status, p->d_A, p->d_B,      p->d_rowexp,
-                    p->d_rowmax};
+                    p->d_rowmax, p->d_partial};
     for (void* q : ptrs)
         if (q) cudaFreeAsync(q, s);
     for (auto& sg : p->segs) {
@@ -472,6 +475,11 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
         }
         p->tc = p->shared;
     }
+    // a few ranges on a shared grid: fuse the sum into the Dunkin propagator
+    if (p->shared && s->formulation == GFK_DUNKIN && nr <= gfk::fused_max_ranges() && mode == kGridMulti) {
+        p->fused = true;
+        p->tc = false;
+    }
     // row chunks bounded by the integrand budget and the grid limit; on a shared
     // grid every row keeps its dense slot (row x Nk), failed rows included
     const int64_t budget = kDefaultRemBudget / (int64_t)sizeof(cd);
@@ -510,7 +518,15 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
     if (!st) st = dalloc(ctx, &p->d_C, nfa);
     if (!st) st = dalloc(ctx, &p->d_G, nfa * nr);
     if (!st) st = dalloc(ctx, &p->d_status, nfa);
-    if (!st) st = dalloc(ctx, &p->d_rem, (size_t)std::max<int64_t>(cap, 1));
+    if (p->fused) {
+        int max_cnf = 0;
+        for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
+            max_cnf = std::max(max_cnf, p->chunk_begin[c + 1] - p->chunk_begin[c]);
+        const int nkb = (g_n + 127) / 128;
+        if (!st) st = dalloc(ctx, &p->d_partial, (size_t)max_cnf * nkb * nr);
+    } else if (!st) {
+        st = dalloc(ctx, &p->d_rem, (size_t)std::max<int64_t>(cap, 1));
+    }
     if (!st && p->shared && !p->tc) st = dalloc(ctx, &p->d_W, (size_t)g_n * nr);
     if (!st && p->tc) {
         int max_cnf = 0;
@@ -542,6 +558,7 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
     for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
         if (p->chunk_begin[c + 1] > p->chunk_begin[c]) nchunks++;
     p->launches_per_exec = p->nf > 0 ? (p->tc ? 3 + 3 * nchunks : 2 + 2 * nchunks + (p->shared ? 1 : 0)) : 0;
+    if (p->fused) p->prop_variant = 0;  // one launch shape; nothing to tune
     *out = p;
     return GFK_OK;
 }
@@ -628,6 +645,15 @@ int plan_enqueue(gfk_plan* p, bool timed) {
         const int cnf = fe - fb;
         if (cnf <= 0) continue;
         const int cmax = p->chunk_max_nk[c];
+        if (p->fused) {
+            if (timed && (st = begin_seg(p, 0, &seg))) return st;
+            gfk::launch_prop_fused(s, p->d_lc, p->d_media, p->d_fd + fb, p->d_wc2 + fb, cnf, p->g_n, p->d_C + fb,
+                                   p->d_W, p->d_ranges, p->nr, p->d_partial, p->d_status + fb,
+                                   p->d_G + (size_t)fb * p->nr);
+            if (timed && (st = end_seg(p, seg))) return st;
+            ctx->launches += 2;
+            continue;
+        }
         if (p->tc) GFK_CUDA(ctx, cudaMemsetAsync(p->d_rowmax, 0, sizeof(unsigned long long) * 2 * cnf, s));
         if (timed && (st = begin_seg(p, 0, &seg))) return st;
         gfk::launch_prop(s, p->d_lc, p->d_media, p->d_fd + fb, p->d_wc2 + fb, cnf, cmax, p->d_C + fb, form, p->d_rem,

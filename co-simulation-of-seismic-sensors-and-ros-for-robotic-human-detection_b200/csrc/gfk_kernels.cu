@@ -209,6 +209,105 @@ void launch_prop(cudaStream_t s, const LayerC* lc, const MediumP* media, const F
     v.fn<<<grid, v.threads, 0, s>>>(lc, media, fd, wc2, C, rem, status, rowmax);
 }
 
+// ------------------------------------------------- fused propagator + sum --
+//
+// For a handful of ranges the wavenumber sum is a dot product per range: each
+// thread multiplies its integrand value k u - C by the Hankel weights
+// W[k][0..nr), the block reduces over its 128 wavenumbers in shared memory in
+// a fixed order, and one partial per (row, k block, range) is written. The
+// integrand never reaches HBM; k_fused_finish adds the partials in block
+// order (deterministic) and the closed k = 0 panel (fk.go:529-532).
+
+constexpr int kFuseThreads = 128;
+
+template <int NR>
+__global__ __launch_bounds__(kFuseThreads, 4) void k_prop_fused(const LayerC* __restrict__ lc,
+                                                                const MediumP* __restrict__ media,
+                                                                const FreqDesc* __restrict__ fd,
+                                                                const cd* __restrict__ wc2, const cd* __restrict__ C,
+                                                                const double* __restrict__ W, int nr, int nkb,
+                                                                cd* __restrict__ partial, int* __restrict__ status) {
+    __shared__ LayerC s_lc[kMaxLayers];
+    __shared__ double s_red[2 * NR][kFuseThreads / 32];
+    const int f = blockIdx.y;
+    const FreqDesc fdesc = fd[f];
+    const MediumP med = media[fdesc.soil];
+    const int nl = med.count;
+    for (int l = threadIdx.x; l < nl; l += blockDim.x) s_lc[l] = lc[fdesc.lc_off + l];
+    __syncthreads();
+    const int n = fdesc.kfar > 0 ? fdesc.nk : 0;
+    const int i = blockIdx.x * kFuseThreads + threadIdx.x + 1;
+    cd r = mk(0.0);
+    if (i <= n) {
+        const double k = (double)i * fdesc.dk;
+        r = k * dunkin_u(s_lc, nl, wc2[f], k, med.mu_ref) - C[f];
+        if (!finite_cd(r)) {
+            atomicOr(status + f, kStNonfinite);
+            r = mk(0.0);
+        }
+    }
+    double acc[2 * NR];
+#pragma unroll
+    for (int j = 0; j < NR; j++) {
+        const double w = (i <= n && j < nr) ? W[(size_t)(i - 1) * nr + j] : 0.0;
+        acc[2 * j] = r.re * w;
+        acc[2 * j + 1] = r.im * w;
+    }
+    // warp tree, then the block's warps in order: a fixed summation order
+#pragma unroll
+    for (int q = 0; q < 2 * NR; q++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], o);
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int q = 0; q < 2 * NR; q++) s_red[q][warp] = acc[q];
+    __syncthreads();
+    if (threadIdx.x < nr) {
+        const int j = threadIdx.x;
+        double re = 0.0, im = 0.0;
+#pragma unroll
+        for (int w = 0; w < kFuseThreads / 32; w++) {
+            re += s_red[2 * j][w];
+            im += s_red[2 * j + 1][w];
+        }
+        partial[((size_t)f * nkb + blockIdx.x) * nr + j] = mk(re, im);
+    }
+}
+
+__global__ void k_fused_finish(const cd* __restrict__ partial, const cd* __restrict__ C,
+                               const double* __restrict__ ranges, const FreqDesc* __restrict__ fd, int nf, int nr,
+                               int nkb, cd* __restrict__ G) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nf * nr) return;
+    const int f = (int)(t / nr), j = (int)(t - (int64_t)f * nr);
+    const cd c = C[f];
+    const double d = fd[f].dk;
+    cd acc = c / ranges[j] - (0.5 * d) * c;
+    for (int b = 0; b < nkb; b++) acc += partial[((size_t)f * nkb + b) * nr + j];
+    G[(size_t)f * nr + j] = acc;
+}
+
+int fused_max_ranges() { return 8; }
+
+void launch_prop_fused(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2,
+                       int nf, int nk, const cd* C, const double* W, const double* ranges, int nr, cd* partial,
+                       int* status, cd* G) {
+    if (nf <= 0 || nk <= 0 || nr <= 0 || nr > 8) return;
+    const int nkb = (nk + kFuseThreads - 1) / kFuseThreads;
+    dim3 grid(nkb, nf);
+    if (nr <= 1)
+        k_prop_fused<1><<<grid, kFuseThreads, 0, s>>>(lc, media, fd, wc2, C, W, nr, nkb, partial, status);
+    else if (nr <= 2)
+        k_prop_fused<2><<<grid, kFuseThreads, 0, s>>>(lc, media, fd, wc2, C, W, nr, nkb, partial, status);
+    else if (nr <= 4)
+        k_prop_fused<4><<<grid, kFuseThreads, 0, s>>>(lc, media, fd, wc2, C, W, nr, nkb, partial, status);
+    else
+        k_prop_fused<8><<<grid, kFuseThreads, 0, s>>>(lc, media, fd, wc2, C, W, nr, nkb, partial, status);
+    const int64_t nt = (int64_t)nf * nr;
+    k_fused_finish<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(partial, C, ranges, fd, nf, nr, nkb, G);
+}
+
 // -------------------------------------------------------------- J0 table --
 
 __global__ void k_j0_table(const double* __restrict__ ranges, int nr, int nk, double dk, double* __restrict__ W) {

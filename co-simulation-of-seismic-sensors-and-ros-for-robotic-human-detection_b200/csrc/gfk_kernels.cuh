@@ -36,6 +36,13 @@ void launch_slice_rem(cudaStream_t s, const cd* rem, int nk, int Kp, int Mp, int
 int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int N, int Mp, int Np, int Kp,
                    const int* row_exp, int col_exp, const cd* C, const double* ranges, double dk, cd* G, int* status);
 
+// Shared grid, nr <= fused_max_ranges(): propagator and wavenumber sum in one
+// pass (the integrand stays on chip); partial holds nf x ceil(nk/128) x nr.
+int fused_max_ranges();
+void launch_prop_fused(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2,
+                       int nf, int nk, const cd* C, const double* W, const double* ranges, int nr, cd* partial,
+                       int* status, cd* G);
+
 // W[(i-1) nr + j] = w_i J0(k_i r_j) dk, w = 1/2 at i = nk.
 void launch_j0_table(cudaStream_t s, const double* ranges, int nr, int nk, double dk, double* W);
 

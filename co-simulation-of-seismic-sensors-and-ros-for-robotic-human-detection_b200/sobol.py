@@ -1,0 +1,297 @@
+"""Sobol sensitivity of footstep metrics to the soil, with every soil's
+Green's function at the sensor solved on the GPU.
+
+The Sobol workload: a Saltelli design over 8 soil parameters (two finite
+layers' Vs, Vp/Vs and Qs, the top layer's thickness and the half-space Vs),
+N(d+2) soils; for each, the vertical velocity at 10 m from one footstep
+(double-hump ground reaction force: 75 kg, 1.2 body-weight peaks, 30 ms
+heel-strike rise) through an SM-24-like geophone (10 Hz, damping 0.7) is
+reduced to its peak and its 2-400 Hz spectral centroid, and first-order and
+total indices are estimated.
+
+Restated on the host (cheap, O(soils x samples)):
+  saltelli / indices / bootstrap   py/analysis/sobol.py:44-99
+  Stance (GRF profile)             internal/grf/grf.go:34-330
+  Geophone response                internal/geophone/geophone.go:36-203
+  measure (peak, centroid)         internal/sweep/sweep.go:128-169
+  causal taper above 0.8 Nyquist   internal/dsp/dsp.go:232-261
+The banks (the f-k solve, all of the cost) run in libgfk as batches.
+
+Choices the workload statement leaves open, fixed here: layer 2 is 2 m
+thick; densities are 1700, 1850 and 2000 kg/m^3 (top, layer 2, half-space);
+the half-space has Vp/Vs = 2, Qs = 40; every layer has Qp = 2 Qs; the trace is
+1024 samples at 1 kHz (bins 1..512 solved), heel strike 50 ms in; the solve
+uses the complex frequency offset w_I = pi/T (T = 1.024 s), undone after the
+inverse transform; wavenumbers: 8192 to k_max = 2.5 w_max/80 m/s.
+"""
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .fk import Batch, Integration, Layer, Medium, Stack
+from . import _native as N
+
+# ------------------------------------------------------------------ design --
+
+# (name, low, high, log-scaled)
+PARAMS = [
+    ("vs1", 80.0, 600.0, True),
+    ("vpvs1", 1.7, 3.0, False),
+    ("qs1", 10.0, 60.0, False),
+    ("vs2", 80.0, 600.0, True),
+    ("vpvs2", 1.7, 3.0, False),
+    ("qs2", 10.0, 60.0, False),
+    ("h1", 0.2, 5.0, True),
+    ("vs_hs", 80.0, 600.0, True),
+]
+
+
+def saltelli(n, k, seed=0):
+    """(N(k+2), k) unit-cube design, blocks A, B, AB_0..AB_{k-1}
+    (py/analysis/sobol.py:44-57): A and B from one scrambled Sobol sequence of
+    dimension 2k."""
+    from scipy.stats import qmc
+    sample = qmc.Sobol(d=2 * k, scramble=True, seed=seed).random(n)
+    a, b = sample[:, :k], sample[:, k:]
+    blocks = [a, b]
+    for i in range(k):
+        ab = a.copy()
+        ab[:, i] = b[:, i]
+        blocks.append(ab)
+    return np.vstack(blocks)
+
+
+def indices(y, n, k):
+    """First-order (Saltelli 2010) and total (Jansen 1999) indices
+    (py/analysis/sobol.py:60-79)."""
+    ya, yb = y[:n], y[n:2 * n]
+    var = np.var(np.concatenate([ya, yb]), ddof=1)
+    if var == 0:
+        return np.zeros(k), np.zeros(k)
+    s1, st = np.empty(k), np.empty(k)
+    for i in range(k):
+        yab = y[(i + 2) * n:(i + 3) * n]
+        s1[i] = np.mean(yb * (yab - ya)) / var
+        st[i] = np.mean((ya - yab) ** 2) / (2 * var)
+    return s1, st
+
+
+def bootstrap(y, n, k, draws=400, seed=0):
+    """5-95% intervals, resampling matched rows across every block
+    (py/analysis/sobol.py:82-99)."""
+    rng = np.random.default_rng(seed)
+    s1s, sts = np.empty((draws, k)), np.empty((draws, k))
+    for d in range(draws):
+        idx = rng.integers(0, n, n)
+        resampled = np.concatenate([y[b * n:(b + 1) * n][idx] for b in range(k + 2)])
+        s1s[d], sts[d] = indices(resampled, n, k)
+    return np.percentile(s1s, [5, 95], axis=0), np.percentile(sts, [5, 95], axis=0)
+
+
+def unit_to_params(u):
+    """Maps the unit cube to parameter values (log-uniform where marked)."""
+    out = np.empty_like(u)
+    for j, (_, lo, hi, log) in enumerate(PARAMS):
+        out[:, j] = np.exp(np.log(lo) + u[:, j] * (np.log(hi) - np.log(lo))) if log else lo + u[:, j] * (hi - lo)
+    return out
+
+
+def soil_of(p):
+    """The stack for one parameter row."""
+    vs1, r1, q1, vs2, r2, q2, h1, vsh = (float(x) for x in p)
+    return Stack([Layer(h1, r1 * vs1, vs1, 1700.0, q1, 2 * q1),
+                  Layer(2.0, r2 * vs2, vs2, 1850.0, q2, 2 * q2),
+                  Layer(0.0, 2.0 * vsh, vsh, 2000.0, 40.0, 80.0)])
+
+
+# ------------------------------------------------------------------ source --
+
+@dataclass
+class Stance:
+    """grf.Stance (internal/grf/grf.go:34-105): vertical GRF of one stance."""
+    mass: float = 75.0
+    duration: float = 0.62
+    first_peak: float = 1.2
+    second_peak: float = 1.2
+    valley: float = 0.75
+    hump_width: float = 0.11          # defaultHumpWidth
+    transient_peak: float = 0.35      # defaultTransientPeak
+    transient_rise: float = 0.030
+    taper: float = 0.098              # defaultTaperFraction
+
+    def body_weight(self):
+        return self.mass * 9.80665
+
+    def profile(self, tau):
+        """ProfileAt (grf.go:280-300) in body weights, vectorised."""
+        tau = np.asarray(tau, dtype=np.float64)
+        inside = (tau > 0) & (tau < 1)
+        w = self.hump_width
+        g1 = np.exp(-((tau - 0.25) / w) ** 2)
+        g2 = np.exp(-((tau - 0.75) / w) ** 2)
+        body = self.valley + (self.first_peak - self.valley) * g1 + (self.second_peak - self.valley) * g2
+        r = self.taper
+        tuk = np.where(tau < r, 0.5 * (1 - np.cos(np.pi * tau / r)),
+                       np.where(tau > 1 - r, 0.5 * (1 - np.cos(np.pi * (1 - tau) / r)), 1.0))
+        # transientAt (grf.go:230-240): a damped sine from heel contact
+        crest, crest_phase = 0.63790, 0.20090
+        period = self.transient_rise / crest_phase / self.duration
+        decay = period / 2
+        tr = np.where(tau > 0, self.transient_peak / crest * np.exp(-np.maximum(tau, 0) / decay)
+                      * np.sin(2 * np.pi * tau / period), 0.0)
+        return np.where(inside, tuk * body + tr, 0.0)
+
+    def force(self, fs, n, lead):
+        """ForceAt on n samples at fs, heel strike at `lead` seconds (newtons)."""
+        t = np.arange(n) / fs - lead
+        return self.profile(t / self.duration) * self.body_weight()
+
+
+@dataclass
+class Geophone:
+    """geophone.Geophone (internal/geophone/geophone.go:36-62), SM-24 values
+    (:64-77) with the natural frequency and damping the workload sets."""
+    natural_freq: float = 10.0
+    sensitivity: float = 28.8
+    coil: float = 375.0
+    shunt: float = 0.0
+    open_circuit_damping: float = 0.7
+    moving_mass: float = 0.011
+    coupling_freq: float = 200.0      # WellPlantedSpike
+    coupling_damping: float = 0.5
+
+    def damping(self):
+        if self.shunt <= 0:
+            return self.open_circuit_damping
+        w0 = 2 * np.pi * self.natural_freq
+        return self.open_circuit_damping + self.sensitivity ** 2 / (2 * w0 * self.moving_mass * (self.coil + self.shunt))
+
+    def response(self, s):
+        """Response = CouplingResponse * TransducerResponse (geophone.go:175-203)
+        at the Laplace variable s (i w on the real axis, i w_c off it), V/(m/s)."""
+        w0 = 2 * np.pi * self.natural_freq
+        div = 1.0 if self.shunt <= 0 else self.shunt / (self.coil + self.shunt)
+        trans = (self.sensitivity * div) * s * s / (s * s + 2 * self.damping() * w0 * s + w0 * w0)
+        if self.coupling_freq <= 0:
+            return trans
+        wc = 2 * np.pi * self.coupling_freq
+        return wc * wc / (s * s + 2 * self.coupling_damping * wc * s + wc * wc) * trans
+
+
+# ---------------------------------------------------------------- synthesis --
+
+@dataclass
+class TraceSetup:
+    fs: float = 1000.0
+    n: int = 1024
+    lead: float = 0.05
+    r: float = 10.0
+    stance: Stance = field(default_factory=Stance)
+    geophone: Geophone = field(default_factory=Geophone)
+
+    @property
+    def omega_imag(self):
+        return math.pi / (self.n / self.fs)
+
+    def freqs(self):
+        return np.arange(1, self.n // 2 + 1) * self.fs / self.n
+
+
+def traces(G, setup):
+    """Geophone output traces (volts) from displacement spectra G[soil, bin]
+    (bins 1..n/2) evaluated at w_c = 2 pi f - i w_I. The response is tapered to
+    zero over the top fifth of the band (dsp.go:232-261) and the damping
+    e^(-w_I t) is undone after the inverse transform."""
+    n, fs, wi = setup.n, setup.fs, setup.omega_imag
+    f = np.arange(n // 2 + 1) * fs / n
+    wc = 2 * np.pi * f - 1j * wi
+    s = 1j * wc
+    t = np.arange(n) / fs
+    force = setup.stance.force(fs, n, setup.lead) * np.exp(-wi * t)
+    F = np.fft.rfft(force)
+    H = np.zeros((G.shape[0], n // 2 + 1), dtype=np.complex128)
+    H[:, 1:] = G * (1j * wc[1:])            # velocity per newton
+    H *= setup.geophone.response(s)[None, :]
+    nyq = fs / 2
+    taper_from = 0.8 * nyq
+    w = np.where(f > taper_from, 0.5 * (1 + np.cos(np.pi * (f - taper_from) / (nyq - taper_from))), 1.0)
+    Y = H * (w * F)[None, :]
+    y = np.fft.irfft(Y, n=n, axis=1)
+    return y * np.exp(wi * t)[None, :]
+
+
+def measure(y, fs):
+    """Peak |y| and the 2-400 Hz magnitude-weighted spectral centroid
+    (sweep.go:137-169), per trace."""
+    peak = np.max(np.abs(y), axis=1)
+    npad = 1 << int(math.ceil(math.log2(y.shape[1])))
+    Y = np.fft.rfft(y, n=npad, axis=1)
+    f = np.arange(npad // 2 + 1) * fs / npad
+    band = (f >= 2) & (f <= 400)
+    a = np.abs(Y[:, band])
+    den = a.sum(axis=1)
+    cen = np.where(den > 0, (a * f[band][None, :]).sum(axis=1) / np.where(den > 0, den, 1), 0.0)
+    return peak, cen
+
+
+# -------------------------------------------------------------------- solve --
+
+NK = 8192
+KMAX = 2.5 * 2 * math.pi * 500.0 / 80.0
+
+
+def solve_banks(params, setup, engine, batch_soils=20000, nk=NK, kmax=KMAX, formulation=N.DUNKIN):
+    """G[soil, bin] at setup.r for every parameter row, batched on the GPU.
+    Returns (G, seconds of GPU execute, rows)."""
+    freqs = setup.freqs()
+    opt = Integration(nk, 0.0, kmax)
+    out = np.zeros((len(params), len(freqs)), dtype=np.complex128)
+    gpu_s = 0.0
+    for b0 in range(0, len(params), batch_soils):
+        chunk = params[b0:b0 + batch_soils]
+        media = [Medium(soil_of(p), formulation=formulation, omega_imag=setup.omega_imag, engine=engine)
+                 for p in chunk]
+        plan = Batch(media, [freqs] * len(media), [setup.r], opt, engine=engine)
+        plan.execute()
+        g, status = plan.download()
+        prop, quad, other = plan.kernel_times()
+        gpu_s += (prop + quad + other) * 1e-3
+        plan.close()
+        if (status != 0).any():
+            bad = int(np.nonzero(status)[0][0])
+            raise RuntimeError(f"soil {b0 + bad // len(freqs)}: status {N.STATUS_NAMES[int(status[bad])]}")
+        out[b0:b0 + len(chunk)] = g.reshape(len(chunk), len(freqs))
+    return out, gpu_s, len(params) * len(freqs)
+
+
+@dataclass
+class SobolResult:
+    n: int
+    s1: dict
+    st: dict
+    metrics: dict
+    seconds: dict
+
+
+def run_plain(engine, n=16384, seed=0, setup=None, batch_soils=20000):
+    """The all-plain Sobol run: every soil through the GPU f-k solve."""
+    setup = setup or TraceSetup()
+    k = len(PARAMS)
+    t0 = time.perf_counter()
+    u = saltelli(n, k, seed)
+    params = unit_to_params(u)
+    G, gpu_s, rows = solve_banks(params, setup, engine, batch_soils)
+    t1 = time.perf_counter()
+    y = traces(G, setup)
+    peak, cen = measure(y, setup.fs)
+    s1p, stp = indices(peak, n, k)
+    s1c, stc = indices(cen, n, k)
+    t2 = time.perf_counter()
+    names = [p[0] for p in PARAMS]
+    return SobolResult(n, {"peak": dict(zip(names, s1p)), "centroid": dict(zip(names, s1c))},
+                       {"peak": dict(zip(names, stp)), "centroid": dict(zip(names, stc))},
+                       {"peak": peak, "centroid": cen},
+                       {"solve_wall": t1 - t0, "solve_gpu": gpu_s, "post": t2 - t1, "rows": rows,
+                        "soils": len(params)})

@@ -331,3 +331,42 @@ def test_graph_execute_matches_stream_execute(gfk, engine):
     b, _ = p.download()
     assert np.array_equal(a, b)
     p.close()
+
+
+def test_fused_sum_for_few_ranges(gfk, engine, oracle):
+    """Up to 8 ranges on a shared grid: the sum is fused into the propagator
+    (the integrand never reaches HBM) and must give what the GEMM path and the
+    oracle give."""
+    wl = gfk.workloads.single_soil()
+    m = wl.medium(gfk.DUNKIN, engine=engine)
+    few = wl.ranges[[0, 4, 9, 31, 63]]
+    many = np.concatenate([few, wl.ranges[[1, 2, 3, 5, 6]]])  # 10 ranges: GEMM path
+    a, sa = m.bank_spectra(few, wl.freqs, wl.integration())
+    b, sb = m.bank_spectra(many, wl.freqs, wl.integration())
+    assert (sa == 0).all() and (sb == 0).all()
+    assert rel_l2(a, b[:, :5]) < 1e-12
+    rows = np.arange(0, len(wl.freqs), 37)
+    want, _ = oracle.bank_spectra(as_tuples(wl.stack), few, wl.freqs[rows], samples=wl.samples, kmax=wl.kmax,
+                                  formulation=oracle.DUNKIN, omega_imag=wl.omega_imag)
+    assert rel_l2(a[rows], want) < 1e-9
+    a2, _ = m.bank_spectra(few, wl.freqs, wl.integration())
+    assert np.array_equal(a, a2)  # fixed reduction order: bit-reproducible
+
+
+def test_sobol_banks_and_metrics_against_oracle(gfk, engine, oracle):
+    """The Sobol workload's per-soil responses at 10 m (fused single-range
+    path) against the oracle, and the metrics computed from them."""
+    S = gfk.sobol
+    setup = S.TraceSetup()
+    u = S.saltelli(4, len(S.PARAMS), seed=2)
+    params = S.unit_to_params(u)
+    G, gpu_s, rows = S.solve_banks(params, setup, engine, batch_soils=16, nk=2048)
+    assert G.shape == (len(params), setup.n // 2) and np.isfinite(G).all()
+    for i in (0, 17):
+        st = S.soil_of(params[i])
+        want, _ = oracle.bank_spectra(as_tuples(st), [setup.r], setup.freqs(), samples=2048, kmax=S.KMAX,
+                                      formulation=oracle.DUNKIN, omega_imag=setup.omega_imag)
+        assert rel_l2(G[i], want[:, 0]) < 1e-9
+        y = S.traces(np.vstack([G[i], want[:, 0]]), setup)
+        pk, cen = S.measure(y, setup.fs)
+        assert abs(pk[0] - pk[1]) / pk[1] < 1e-8 and abs(cen[0] - cen[1]) < 1e-6
