@@ -29,6 +29,10 @@ EXPORTS = [
     "gfk_plan_launches_per_execute", "gfk_plan_tuning", "gfk_plan_kernel_times", "gfk_plan_destroy",
     "gfk_plan_use_graph", "gfk_batch_create",
     "gfk_bank_pack", "gfk_bank_write", "gfk_vertical_displacement_multi_noalloc",
+    "gfk_trace_metrics",
+    "gfk_dataset_create", "gfk_dataset_fill", "gfk_dataset_stats", "gfk_dataset_labels", "gfk_dataset_destroy",
+    "gfk_net_create", "gfk_net_set_scales", "gfk_net_train", "gfk_net_predict", "gfk_net_evaluate",
+    "gfk_net_param_count", "gfk_net_params", "gfk_net_fourier", "gfk_net_probe", "gfk_net_destroy",
 ]
 
 
@@ -57,6 +61,14 @@ class GfkSolve(ctypes.Structure):
                 ("_pad", ctypes.c_int32), ("omega_imag", ctypes.c_double)]
 
 
+class GfkNetConfig(ctypes.Structure):
+    _fields_ = [("nsoil_scalars", ctypes.c_int32), ("batch", ctypes.c_int32), ("warmup_steps", ctypes.c_int32),
+                ("total_steps", ctypes.c_int32), ("lr_max", ctypes.c_float), ("lr_min", ctypes.c_float),
+                ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
+                ("weight_decay", ctypes.c_float), ("phase_weight", ctypes.c_float),
+                ("fourier_sigma", ctypes.c_float), ("seed", ctypes.c_uint64)]
+
+
 _lib = None
 
 
@@ -69,7 +81,7 @@ def lib():
         raise RuntimeError(f"libgfk is not built ({LIB_PATH} missing); run build.build() — "
                            "there is no CPU fallback")
     L = ctypes.CDLL(str(LIB_PATH))
-    P, d, i32, i64 = ctypes.POINTER, ctypes.c_double, ctypes.c_int32, ctypes.c_int64
+    P, d, i32, i64, f32 = ctypes.POINTER, ctypes.c_double, ctypes.c_int32, ctypes.c_int64, ctypes.c_float
     vp = ctypes.c_void_p
     sig = {
         "gfk_open": (ctypes.c_int, [ctypes.c_int, P(vp)]),
@@ -103,6 +115,22 @@ def lib():
         "gfk_bank_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, P(ctypes.c_float), i64]),
         "gfk_vertical_displacement_multi_noalloc": (ctypes.c_int, [P(GfkMedium), P(GfkSolve), P(d), i32, d,
                                                                    GfkIntegration, P(d), vp]),
+        "gfk_trace_metrics": (ctypes.c_int, [vp, vp, i64, i32, i32, P(d), i32, d, d, i32, i32, P(d), P(d)]),
+        "gfk_dataset_create": (ctypes.c_int, [vp, i32, i32, P(d), P(d), i32, P(d), i32, d, P(vp)]),
+        "gfk_dataset_fill": (ctypes.c_int, [vp, vp, i32, i32]),
+        "gfk_dataset_stats": (ctypes.c_int, [vp, P(d)]),
+        "gfk_dataset_labels": (ctypes.c_int, [vp, i32, P(f32)]),
+        "gfk_dataset_destroy": (ctypes.c_int, [vp]),
+        "gfk_net_create": (ctypes.c_int, [vp, P(GfkNetConfig), P(vp)]),
+        "gfk_net_set_scales": (ctypes.c_int, [vp, d, d, d, d, P(f32)]),
+        "gfk_net_train": (ctypes.c_int, [vp, vp, P(i32), i32, i32, P(f32)]),
+        "gfk_net_predict": (ctypes.c_int, [vp, P(d), i32, P(d), i32, P(d), i32, vp, i32]),
+        "gfk_net_evaluate": (ctypes.c_int, [vp, vp, P(i32), i32, P(d)]),
+        "gfk_net_param_count": (i64, [vp]),
+        "gfk_net_params": (ctypes.c_int, [vp, P(f32), i64, i32]),
+        "gfk_net_fourier": (ctypes.c_int, [vp, P(f32), i32]),
+        "gfk_net_probe": (ctypes.c_int, [vp, P(f32), P(f32), P(f32), P(f32)]),
+        "gfk_net_destroy": (ctypes.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -1,0 +1,30 @@
+// gfk_ctx.h — the context object behind the C ABI's gfk_ctx handle, shared
+// by the translation units of libgfk.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+struct gfk_plan;
+struct gfk_dataset;
+struct gfk_net;
+
+struct gfk_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    int64_t launches = 0;
+    std::vector<gfk_plan*> plans;        // live plans, destroyed by gfk_close
+    std::vector<gfk_dataset*> datasets;  // live surrogate data sets and networks,
+    std::vector<gfk_net*> nets;          // destroyed by gfk_close as well
+    // propagator launch shape chosen by tuning, per (layer count, wavenumber count)
+    struct Tuned {
+        int nl, nk, variant;
+    };
+    std::vector<Tuned> tuned;
+};
+
+// Frees every surrogate object the context still holds (gfk_surrogate.cu).
+void gfk_release_surrogates(gfk_ctx* ctx);

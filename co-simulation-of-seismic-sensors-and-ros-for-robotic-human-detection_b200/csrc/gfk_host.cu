@@ -10,26 +10,13 @@
 #include <vector>
 
 #include "../../include/gfk.h"
+#include "gfk_ctx.h"
 #include "gfk_kernels.cuh"
 
 
 
 // ------------------------------------------------------------------ ctx --
 
-struct gfk_plan;
-
-struct gfk_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string last_error;
-    int64_t launches = 0;
-    std::vector<gfk_plan*> plans;  // live plans, destroyed by gfk_close
-    // propagator launch shape chosen by tuning, per (layer count, wavenumber count)
-    struct Tuned {
-        int nl, nk, variant;
-    };
-    std::vector<Tuned> tuned;
-};
 
 namespace {
 
@@ -806,6 +793,7 @@ int gfk_close(gfk_ctx* ctx) {
         delete p;
     }
     ctx->plans.clear();
+    gfk_release_surrogates(ctx);
     if (ctx->stream) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);

@@ -1,0 +1,105 @@
+// gfk_trace.cu — geophone traces and their sweep metrics, one soil per CTA.
+//
+// For a displacement spectrum G[k-1] on bins k = 1..n/2 at the complex
+// frequency w_c = 2 pi f - i w_I, the recorded trace is
+//     Y_k = G[k-1] S_k,   S_k = (i w_c) geophone(i w_c) taper_k F_k
+// (velocity per newton through the sensor, times the footstep spectrum, the
+// host precomputes S once per setup), y = irfft(Y, n) e^{w_I t}
+// (internal/dsp/dsp.go:232-261 taper and inverse transform; the damping
+// undone after it). The metrics follow sweep.Measure
+// (internal/sweep/sweep.go:128-169): the peak |y| and the magnitude-weighted
+// centroid of |rfft(y)| over the band bins [k_lo, k_hi].
+//
+// Both transforms are n = 1024 complex radix-2 Stockham FFTs in FP64 in
+// shared memory (the autosort formulation of Govindaraju et al., SC 2008:
+// butterfly j reads x[j], x[j + n/2] and writes y[2 Ns (j / Ns) + j % Ns]
+// and that + Ns, twiddle e^{-2 pi i (j % Ns) / (2 Ns)}). The inverse
+// transform of the Hermitian spectrum is Re(FFT(conj(Y~))) / n.
+#include "gfk_kernels.cuh"
+#include "gfk_mlp.cuh"
+
+namespace gfk {
+namespace trace {
+
+constexpr int kThreads = 256;
+
+__device__ void fft1024(cd* x, cd* y, const cd* __restrict__ tw) {
+    // x holds the input; the result ends in x (10 stages, even count).
+    cd* src = x;
+    cd* dst = y;
+    for (int ns = 1; ns < kN; ns <<= 1) {
+        for (int j = threadIdx.x; j < kN / 2; j += blockDim.x) {
+            const int k = j & (ns - 1);
+            const cd w = tw[k * (kN / (2 * ns))];
+            const cd a0 = src[j];
+            const cd a1 = src[j + kN / 2] * w;
+            const int d = ((j - k) << 1) + k;
+            dst[d] = a0 + a1;
+            dst[d + ns] = a0 - a1;
+        }
+        __syncthreads();
+        cd* t = src;
+        src = dst;
+        dst = t;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_metrics(const cd* __restrict__ G, long long stride, int nbins,
+                                                      const cd* __restrict__ S, const cd* __restrict__ tw, double fs,
+                                                      double wi, int k_lo, int k_hi, double* peak,
+                                                      double* centroid) {
+    __shared__ cd buf[2][kN];
+    __shared__ double red[2][kThreads];
+    const int s = blockIdx.x, tid = threadIdx.x;
+    const cd* g = G + (size_t)s * stride;
+    // conj of the Hermitian extension of Y: k = 0 and n/2 real parts only
+    for (int k = tid; k <= kN / 2; k += blockDim.x) {
+        cd Y = mk(0.0);
+        if (k >= 1 && k <= nbins) Y = g[k - 1] * S[k];
+        if (k == kN / 2) Y.im = 0.0;
+        buf[0][k] = mk(Y.re, -Y.im);
+        if (k > 0 && k < kN / 2) buf[0][kN - k] = Y;
+    }
+    __syncthreads();
+    fft1024(buf[0], buf[1], tw);
+    // y_t = Re / n e^{w_I t}; keep y as the real input of the second transform
+    double pk = 0.0;
+    for (int t = tid; t < kN; t += blockDim.x) {
+        const double yt = buf[0][t].re * (1.0 / kN) * exp(wi * t / fs);
+        pk = fmax(pk, fabs(yt));
+        buf[0][t] = mk(yt);
+    }
+    __syncthreads();
+    fft1024(buf[0], buf[1], tw);
+    double num = 0.0, den = 0.0;
+    for (int k = k_lo + tid; k <= k_hi; k += blockDim.x) {
+        const double a = hypot(buf[0][k].re, buf[0][k].im);
+        num += a * (k * fs / kN);
+        den += a;
+    }
+    red[0][tid] = num;
+    red[1][tid] = den;
+    __shared__ double pmax[kThreads];
+    pmax[tid] = pk;
+    __syncthreads();
+    for (int w = kThreads / 2; w > 0; w >>= 1) {
+        if (tid < w) {
+            red[0][tid] += red[0][tid + w];
+            red[1][tid] += red[1][tid + w];
+            pmax[tid] = fmax(pmax[tid], pmax[tid + w]);
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        peak[s] = pmax[0];
+        centroid[s] = red[1][0] > 0.0 ? red[0][0] / red[1][0] : 0.0;
+    }
+}
+
+void launch_metrics(cudaStream_t s, const cd* G, long long stride, int ns, int nbins, const cd* S, const cd* twiddle,
+                    double fs, double omega_imag, int k_lo, int k_hi, double* peak, double* centroid) {
+    k_metrics<<<ns, kThreads, 0, s>>>(G, stride, nbins, S, twiddle, fs, omega_imag, k_lo, k_hi, peak, centroid);
+}
+
+}  // namespace trace
+}  // namespace gfk

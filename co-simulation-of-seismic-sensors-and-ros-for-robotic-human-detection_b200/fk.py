@@ -314,6 +314,12 @@ class Plan:
             self.engine.check(st)
         return out[:, 0::2] + 1j * out[:, 1::2], status
 
+    def statuses(self):
+        """Per-row status codes of the last execute, without moving the result."""
+        status = np.zeros(len(self.freqs), dtype=np.int32)
+        N.lib().gfk_plan_download(self.p, None, status.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        return status
+
     def launches_per_execute(self):
         return int(N.lib().gfk_plan_launches_per_execute(self.p))
 

@@ -24,6 +24,7 @@ the half-space has Vp/Vs = 2, Qs = 40; every layer has Qp = 2 Qs; the trace is
 uses the complex frequency offset w_I = pi/T (T = 1.024 s), undone after the
 inverse transform; wavenumbers: 8192 to k_max = 2.5 w_max/80 m/s.
 """
+import ctypes
 import math
 import time
 from dataclasses import dataclass, field
@@ -275,23 +276,164 @@ class SobolResult:
     seconds: dict
 
 
-def run_plain(engine, n=16384, seed=0, setup=None, batch_soils=20000):
-    """The all-plain Sobol run: every soil through the GPU f-k solve."""
+def shaping(setup):
+    """S_k, k = 0..n/2: what traces() multiplies G[k-1] by (velocity per
+    newton, sensor, taper above 0.8 Nyquist, footstep spectrum) at w_c."""
+    n, fs, wi = setup.n, setup.fs, setup.omega_imag
+    f = np.arange(n // 2 + 1) * fs / n
+    wc = 2 * np.pi * f - 1j * wi
+    t = np.arange(n) / fs
+    F = np.fft.rfft(setup.stance.force(fs, n, setup.lead) * np.exp(-wi * t))
+    nyq = fs / 2
+    taper_from = 0.8 * nyq
+    w = np.where(f > taper_from, 0.5 * (1 + np.cos(np.pi * (f - taper_from) / (nyq - taper_from))), 1.0)
+    S = (1j * wc) * setup.geophone.response(1j * wc) * (w * F)
+    S[0] = 0.0
+    return S
+
+
+def band(setup, lo=2.0, hi=400.0):
+    """First and last rfft bin of measure()'s centroid band."""
+    npad = 1 << int(math.ceil(math.log2(setup.n)))
+    f = np.arange(npad // 2 + 1) * setup.fs / npad
+    idx = np.nonzero((f >= lo) & (f <= hi))[0]
+    return int(idx[0]), int(idx[-1])
+
+
+def metrics_device(engine, d_G, stride, ns, setup):
+    """(peak, centroid) of ns soils whose spectra G[s][k-1] (bins 1..n/2) are
+    device (re, im) pairs at d_G + 16 s stride: gfk_trace_metrics."""
+    Sc = shaping(setup)
+    S = np.ascontiguousarray(np.stack([Sc.real, Sc.imag], axis=1).ravel())
+    k_lo, k_hi = band(setup)
+    peak = np.zeros(ns)
+    cen = np.zeros(ns)
+
+    def dp(a):
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+    engine.check(N.lib().gfk_trace_metrics(engine.ctx, ctypes.c_void_p(d_G), int(stride), int(ns), setup.n // 2,
+                                           dp(S), setup.n, setup.fs, setup.omega_imag, k_lo, k_hi, dp(peak),
+                                           dp(cen)))
+    return peak, cen
+
+
+def solve_metrics(params, setup, engine, batch_soils=20000, nk=NK, kmax=KMAX, formulation=N.DUNKIN):
+    """(peak, centroid) of every parameter row through the GPU f-k solve and
+    the GPU trace metrics; the banks never leave the device. Returns
+    (peak, centroid, GPU solver seconds)."""
+    freqs = setup.freqs()
+    opt = Integration(nk, 0.0, kmax)
+    peak = np.zeros(len(params))
+    cen = np.zeros(len(params))
+    gpu_s = 0.0
+    for b0 in range(0, len(params), batch_soils):
+        chunk = params[b0:b0 + batch_soils]
+        media = [Medium(soil_of(p), formulation=formulation, omega_imag=setup.omega_imag, engine=engine)
+                 for p in chunk]
+        plan = Batch(media, [freqs] * len(media), [setup.r], opt, engine=engine)
+        try:
+            plan.execute()
+            status = plan.statuses()
+            if (status != 0).any():
+                bad = int(np.nonzero(status)[0][0])
+                raise RuntimeError(f"soil {b0 + bad // len(freqs)}: status {N.STATUS_NAMES[int(status[bad])]}")
+            a, b, c = plan.kernel_times()
+            gpu_s += (a + b + c) * 1e-3
+            pk, ce = metrics_device(engine, plan.result_device_ptr(), len(freqs), len(chunk), setup)
+        finally:
+            plan.close()
+        peak[b0:b0 + len(chunk)] = pk
+        cen[b0:b0 + len(chunk)] = ce
+    return peak, cen, gpu_s
+
+
+def _result(n, k, peak, cen, seconds):
+    s1p, stp = indices(peak, n, k)
+    s1c, stc = indices(cen, n, k)
+    names = [p[0] for p in PARAMS]
+    return SobolResult(n, {"peak": dict(zip(names, s1p)), "centroid": dict(zip(names, s1c))},
+                       {"peak": dict(zip(names, stp)), "centroid": dict(zip(names, stc))},
+                       {"peak": peak, "centroid": cen}, seconds)
+
+
+def run_plain(engine, n=16384, seed=0, setup=None, batch_soils=20000, host_metrics=False):
+    """The all-plain Sobol run: every soil through the GPU f-k solve. The
+    metrics run on the GPU (gfk_trace_metrics) unless host_metrics, which
+    downloads the banks and uses traces()/measure()."""
     setup = setup or TraceSetup()
     k = len(PARAMS)
     t0 = time.perf_counter()
     u = saltelli(n, k, seed)
     params = unit_to_params(u)
-    G, gpu_s, rows = solve_banks(params, setup, engine, batch_soils)
-    t1 = time.perf_counter()
-    y = traces(G, setup)
-    peak, cen = measure(y, setup.fs)
-    s1p, stp = indices(peak, n, k)
-    s1c, stc = indices(cen, n, k)
+    if host_metrics:
+        G, gpu_s, rows = solve_banks(params, setup, engine, batch_soils)
+        t1 = time.perf_counter()
+        peak, cen = measure(traces(G, setup), setup.fs)
+    else:
+        peak, cen, gpu_s = solve_metrics(params, setup, engine, batch_soils)
+        t1 = time.perf_counter()
+    res = _result(n, k, peak, cen, {})
     t2 = time.perf_counter()
-    names = [p[0] for p in PARAMS]
-    return SobolResult(n, {"peak": dict(zip(names, s1p)), "centroid": dict(zip(names, s1c))},
-                       {"peak": dict(zip(names, stp)), "centroid": dict(zip(names, stc))},
-                       {"peak": peak, "centroid": cen},
-                       {"solve_wall": t1 - t0, "solve_gpu": gpu_s, "post": t2 - t1, "rows": rows,
-                        "soils": len(params)})
+    res.seconds = {"solve_wall": t1 - t0, "solve_gpu": gpu_s, "post": t2 - t1, "total": t2 - t0,
+                   "rows": len(params) * len(setup.freqs()), "soils": len(params)}
+    return res
+
+
+def ensemble_metrics(nets, params8, setup, engine, chunk_soils=32768):
+    """Every network's (peak, centroid) for the Sobol rows: each network
+    predicts G at the sensor range on the device and the trace metrics run
+    on that device buffer. Returns arrays [members][soils]."""
+    import torch  # device buffers only
+
+    from .surrogate import from_sobol
+    p11 = from_sobol(params8)
+    freqs = setup.freqs()
+    nb = len(freqs)
+    peaks = np.zeros((len(nets), len(p11)))
+    cens = np.zeros((len(nets), len(p11)))
+    buf = torch.empty(min(chunk_soils, len(p11)) * nb * 2, dtype=torch.float64, device=f"cuda:{engine.device}")
+    for e, net in enumerate(nets):
+        for b0 in range(0, len(p11), chunk_soils):
+            chunk = p11[b0:b0 + chunk_soils]
+            net.predict(chunk, [setup.r], freqs, out_device_ptr=buf.data_ptr())
+            pk, ce = metrics_device(engine, buf.data_ptr(), nb, len(chunk), setup)
+            peaks[e, b0:b0 + len(chunk)] = pk
+            cens[e, b0:b0 + len(chunk)] = ce
+    del buf
+    return peaks, cens
+
+
+def spread(values):
+    """Relative spread (max - min) / |mean| over the ensemble axis 0."""
+    v = np.asarray(values)
+    return (v.max(axis=0) - v.min(axis=0)) / np.maximum(np.abs(v.mean(axis=0)), 1e-300)
+
+
+def run_surrogate(engine, nets, n=16384, seed=0, setup=None, threshold=0.01, batch_soils=20000):
+    """The Sobol run with the surrogate answering: every network of the
+    ensemble predicts each soil's metrics; where the ensemble's relative
+    spread of either metric exceeds `threshold` the soil is re-solved by the
+    plain GPU f-k path, whose answer replaces the ensemble mean."""
+    setup = setup or TraceSetup()
+    k = len(PARAMS)
+    t0 = time.perf_counter()
+    u = saltelli(n, k, seed)
+    params = unit_to_params(u)
+    peaks, cens = ensemble_metrics(nets, params, setup, engine)
+    t1 = time.perf_counter()
+    peak, cen = peaks.mean(axis=0), cens.mean(axis=0)
+    sp = np.maximum(spread(peaks), spread(cens))
+    fb = np.nonzero(sp > threshold)[0]
+    gpu_s = 0.0
+    if len(fb):
+        pk, ce, gpu_s = solve_metrics(params[fb], setup, engine, batch_soils)
+        peak[fb], cen[fb] = pk, ce
+    t2 = time.perf_counter()
+    res = _result(n, k, peak, cen, {})
+    t3 = time.perf_counter()
+    res.seconds = {"surrogate": t1 - t0, "fallback_wall": t2 - t1, "fallback_gpu": gpu_s, "post": t3 - t2,
+                   "total": t3 - t0, "soils": len(params), "fallback_soils": int(len(fb)),
+                   "fallback_fraction": len(fb) / len(params), "members": len(nets), "threshold": threshold}
+    res.metrics["spread"] = sp
+    return res

@@ -259,6 +259,103 @@ int gfk_bank_pack(const double *spectra, int32_t nf, int32_t nr,
 int gfk_bank_write(const char *path, const char *header_json,
                    const float *payload, int64_t nfloats);
 
+/* ---- sweep metrics of geophone traces ------------------------------------ */
+/* For each of ns soils, the geophone trace synthesised from its displacement
+ * spectrum and its two sweep metrics (internal/sweep/sweep.go:128-169 Measure:
+ * peak |y| and the |Y|-weighted spectral centroid over the band). d_G is a
+ * device array of (re, im) pairs: soil s's bins k = 1..nbins at
+ * d_G[2 (s stride + k - 1)]. shaping holds the n/2+1 complex factors S_k the
+ * spectrum is multiplied by (velocity per newton, sensor response, taper
+ * above 0.8 Nyquist and the footstep's spectrum; internal/geophone/
+ * geophone.go:175-203, internal/dsp/dsp.go:232-261, internal/grf/grf.go:
+ * 280-330), computed by the caller at w_c = 2 pi f - i omega_imag; the trace
+ * is irfft(G S, n) e^(omega_imag t). n must be 1024. Band bins are
+ * [k_lo, k_hi]. peak and centroid are host arrays of ns doubles. */
+int gfk_trace_metrics(gfk_ctx *ctx, const double *d_G, int64_t stride, int32_t ns, int32_t nbins,
+                      const double *shaping, int32_t n, double fs_hz, double omega_imag,
+                      int32_t k_lo, int32_t k_hi, double *peak, double *centroid);
+
+/* ---- surrogate network ---------------------------------------------------- */
+/* No counterpart in the reference (it has no learned component). A small
+ * network maps (soil scalars, range, frequency) to the vertical displacement
+ * spectrum as t0 = log|G| and t1 = -phi/(w r), phi the phase unwrapped along
+ * range like internal/bank/interp.go:66-102: 128 input features (the soil
+ * scalars, range and frequency, their logarithms and 56 Fourier pairs of
+ * (range, frequency)), five SiLU layers of width 512 and a 2-wide FP32 output
+ * layer. BF16 weights and activations, FP32 accumulation, FP32 master weights
+ * and AdamW moments; every step runs libgfk's own forward, backward and
+ * optimiser kernels and is replayed as one CUDA graph.
+ *
+ * A data set holds the labels of nsoil soils over one range and frequency
+ * grid in device memory, filled from device banks the solver produced. */
+typedef struct gfk_dataset gfk_dataset;
+typedef struct gfk_net gfk_net;
+
+#define GFK_NET_MAX_SOIL 11
+#define GFK_NET_WIDTH 512
+#define GFK_NET_INPUTS 128
+
+typedef struct {
+    int32_t nsoil_scalars;  /* soil scalars per soil, <= GFK_NET_MAX_SOIL */
+    int32_t batch;          /* rows per step, a multiple of 128 */
+    int32_t warmup_steps;   /* linear warm-up, then cosine decay ... */
+    int32_t total_steps;    /* ... to lr_min at this step */
+    float lr_max, lr_min;
+    float beta1, beta2, eps, weight_decay;
+    float phase_weight;     /* loss weight of the phase target */
+    float fourier_sigma;    /* std of the Fourier frequencies, cycles per domain */
+    uint64_t seed;          /* initial weights, Fourier frequencies, batches */
+} gfk_net_config;
+
+/* Soil scalars are given already mapped to [-1, 1] by the caller. Labels are
+ * built from banks with an amplitude floor floor_rel times the soil's largest
+ * |G|: t0 is clamped at the floor, and a cell's phase is not learnt once its
+ * unwrapping chain has met a cell below it. nr <= 128. */
+int gfk_dataset_create(gfk_ctx *ctx, int32_t nsoil_scalars, int32_t nsoil, const double *soil_scalars,
+                       const double *ranges_m, int32_t nr, const double *freqs_hz, int32_t nf,
+                       double floor_rel, gfk_dataset **out);
+/* Labels of soils [first_soil, first_soil + nsoil) from the device bank d_G
+ * [nsoil][nf][nr] (re, im) pairs (gfk_plan_result_device of a batch plan). */
+int gfk_dataset_fill(gfk_dataset *ds, const double *d_G, int32_t first_soil, int32_t nsoil);
+/* Sums over the filled soils: cells, sum t0, sum t0^2, phase cells, sum t1,
+ * sum t1^2. */
+int gfk_dataset_stats(gfk_dataset *ds, double out[6]);
+/* One soil's labels, host [nr][nf][2] floats (NaN where the phase is not learnt). */
+int gfk_dataset_labels(gfk_dataset *ds, int32_t soil, float *out);
+int gfk_dataset_destroy(gfk_dataset *ds);
+
+int gfk_net_create(gfk_ctx *ctx, const gfk_net_config *cfg, gfk_net **out);
+/* The input domain (range and frequency spans the features are scaled on)
+ * and the target standardisation y = (t - mean) / std: mean_std =
+ * {mean0, std0, mean1, std1}. Set before training or prediction. */
+int gfk_net_set_scales(gfk_net *net, double r_lo, double r_hi, double f_lo, double f_hi,
+                       const float mean_std[4]);
+/* `steps` optimiser steps on batches drawn uniformly from the cells of the
+ * listed soils. loss (optional, host [steps][2]) receives each step's mean
+ * squared error of the two standardised targets. */
+int gfk_net_train(gfk_net *net, gfk_dataset *ds, const int32_t *train_soils, int32_t ntrain,
+                  int32_t steps, float *loss);
+/* G for ns soils at every (frequency, range) pair: out[2 ((s nf + j) nr + i)]
+ * (re, im). out is device memory when out_on_device is nonzero. */
+int gfk_net_predict(gfk_net *net, const double *soil_scalars, int32_t ns, const double *ranges_m,
+                    int32_t nr, const double *freqs_hz, int32_t nf, double *out, int32_t out_on_device);
+/* Held-out error against the data set's labels for the listed soils, over the
+ * data set's grid: out = {cells, sum e0^2, phase cells, sum e1^2,
+ * sum (e1 w r)^2, sum |G_pred - G|^2, sum |G|^2}. */
+int gfk_net_evaluate(gfk_net *net, gfk_dataset *ds, const int32_t *soils, int32_t ns, double out[7]);
+int64_t gfk_net_param_count(const gfk_net *net);
+/* Get (set = 0) or set (set != 0) the FP32 master parameters, n floats:
+ * W1 [512][128], b1, W2..W5 [512][512] and their biases, W6 [2][512], b6 [2]. */
+int gfk_net_params(gfk_net *net, float *host, int64_t n, int32_t set);
+/* Get or set the 56 x 2 Fourier frequencies. */
+int gfk_net_fourier(gfk_net *net, float *host, int32_t set);
+/* One forward and backward pass on a given batch without an update, for
+ * gradient checks: X host [batch][128] features, Y host [batch][2]
+ * standardised targets (NaN: no phase term). grad receives the full gradient
+ * of the loss (layout of gfk_net_params), loss the two mean squared errors. */
+int gfk_net_probe(gfk_net *net, const float *X, const float *Y, float *grad, float loss[2]);
+int gfk_net_destroy(gfk_net *net);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,177 @@
+"""GPU checks of the surrogate kernels and the trace metrics against the CPU
+oracle (oracle/surrogate_oracle.py) and the host restatement of the Sobol
+post-processing."""
+import ctypes
+import pathlib
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT / "oracle"))
+import surrogate_oracle as SO  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pkg():
+    sys.path.insert(0, str(ROOT))
+    import __graft_entry__ as g
+    return g.load_package()
+
+
+@pytest.fixture(scope="module")
+def eng(pkg):
+    e = pkg.Engine(0)
+    yield e
+    e.close()
+
+
+def seg_rel(a, b, lo, hi):
+    return np.linalg.norm(a[lo:hi] - b[lo:hi]) / max(np.linalg.norm(b[lo:hi]), 1e-300)
+
+
+def test_gradients_match_oracle(pkg, eng):
+    """One forward/backward pass of libgfk's BF16 kernels against the FP64
+    oracle with BF16 rounding at the same places (tolerance: FP32
+    accumulation order), and against the unrounded FP64 gradient."""
+    sur = pkg.surrogate
+    net = sur.Net(sur.NetConfig(batch=256, seed=3), eng)
+    net.set_scales(1.0, 64.0, 1.0, 500.0, [0.0, 1.0, 0.0, 1.0])
+    p = net.params().astype(np.float64)
+    rng = np.random.default_rng(4)
+    X = rng.uniform(-1, 1, (256, 128)).astype(np.float32)
+    Y = rng.normal(size=(256, 2)).astype(np.float32)
+    Y[::7, 1] = np.nan
+    g_gpu, loss = net.probe(X, Y)
+    g_emu, (m0, m1) = SO.backward(p, X, Y, phase_weight=net.config.phase_weight, emulate=True)
+    g_ref, _ = SO.backward(p, X, Y, phase_weight=net.config.phase_weight, emulate=False)
+    assert abs(loss[0] - m0) <= 2e-3 * m0 and abs(loss[1] - m1) <= 2e-3 * m1
+    layers, w6, b6, n = SO.layout()
+    segs = [(w, w + SO.WIDTH * fi) for (w, _, fi) in layers] + [(b, b + SO.WIDTH) for (_, b, _) in layers]
+    segs += [(w6, w6 + 2 * SO.WIDTH), (b6, b6 + 2)]
+    for lo, hi in segs:
+        assert seg_rel(g_gpu, g_emu, lo, hi) < 1e-2, (lo, seg_rel(g_gpu, g_emu, lo, hi))
+        assert seg_rel(g_gpu, g_ref, lo, hi) < 5e-2, (lo, seg_rel(g_gpu, g_ref, lo, hi))
+    net.close()
+
+
+def test_predict_matches_oracle_forward(pkg, eng):
+    """Features, inference GEMMs and the output mapping against the oracle."""
+    sur = pkg.surrogate
+    net = sur.Net(sur.NetConfig(batch=256, seed=5), eng)
+    ms = [-20.0, 2.0, 0.006, 0.002]
+    net.set_scales(1.0, 64.0, 500 / 512, 500.0, ms)
+    params = sur.draw(3, 11)
+    ranges = np.array([1.0, 2.0, 3.5])
+    freqs = np.array([500 / 512, 10.0, 30.0, 45.0])
+    G = net.predict(params, ranges, freqs)
+    assert G.shape == (3, 4, 3)
+    p = net.params().astype(np.float64)
+    B = net.fourier()
+    sc = sur.to_scalars(params)
+    for s in range(3):
+        rr, ff = np.meshgrid(ranges, freqs)
+        X = SO.features(np.repeat(sc[s:s + 1], rr.size, axis=0), rr.ravel(), ff.ravel(),
+                        (1.0, 64.0, 500 / 512, 500.0), B)
+        y, _ = SO.forward(p, X, emulate=True)
+        t0 = y[:, 0] * ms[1] + ms[0]
+        t1 = y[:, 1] * ms[3] + ms[2]
+        want = np.exp(t0) * np.exp(-1j * t1 * 2 * np.pi * ff.ravel() * rr.ravel())
+        got = G[s].ravel()
+        assert np.allclose(np.log(np.abs(got)), t0, atol=2e-2)
+        assert np.abs(got - want).max() / np.abs(want).max() < 5e-2
+    net.close()
+
+
+def test_labels_match_oracle(pkg, eng):
+    """Bank -> labels on the device against the oracle's restatement."""
+    sur = pkg.surrogate
+    grid = sur.LabelGrid(ranges=np.arange(1.0, 33.0), nk=4096)
+    params = sur.draw(3, 21)
+    ds = sur.Dataset(params, grid, floor_rel=1e-6, engine=eng)
+    banks = []
+
+    def each(plan, first, count):
+        eng.check(pkg._native.lib().gfk_dataset_fill(ds.p, ctypes.c_void_p(plan.result_device_ptr()), first,
+                                                     count))
+        g, _ = plan.download()
+        banks.append(g.reshape(count, len(grid.freqs), len(grid.ranges)))
+
+    sur.solve_media(params, grid, eng, batch_soils=2, each=each)
+    G = np.concatenate(banks)
+    for s in range(3):
+        want = SO.labels(G[s], grid.ranges, grid.freqs, 1e-6)
+        got = ds.labels(s)
+        assert np.array_equal(np.isnan(got[..., 1]), np.isnan(want[..., 1]))
+        ok = ~np.isnan(want[..., 1])
+        assert ok.mean() > 0.3
+        assert np.allclose(got[..., 0], want[..., 0], rtol=1e-6, atol=1e-6)
+        assert np.allclose(got[..., 1][ok], want[..., 1][ok], rtol=1e-6, atol=0)
+    m0, s0, m1, s1, frac = ds.stats()
+    assert s0 > 0 and s1 > 0 and 0 < frac <= 1
+    ds.close()
+
+
+def test_trace_metrics_match_host(pkg, eng):
+    """gfk_trace_metrics against traces()/measure() on the same spectra."""
+    import torch
+    sob = pkg.sobol
+    setup = sob.TraceSetup()
+    rng = np.random.default_rng(6)
+    f = setup.freqs()
+    G = (rng.normal(size=(40, 512)) + 1j * rng.normal(size=(40, 512))) * 1e-9 * np.exp(-f / 80.0)[None, :]
+    peak, cen = sob.measure(sob.traces(G, setup), setup.fs)
+    d = torch.from_numpy(np.stack([G.real, G.imag], axis=-1).ravel()).to("cuda:0")
+    pk, ce = sob.metrics_device(eng, d.data_ptr(), 512, 40, setup)
+    assert np.allclose(pk, peak, rtol=1e-10, atol=0)
+    assert np.allclose(ce, cen, rtol=1e-10, atol=0)
+
+
+def test_sobol_plain_gpu_metrics_equal_host(pkg, eng):
+    """The plain Sobol run with device metrics equals the host path."""
+    sob = pkg.sobol
+    a = sob.run_plain(eng, n=8, seed=2, host_metrics=True)
+    b = sob.run_plain(eng, n=8, seed=2)
+    assert np.allclose(a.metrics["peak"], b.metrics["peak"], rtol=1e-9)
+    assert np.allclose(a.metrics["centroid"], b.metrics["centroid"], rtol=1e-9)
+
+
+def test_training_reduces_loss_and_beats_mean(pkg, eng):
+    """A short training run on a small data set: the loss falls, and the
+    trained network's held-out error beats the best constant prediction."""
+    sur = pkg.surrogate
+    grid = sur.LabelGrid(ranges=np.arange(1.0, 17.0), nk=2048)
+    params = sur.draw(40, 31)
+    ds = sur.Dataset(params, grid, engine=eng).fill(batch_soils=40)
+    train, held = sur.split_soils(40, 0.1, 1)
+    net = sur.Net(sur.NetConfig(batch=1024, warmup_steps=50, total_steps=600, lr_max=2e-3, seed=9), eng)
+    net.scales_from(ds)
+    loss = net.train(ds, train, 600)
+    assert np.isfinite(loss).all()
+    assert loss[-50:, 0].mean() < 0.2 * loss[:50, 0].mean()
+    ev = net.evaluate(ds, held)
+    # the constant predictor (t = mean) has standardised RMS 1 on log-amplitude
+    m0, s0, _, _, _ = ds.stats()
+    assert ev["rms_log_amp"] / s0 < 0.5
+    ds.close()
+    net.close()
+
+
+def test_surrogate_sobol_plumbing(pkg, eng):
+    """End to end with an untrained two-member ensemble: every soil the
+    ensemble disagrees on is re-solved, and those soils' metrics equal the
+    plain run's exactly."""
+    sob, sur = pkg.sobol, pkg.surrogate
+    nets = [sur.Net(sur.NetConfig(batch=256, seed=s), eng) for s in (1, 2)]
+    for n_ in nets:
+        n_.set_scales(1.0, 64.0, 500 / 512, 500.0, [-22.0, 2.0, 0.006, 0.002])
+    res = sob.run_surrogate(eng, nets, n=8, seed=2, threshold=0.01)
+    plain = sob.run_plain(eng, n=8, seed=2)
+    fb = np.nonzero(res.metrics["spread"] > 0.01)[0]
+    assert res.seconds["fallback_soils"] == len(fb) and len(fb) > 0
+    assert np.allclose(res.metrics["peak"][fb], plain.metrics["peak"][fb], rtol=1e-12)
+    for n_ in nets:
+        n_.close()
