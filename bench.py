@@ -325,6 +325,62 @@ def run_sobol(args, gfk, torch, rank, world, local):
         print(json.dumps(out))
 
 
+def run_surrogate(args, gfk, torch, rank, world, local):
+    """The learned part end to end on one GPU: labels for the 3-layer soil
+    family from the batched FP64 solver, an ensemble of BF16 networks trained
+    by libgfk's kernels, held-out error, then the Sobol run with the
+    surrogate answering and the plain f-k solve as fallback, against the
+    all-plain Sobol run. One step is the whole pipeline."""
+    S, U = gfk.sobol, gfk.surrogate
+    eng = gfk.Engine(local)
+    log = (lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else (lambda m: None)
+    t0 = time.perf_counter()
+    params = U.draw(args.sur_soils, 20240611)
+    ds = U.Dataset(params, U.LabelGrid(), floor_rel=1e-6, engine=eng).fill(batch_soils=8192)
+    t_data = time.perf_counter() - t0
+    m0, s0, m1, s1, frac = ds.stats()
+    log(f"labels: {args.sur_soils} soils in {t_data:.1f} s (solver {ds.solve_ms / 1e3:.1f} s GPU); "
+        f"t0 {m0:.3f}+-{s0:.3f}, t1 {m1:.3e}+-{s1:.3e}, phase cells {frac:.3f}")
+    train, held = U.split_soils(args.sur_soils, 0.05, 0)
+    cfg = U.NetConfig(total_steps=args.sur_steps, lr_max=args.sur_lr, fourier_sigma=args.sur_sigma)
+    t1 = time.perf_counter()
+    nets = U.train_ensemble(ds, train, members=args.members, steps=args.sur_steps, config=cfg, engine=eng, log=log)
+    t_train = time.perf_counter() - t1
+    evals = [n.evaluate(ds, held) for n in nets]
+    for i, e in enumerate(evals):
+        log(f"member {i} held-out: " + ", ".join(f"{k} {v:.4g}" for k, v in e.items()))
+    if args.save_nets:
+        pathlib.Path(args.save_nets).mkdir(parents=True, exist_ok=True)
+        for i, n in enumerate(nets):
+            n.save(pathlib.Path(args.save_nets) / f"member{i}.npz")
+    ds.close()
+    res_p = S.run_plain(eng, n=args.sobol_n, seed=0)
+    log(f"plain sobol: {res_p.seconds}")
+    res_s = S.run_surrogate(eng, nets, n=args.sobol_n, seed=0, threshold=args.threshold)
+    log(f"surrogate sobol: {res_s.seconds}")
+    err = {}
+    for kind, a, b in (("S1", res_s.s1, res_p.s1), ("ST", res_s.st, res_p.st)):
+        for out in ("peak", "centroid"):
+            err[f"{kind}_{out}"] = max(abs(a[out][k] - b[out][k]) for k in a[out])
+    rel = {out: float(np.median(np.abs(res_s.metrics[out] / res_p.metrics[out] - 1))) for out in ("peak", "centroid")}
+    eng.close()
+    if rank == 0:
+        speed = res_p.seconds["total"] / res_s.seconds["total"]
+        out = {"metric": "surrogate speedup at <=1% error (Sobol indices, surrogate+fallback vs all-plain GPU)",
+               "value": speed, "unit": "x", "n_gpus": world, "steps": 1, "warmup": 0,
+               "ms_per_step": 1e3 * res_s.seconds["total"], "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+               "config": {"workload": f"surrogate: {args.sur_soils} 3-layer soils x 64 ranges x 512 bins labels, "
+                                      f"{args.members} x MLP 6x512 SiLU BF16 {args.sur_steps} steps batch 8192; "
+                                      f"Sobol N={args.sobol_n} d=8 at 10 m, fallback above {args.threshold:.0%} "
+                                      "ensemble spread"},
+               "index_abs_error": err, "median_rel_metric_error": rel,
+               "held_out": evals, "seconds": {"labels": t_data, "train": t_train,
+                                             "plain_sobol": res_p.seconds, "surrogate_sobol": res_s.seconds},
+               "sobol": {"surrogate": {"S1": res_s.s1, "ST": res_s.st}, "plain": {"S1": res_p.s1, "ST": res_p.st}}}
+        print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -334,11 +390,18 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--freq-stride", type=int, default=1,
                     help="profiling only: keep every n-th frequency (a smaller case of the same kernels)")
-    ap.add_argument("--workload", default="graded", choices=["graded", "batched", "sobol"],
+    ap.add_argument("--workload", default="graded", choices=["graded", "batched", "sobol", "surrogate"],
                     help="graded: the 10-layer graded soil (default); batched: seeded uneven soils; "
                          "sobol: the all-plain Sobol run")
     ap.add_argument("--sobol-n", type=int, default=16384, help="sobol workload: Saltelli base size N")
     ap.add_argument("--soils", type=int, default=4096, help="batched workload: number of soils")
+    ap.add_argument("--sur-soils", type=int, default=65536, help="surrogate workload: labelled soils")
+    ap.add_argument("--sur-steps", type=int, default=30000, help="surrogate workload: steps per member")
+    ap.add_argument("--sur-lr", type=float, default=1e-3)
+    ap.add_argument("--sur-sigma", type=float, default=8.0, help="Fourier feature frequency std")
+    ap.add_argument("--members", type=int, default=4, help="surrogate ensemble size")
+    ap.add_argument("--threshold", type=float, default=0.01, help="ensemble spread above which soils fall back")
+    ap.add_argument("--save-nets", default="", help="directory to save the trained members")
     ap.add_argument("--quadrature", default="split", choices=["split", "fp64"],
                     help="split: exact int8-slice tensor-core sum (default); fp64: the plain FP64 sum")
     ap.add_argument("--profile", action="store_true",
@@ -356,6 +419,8 @@ def main():
         return run_batched(args, gfk, torch, rank, world, local)
     if args.workload == "sobol":
         return run_sobol(args, gfk, torch, rank, world, local)
+    if args.workload == "surrogate":
+        return run_surrogate(args, gfk, torch, rank, world, local)
     wl = gfk.workloads.graded_soil()
     if args.freq_stride > 1:
         wl.freqs = wl.freqs[::args.freq_stride].copy()
