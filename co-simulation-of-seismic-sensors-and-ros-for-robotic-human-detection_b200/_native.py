@@ -18,6 +18,10 @@ REFERENCE_DIRECT = 0
 DUNKIN = 1
 PLAIN_FP64 = 0
 SPLIT_INT8 = 1
+LOSS_PLAIN = 0
+LOSS_COMPLEX = 1
+NET_TIMES = 6
+NET_FOURIER = 47
 
 # every symbol include/gfk.h declares
 EXPORTS = [
@@ -66,7 +70,8 @@ class GfkNetConfig(ctypes.Structure):
                 ("total_steps", ctypes.c_int32), ("lr_max", ctypes.c_float), ("lr_min", ctypes.c_float),
                 ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
                 ("weight_decay", ctypes.c_float), ("phase_weight", ctypes.c_float),
-                ("fourier_sigma", ctypes.c_float), ("seed", ctypes.c_uint64)]
+                ("fourier_sigma", ctypes.c_float), ("loss_mode", ctypes.c_int32), ("weight_floor", ctypes.c_float),
+                ("phase_cap", ctypes.c_float), ("_pad", ctypes.c_int32), ("seed", ctypes.c_uint64)]
 
 
 _lib = None
@@ -116,7 +121,7 @@ def lib():
         "gfk_vertical_displacement_multi_noalloc": (ctypes.c_int, [P(GfkMedium), P(GfkSolve), P(d), i32, d,
                                                                    GfkIntegration, P(d), vp]),
         "gfk_trace_metrics": (ctypes.c_int, [vp, vp, i64, i32, i32, P(d), i32, d, d, i32, i32, P(d), P(d)]),
-        "gfk_dataset_create": (ctypes.c_int, [vp, i32, i32, P(d), P(d), i32, P(d), i32, d, P(vp)]),
+        "gfk_dataset_create": (ctypes.c_int, [vp, i32, i32, P(d), P(d), P(d), i32, P(d), i32, d, P(vp)]),
         "gfk_dataset_fill": (ctypes.c_int, [vp, vp, i32, i32]),
         "gfk_dataset_stats": (ctypes.c_int, [vp, P(d)]),
         "gfk_dataset_labels": (ctypes.c_int, [vp, i32, P(f32)]),
@@ -124,12 +129,12 @@ def lib():
         "gfk_net_create": (ctypes.c_int, [vp, P(GfkNetConfig), P(vp)]),
         "gfk_net_set_scales": (ctypes.c_int, [vp, d, d, d, d, P(f32)]),
         "gfk_net_train": (ctypes.c_int, [vp, vp, P(i32), i32, i32, P(f32)]),
-        "gfk_net_predict": (ctypes.c_int, [vp, P(d), i32, P(d), i32, P(d), i32, vp, i32]),
+        "gfk_net_predict": (ctypes.c_int, [vp, P(d), P(d), i32, P(d), i32, P(d), i32, vp, i32]),
         "gfk_net_evaluate": (ctypes.c_int, [vp, vp, P(i32), i32, P(d)]),
         "gfk_net_param_count": (i64, [vp]),
         "gfk_net_params": (ctypes.c_int, [vp, P(f32), i64, i32]),
         "gfk_net_fourier": (ctypes.c_int, [vp, P(f32), i32]),
-        "gfk_net_probe": (ctypes.c_int, [vp, P(f32), P(f32), P(f32), P(f32)]),
+        "gfk_net_probe": (ctypes.c_int, [vp, P(f32), P(f32), P(f32), P(f32), P(f32)]),
         "gfk_net_destroy": (ctypes.c_int, [vp]),
     }
     for name, (res, args) in sig.items():

@@ -241,7 +241,7 @@ __device__ __forceinline__ int pick(unsigned long long h32, int n) {
 }
 
 struct PointScalars {
-    float ur, uf, lr, lf;
+    float ur, uf, lr, lf, f;
 };
 
 __device__ __forceinline__ PointScalars point_scalars(double r, double f, const FeatureDomain& d) {
@@ -250,9 +250,11 @@ __device__ __forceinline__ PointScalars point_scalars(double r, double f, const 
     p.uf = static_cast<float>((f - d.f_lo) / (d.f_hi - d.f_lo));
     p.lr = static_cast<float>(2.0 * log(r / d.r_lo) / log(d.r_hi / d.r_lo) - 1.0);
     p.lf = static_cast<float>(2.0 * log(f / d.f_lo) / log(d.f_hi / d.f_lo) - 1.0);
+    p.f = static_cast<float>(f);
     return p;
 }
 
+// sf: one soil table row (scalars at [0, 11), travel times at [16, 22)).
 __device__ __forceinline__ float feature(int j, const float* sf, const PointScalars& p, const float* four) {
     if (j < kMaxSoil) return sf[j];
     if (j < kScalars) {
@@ -264,7 +266,17 @@ __device__ __forceinline__ float feature(int j, const float* sf, const PointScal
             default: return 0.0f;
         }
     }
-    const int q = (j - kScalars) >> 1;
+    if (j < kLogTimeFeat) {
+        const int q = (j - kTimeFeat) >> 1;
+        float sn, cs;
+        sincospif(2.0f * (p.f * sf[kScalars + q]), &sn, &cs);
+        return (j & 1) ? cs : sn;
+    }
+    if (j < kFourierFeat) {
+        const float x = p.f * sf[kScalars + (j - kLogTimeFeat)];
+        return x > 0.0f ? fminf(fmaxf((logf(x) + 2.0f) / 3.0f, -2.0f), 2.0f) : -2.0f;
+    }
+    const int q = (j - kFourierFeat) >> 1;
     float sn, cs;
     sincospif(2.0f * (four[2 * q] * p.ur + four[2 * q + 1] * p.uf), &sn, &cs);
     return (j & 1) ? cs : sn;
@@ -298,11 +310,22 @@ __global__ void __launch_bounds__(kIn) k_batch(BatchArgs a) {
         const unsigned long long h2 = mix64(h);
         const int ir = pick(h2, a.nr), jf = pick(h2 >> 32, a.nf);
         const PointScalars p = point_scalars(a.ranges[ir], a.freqs[jf], a.dom);
-        tile[i][j] = __float2bfloat16_rn(feature(j, a.soilfeat + (size_t)soil * kScalars, p, a.fourier));
+        tile[i][j] = __float2bfloat16_rn(feature(j, a.soilfeat + (size_t)soil * kSoilStride, p, a.fourier));
         if (j == 0) {
             const float* L = a.labels + (((size_t)soil * a.nr + ir) * a.nf + jf) * 2;
+            const bool ph = !isnan(L[1]);
             a.Y[2 * b] = (L[0] - a.y_mean0) / a.y_std0;
             a.Y[2 * b + 1] = (L[1] - a.y_mean1) / a.y_std1;  // NaN stays NaN
+            float c0 = 1.0f, c1 = ph ? a.phase_weight : 0.0f;
+            if (a.loss_mode == 1) {
+                const float w = fmaxf(__expf(2.0f * (L[0] - a.lmax[(size_t)soil * a.nr + ir])), a.weight_floor);
+                const float wr = static_cast<float>(2.0 * 3.14159265358979323846 * a.freqs[jf] * a.ranges[ir]) *
+                                 (a.y_std1 / a.y_std0);
+                c0 = w;
+                c1 = ph ? a.phase_weight * w * fminf(wr * wr, a.phase_cap) : 0.0f;
+            }
+            a.C[2 * b] = c0;
+            a.C[2 * b + 1] = c1;
         }
     }
     __syncthreads();
@@ -315,12 +338,12 @@ __global__ void __launch_bounds__(kIn) k_batch(BatchArgs a) {
 // 8 warps x 4 rows; lane owns columns u*256 + lane*8 + e (u = 0, 1; e < 8).
 __global__ void __launch_bounds__(256) k_head_train(const bf16* __restrict__ H, const bf16* __restrict__ Z,
                                                     const float* __restrict__ W6, const float* __restrict__ b6,
-                                                    const float* __restrict__ Y, float pw, int B,
+                                                    const float* __restrict__ Y, const float* __restrict__ Cw, int B,
                                                     bf16* __restrict__ dZ, bf16* __restrict__ dZT,
                                                     float* __restrict__ gpart, float* __restrict__ lpart) {
     __shared__ __align__(16) bf16 tile[kHeadRows][kWidth + 8];
     __shared__ float red[2 * kWidth + 2];
-    __shared__ float lred[8][3];
+    __shared__ float lred[8][4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r0 = blockIdx.x * kHeadRows;
     float w0[16], w1[16], g0[16], g1[16];
@@ -334,7 +357,7 @@ __global__ void __launch_bounds__(256) k_head_train(const bf16* __restrict__ H, 
             g0[u * 8 + e] = 0.0f;
             g1[u * 8 + e] = 0.0f;
         }
-    float l0 = 0.0f, l1 = 0.0f, cnt = 0.0f, ds0 = 0.0f, ds1 = 0.0f;
+    float l0 = 0.0f, l1 = 0.0f, sc0 = 0.0f, sc1 = 0.0f, ds0 = 0.0f, ds1 = 0.0f;
     for (int t = 0; t < 4; t++) {
         const int rl = warp * 4 + t, row = r0 + rl;
         float h[16], z[16];
@@ -357,12 +380,14 @@ __global__ void __launch_bounds__(256) k_head_train(const bf16* __restrict__ H, 
         y0 += b6[0];
         y1 += b6[1];
         const float t0 = Y[2 * row], t1 = Y[2 * row + 1];
-        const bool ph = !isnan(t1);
+        const float c0 = Cw[2 * row], c1 = Cw[2 * row + 1];
+        const bool ph = !isnan(t1) && c1 > 0.0f;
         const float e0 = y0 - t0, e1 = ph ? y1 - t1 : 0.0f;
-        const float d0 = 2.0f * e0 / B, d1 = ph ? 2.0f * pw * e1 / B : 0.0f;
-        l0 += e0 * e0;
-        l1 += e1 * e1;
-        cnt += ph ? 1.0f : 0.0f;
+        const float d0 = 2.0f * c0 * e0 / B, d1 = ph ? 2.0f * c1 * e1 / B : 0.0f;
+        l0 += c0 * e0 * e0;
+        l1 += ph ? c1 * e1 * e1 : 0.0f;
+        sc0 += c0;
+        sc1 += ph ? c1 : 0.0f;
         ds0 += d0;
         ds1 += d1;
         float dz[16];
@@ -398,7 +423,8 @@ __global__ void __launch_bounds__(256) k_head_train(const bf16* __restrict__ H, 
                 red[2 * kWidth + 1] = (w ? red[2 * kWidth + 1] : 0.0f) + ds1;
                 lred[w][0] = l0;
                 lred[w][1] = l1;
-                lred[w][2] = cnt;
+                lred[w][2] = sc0;
+                lred[w][3] = sc1;
             }
         }
         __syncthreads();
@@ -406,16 +432,10 @@ __global__ void __launch_bounds__(256) k_head_train(const bf16* __restrict__ H, 
     for (int i = threadIdx.x; i < kHeadStride; i += blockDim.x)
         gpart[(size_t)blockIdx.x * kHeadStride + i] = i < 2 * kWidth + 2 ? red[i] : 0.0f;
     if (threadIdx.x == 0) {
-        float s0 = 0.0f, s1 = 0.0f, sc = 0.0f;
-        for (int w = 0; w < 8; w++) {
-            s0 += lred[w][0];
-            s1 += lred[w][1];
-            sc += lred[w][2];
-        }
-        lpart[blockIdx.x * 4 + 0] = s0;
-        lpart[blockIdx.x * 4 + 1] = s1;
-        lpart[blockIdx.x * 4 + 2] = sc;
-        lpart[blockIdx.x * 4 + 3] = 0.0f;
+        float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        for (int w = 0; w < 8; w++)
+            for (int q = 0; q < 4; q++) s[q] += lred[w][q];
+        for (int q = 0; q < 4; q++) lpart[blockIdx.x * 4 + q] = s[q];
     }
     // dZ^T: 32 consecutive rows of column c, 64 bytes per store group
     for (int c = threadIdx.x; c < kWidth; c += blockDim.x) {
@@ -514,24 +534,19 @@ __global__ void k_grad_flat(AdamArgs a, long long nparam, float* out) {
     out[i] = grad;
 }
 
-// One warp: fixed-order sums of the head kernel's loss partials.
+// One warp: fixed-order sums of the head kernel's loss partials; each slot
+// holds the step's two coefficient-weighted mean squared errors.
 __global__ void k_loss_hist(const float* lpart, int nblk, int B, const TrainScalars* ts, float* hist, int cap) {
-    float s0 = 0.0f, s1 = 0.0f, c = 0.0f;
-    for (int b = threadIdx.x; b < nblk; b += 32) {
-        s0 += lpart[4 * b];
-        s1 += lpart[4 * b + 1];
-        c += lpart[4 * b + 2];
-    }
+    float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int b = threadIdx.x; b < nblk; b += 32)
+        for (int q = 0; q < 4; q++) s[q] += lpart[4 * b + q];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-        c += __shfl_xor_sync(0xffffffffu, c, o);
-    }
+    for (int o = 16; o > 0; o >>= 1)
+        for (int q = 0; q < 4; q++) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
     if (threadIdx.x == 0) {
         const long long slot = (ts->step - 1) % cap;
-        hist[2 * slot] = s0 / B;
-        hist[2 * slot + 1] = c > 0.0f ? s1 / c : 0.0f;
+        hist[2 * slot] = s[2] > 0.0f ? s[0] / s[2] : 0.0f;
+        hist[2 * slot + 1] = s[3] > 0.0f ? s[1] / s[3] : 0.0f;
     }
 }
 
@@ -551,7 +566,7 @@ __global__ void __launch_bounds__(kIn) k_features(FeatureArgs a, long long rows_
             const int jf = static_cast<int>(t % a.nf);
             const long long s = t / a.nf;
             const PointScalars ps = point_scalars(a.ranges[ir], a.freqs[jf], a.dom);
-            v = feature(j, a.soilfeat + s * kScalars, ps, a.fourier);
+            v = feature(j, a.soilfeat + s * kSoilStride, ps, a.fourier);
         }
         a.X[q * kIn + j] = __float2bfloat16_rn(v);
     }
@@ -631,11 +646,12 @@ __global__ void __launch_bounds__(kLabelThreads) k_labels(LabelArgs a) {
     const double two_pi = 2.0 * CUDART_PI;
     if (tid < a.nr) {
         const int i = tid;
-        double dprev = 0.0, wprev = 0.0;
+        double dprev = 0.0, wprev = 0.0, rmax = 0.0;
         int n = 0;
         bool ok = true;
         for (int j = 0; j < a.nf; j++) {
             const cd g = G[(size_t)j * a.nr + i];
+            rmax = fmax(rmax, amp_of(g));
             const double w = atan2(g.im, g.re);
             if (i == 0) {
                 if (j > 0) {
@@ -657,6 +673,7 @@ __global__ void __launch_bounds__(kLabelThreads) k_labels(LabelArgs a) {
                 cyc[(size_t)i * a.nf + j] = ok ? static_cast<int16_t>(m) : kBroken;
             }
         }
+        a.lmax[(size_t)s * a.nr + i] = static_cast<float>(log(fmax(rmax, 1e-300)));
     }
     __syncthreads();
     double st[6] = {0, 0, 0, 0, 0, 0};
@@ -799,8 +816,8 @@ void launch_step_begin(cudaStream_t s, TrainScalars* ts) { k_step_begin<<<1, 1, 
 void launch_batch(cudaStream_t s, const BatchArgs& a) { k_batch<<<a.B / 32, kIn, 0, s>>>(a); }
 
 void launch_head_train(cudaStream_t s, const bf16* H, const bf16* Z, const float* W6, const float* b6, const float* Y,
-                       float pw, int B, bf16* dZ, bf16* dZT, float* gpart, float* lpart) {
-    k_head_train<<<B / kHeadRows, 256, 0, s>>>(H, Z, W6, b6, Y, pw, B, dZ, dZT, gpart, lpart);
+                       const float* C, int B, bf16* dZ, bf16* dZT, float* gpart, float* lpart) {
+    k_head_train<<<B / kHeadRows, 256, 0, s>>>(H, Z, W6, b6, Y, C, B, dZ, dZT, gpart, lpart);
 }
 
 void launch_bias_grad(cudaStream_t s, const bf16* const* dZT, int layers, int B, float* gb) {

@@ -12,10 +12,15 @@ namespace mlp {
 using bf16 = __nv_bfloat16;
 
 constexpr int kWidth = 512;    // hidden width
-constexpr int kIn = 128;       // input features (16 scalars + 56 Fourier pairs)
+constexpr int kIn = 128;       // input features
 constexpr int kScalars = 16;   // soil scalars (<= 11 used), range/frequency scalars
 constexpr int kMaxSoil = 11;   // soil parameters a network may take
-constexpr int kFourier = 56;   // Fourier pairs of (range, frequency)
+constexpr int kTimes = 6;      // vertical travel times per soil (h/Vs, h/Vp of up to 3 layers)
+constexpr int kTimeFeat = kScalars;                  // sin, cos(2 pi f T_q): [16, 28)
+constexpr int kLogTimeFeat = kTimeFeat + 2 * kTimes; // log-scaled f T_q: [28, 34)
+constexpr int kFourierFeat = kLogTimeFeat + kTimes;  // Fourier pairs of (range, frequency): [34, 128)
+constexpr int kFourier = (kIn - kFourierFeat) / 2;   // 47
+constexpr int kSoilStride = 32;  // soil table row: scalars [0, 11), travel times [16, 22)
 constexpr int kHeadRows = 32;  // rows per block of the head kernels
 constexpr int kHeadStride = 2 * kWidth + 2 + 2;  // head partial: dW6 [2][W], db6 [2], pad
 
@@ -60,13 +65,25 @@ struct FeatureDomain {
 };
 
 // The input row of one (soil, range, frequency) point:
-//   [0, 11)  soil scalars, mapped to [-1, 1]
-//   11, 12   range and frequency, linear on the domain, in [-1, 1]
-//   13, 14   their logarithms, in [-1, 1]
-//   16 + 2q, 17 + 2q   sin, cos(2 pi (B_q0 u_r + B_q1 u_f)), u in [0, 1]
+//   [0, 11)   soil scalars, mapped to [-1, 1]
+//   11, 12    range and frequency, linear on the domain, in [-1, 1]
+//   13, 14    their logarithms, in [-1, 1]
+//   16 + 2q, 17 + 2q   sin, cos(2 pi f T_q), T_q the soil's vertical travel times
+//   28 + q    (ln(f T_q) + 2) / 3, clamped to [-2, 2]
+//   34 + 2q, 35 + 2q   sin, cos(2 pi (B_q0 u_r + B_q1 u_f)), u in [0, 1]
+// The travel-time phases give the network the layer resonances (f T = 1/4,
+// 3/4, ...) directly instead of leaving it to synthesise oscillations whose
+// period depends on the soil.
+//
+// Loss per sample: c0 e0^2 + c1 e1^2 on the standardised errors, with
+//   mode 0: c0 = 1, c1 = phase_weight (0 where the phase is not learnt);
+//   mode 1 (complex): c0 = w, c1 = phase_weight w min((w_f r s1/s0)^2, cap),
+//   w = max(|G|^2 / max_f |G(r, .)|^2, weight_floor): the squared error of G
+//   relative to the soil's spectral peak at that range, phase in radians.
 struct BatchArgs {
     const float* labels;   // [nsoil][nr][nf][2]: log|G|, -phi/(w r) (NaN: phase not learnt)
-    const float* soilfeat; // [nsoil][16]
+    const float* lmax;     // [nsoil][nr]: log max_f |G|
+    const float* soilfeat; // [nsoil][kSoilStride]
     const int* train;      // soils the batch draws from
     int ntrain, nr, nf, B;
     const double* ranges;  // [nr]
@@ -74,21 +91,24 @@ struct BatchArgs {
     FeatureDomain dom;
     const float* fourier;  // [kFourier][2]
     float y_mean0, y_std0, y_mean1, y_std1;
+    int loss_mode;
+    float phase_weight, weight_floor, phase_cap;
     unsigned long long seed;
     const TrainScalars* ts;
     bf16* X;               // [B][kIn]
     bf16* XT;              // [kIn][B]
     float* Y;              // [B][2] standardised targets (NaN phase kept)
+    float* C;              // [B][2] loss coefficients
 };
 void launch_step_begin(cudaStream_t s, TrainScalars* ts);
 void launch_batch(cudaStream_t s, const BatchArgs& a);
 
-// The output layer (512 -> 2, FP32) and the squared-error loss; writes dz of
-// the last hidden layer (and its transpose), and per-block partials of dW6,
-// db6 [kHeadStride] and of the loss [4].
+// The output layer (512 -> 2, FP32) and the loss (1/B) sum c0 e0^2 + c1 e1^2;
+// writes dz of the last hidden layer (and its transpose), and per-block
+// partials of dW6, db6 [kHeadStride] and of the loss [4]: sum c0 e0^2,
+// sum c1 e1^2, sum c0, sum c1.
 void launch_head_train(cudaStream_t s, const bf16* H, const bf16* Z, const float* W6, const float* b6,
-                       const float* Y, float phase_weight, int B, bf16* dZ, bf16* dZT, float* gpart,
-                       float* lpart);
+                       const float* Y, const float* C, int B, bf16* dZ, bf16* dZT, float* gpart, float* lpart);
 // Column sums of dz^T rows: gb[l][o] = sum_b dZT_l[o][b] for `layers` layers.
 void launch_bias_grad(cudaStream_t s, const bf16* const* dZT, int layers, int B, float* gb);
 
@@ -123,7 +143,7 @@ void launch_loss_hist(cudaStream_t s, const float* lpart, int nblk, int B, const
 
 // Inference rows: row p = (soil * nf + jf) * nr + ir for soils [s0, s0 + ns).
 struct FeatureArgs {
-    const float* soilfeat;  // [ns][16] of the soils being evaluated
+    const float* soilfeat;  // [ns][kSoilStride] of the soils being evaluated
     int ns, nr, nf;
     long long p0, rows;     // first row and rows in this chunk
     const double* ranges;
@@ -157,6 +177,7 @@ struct LabelArgs {
     const double* freqs;
     double floor_rel;       // amplitude floor relative to the soil's maximum
     float* labels;          // [ns][nr][nf][2]
+    float* lmax;            // [ns][nr]: log max_f |G|
     double* stats;          // [ns][6]: n0, sum t0, sum t0^2, n1, sum t1, sum t1^2
 };
 int launch_labels(cudaStream_t s, const LabelArgs& a);

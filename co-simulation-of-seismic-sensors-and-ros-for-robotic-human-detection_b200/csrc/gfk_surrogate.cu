@@ -88,8 +88,9 @@ struct gfk_dataset {
     int nparam = 0, nsoil = 0, nr = 0, nf = 0;
     double floor_rel = 0;
     std::vector<double> ranges, freqs;
-    std::vector<float> soilfeat;  // [nsoil][16]
+    std::vector<float> soilfeat;  // [nsoil][kSoilStride]
     float* d_labels = nullptr;
+    float* d_lmax = nullptr;      // [nsoil][nr] log max_f |G|
     float* d_soilfeat = nullptr;
     double *d_ranges = nullptr, *d_freqs = nullptr, *d_stats = nullptr;
     std::vector<char> filled;
@@ -121,7 +122,7 @@ struct gfk_net {
     bf16 *X = nullptr, *XT = nullptr;
     float* Y = nullptr;
     bf16 *Z[kLayers] = {}, *H[kLayers] = {}, *HT[kLayers] = {}, *dZ[kLayers] = {}, *dZT[kLayers] = {};
-    float *gpart = nullptr, *lpart = nullptr, *gb = nullptr, *hist = nullptr, *gflat = nullptr;
+    float *Cw = nullptr, *gpart = nullptr, *lpart = nullptr, *gb = nullptr, *hist = nullptr, *gflat = nullptr;
     int* d_status = nullptr;
     int* d_train = nullptr;
     int ntrain = 0;
@@ -140,6 +141,7 @@ namespace {
 void dataset_free(gfk_dataset* d) {
     gfk_ctx* c = d->ctx;
     sfree(c, d->d_labels);
+    sfree(c, d->d_lmax);
     sfree(c, d->d_soilfeat);
     sfree(c, d->d_ranges);
     sfree(c, d->d_freqs);
@@ -163,8 +165,8 @@ void net_free(gfk_net* n) {
         sfree(c, n->dZ[l]);
         sfree(c, n->dZT[l]);
     }
-    float** fl[] = {&n->d_p, &n->d_m, &n->d_v, &n->d_four, &n->Y, &n->gpart, &n->lpart, &n->gb, &n->hist,
-                    &n->gflat, &n->iT};
+    float** fl[] = {&n->d_p, &n->d_m, &n->d_v, &n->d_four, &n->Y, &n->Cw, &n->gpart, &n->lpart, &n->gb,
+                    &n->hist, &n->gflat, &n->iT};
     for (float** q : fl) sfree(c, *q);
     sfree(c, n->d_ts);
     sfree(c, n->X);
@@ -210,7 +212,7 @@ int enqueue_fwd_bwd(gfk_net* n) {
         SG_TRY(gemm(n, M::kFwdTrain, l ? n->H[l - 1] : n->X, n->L[l].wb, B, kW, n->L[l].in, 1, g));
     }
     M::launch_head_train(s, n->H[kLayers - 1], n->Z[kLayers - 1], n->d_p + n->w6off, n->d_p + n->b6off, n->Y,
-                         n->cfg.phase_weight, B, n->dZ[kLayers - 1], n->dZT[kLayers - 1], n->gpart, n->lpart);
+                         n->Cw, B, n->dZ[kLayers - 1], n->dZT[kLayers - 1], n->gpart, n->lpart);
     n->ctx->launches++;
     for (int l = kLayers - 1; l >= 1; l--) {
         M::GemmArgs g{};
@@ -238,6 +240,7 @@ int enqueue_step(gfk_net* n, const gfk_dataset* d) {
     M::launch_step_begin(s, n->d_ts);
     M::BatchArgs b{};
     b.labels = d->d_labels;
+    b.lmax = d->d_lmax;
     b.soilfeat = d->d_soilfeat;
     b.train = n->d_train;
     b.ntrain = n->ntrain;
@@ -252,11 +255,16 @@ int enqueue_step(gfk_net* n, const gfk_dataset* d) {
     b.y_std0 = n->ms[1];
     b.y_mean1 = n->ms[2];
     b.y_std1 = n->ms[3];
+    b.loss_mode = n->cfg.loss_mode;
+    b.phase_weight = n->cfg.phase_weight;
+    b.weight_floor = n->cfg.weight_floor;
+    b.phase_cap = n->cfg.phase_cap > 0 ? n->cfg.phase_cap : 3.0e38f;
     b.seed = n->cfg.seed * 0x9e3779b97f4a7c15ULL + 17;
     b.ts = n->d_ts;
     b.X = n->X;
     b.XT = n->XT;
     b.Y = n->Y;
+    b.C = n->Cw;
     M::launch_batch(s, b);
     n->ctx->launches += 2;
     SG_TRY(enqueue_fwd_bwd(n));
@@ -276,10 +284,15 @@ int ensure_inference(gfk_net* n) {
     return GFK_OK;
 }
 
-std::vector<float> soil_table(const double* scalars, int ns, int np) {
-    std::vector<float> t((size_t)ns * M::kScalars, 0.0f);
-    for (int s = 0; s < ns; s++)
-        for (int j = 0; j < np; j++) t[(size_t)s * M::kScalars + j] = static_cast<float>(scalars[(size_t)s * np + j]);
+// Soil table rows: scalars at [0, np), travel times at [kScalars, kScalars + kTimes).
+std::vector<float> soil_table(const double* scalars, const double* times, int ns, int np) {
+    std::vector<float> t((size_t)ns * M::kSoilStride, 0.0f);
+    for (int s = 0; s < ns; s++) {
+        for (int j = 0; j < np; j++) t[(size_t)s * M::kSoilStride + j] = static_cast<float>(scalars[(size_t)s * np + j]);
+        if (times)
+            for (int q = 0; q < M::kTimes; q++)
+                t[(size_t)s * M::kSoilStride + M::kScalars + q] = static_cast<float>(times[(size_t)s * M::kTimes + q]);
+    }
     return t;
 }
 
@@ -370,8 +383,9 @@ int gfk_trace_metrics(gfk_ctx* ctx, const double* d_G, int64_t stride, int32_t n
     return GFK_OK;
 }
 
-int gfk_dataset_create(gfk_ctx* ctx, int32_t np, int32_t nsoil, const double* scalars, const double* ranges,
-                       int32_t nr, const double* freqs, int32_t nf, double floor_rel, gfk_dataset** out) {
+int gfk_dataset_create(gfk_ctx* ctx, int32_t np, int32_t nsoil, const double* scalars, const double* times,
+                       const double* ranges, int32_t nr, const double* freqs, int32_t nf, double floor_rel,
+                       gfk_dataset** out) {
     if (!ctx || !out || !scalars || !ranges || !freqs) return GFK_EARG;
     *out = nullptr;
     if (np < 1 || np > M::kMaxSoil || nsoil < 1 || nr < 1 || nr > 128 || nf < 1 || !(floor_rel > 0 && floor_rel < 1))
@@ -391,10 +405,17 @@ int gfk_dataset_create(gfk_ctx* ctx, int32_t np, int32_t nsoil, const double* sc
     d->floor_rel = floor_rel;
     d->ranges.assign(ranges, ranges + nr);
     d->freqs.assign(freqs, freqs + nf);
-    d->soilfeat = soil_table(scalars, nsoil, np);
+    if (times)
+        for (size_t i = 0; i < (size_t)nsoil * M::kTimes; i++)
+            if (!(times[i] >= 0) || times[i] > 1.0) {
+                delete d;
+                return sfail(ctx, GFK_EARG, "data set: travel times must lie in [0, 1] s");
+            }
+    d->soilfeat = soil_table(scalars, times, nsoil, np);
     d->filled.assign(nsoil, 0);
     int st = GFK_OK;
-    if ((st = salloc(ctx, &d->d_labels, (size_t)nsoil * nr * nf * 2)) || (st = salloc(ctx, &d->d_soilfeat, d->soilfeat.size())) ||
+    if ((st = salloc(ctx, &d->d_labels, (size_t)nsoil * nr * nf * 2)) || (st = salloc(ctx, &d->d_lmax, (size_t)nsoil * nr)) ||
+        (st = salloc(ctx, &d->d_soilfeat, d->soilfeat.size())) ||
         (st = salloc(ctx, &d->d_ranges, nr)) || (st = salloc(ctx, &d->d_freqs, nf)) ||
         (st = salloc(ctx, &d->d_stats, (size_t)nsoil * 6))) {
         dataset_free(d);
@@ -422,7 +443,8 @@ int gfk_dataset_fill(gfk_dataset* d, const double* d_G, int32_t first, int32_t n
     if (first < 0 || ns < 1 || first + ns > d->nsoil) return sfail(ctx, GFK_EARG, "data set fill: soils out of range");
     cudaSetDevice(ctx->device);
     M::LabelArgs a{reinterpret_cast<const cd*>(d_G), ns, d->nr, d->nf, d->d_ranges, d->d_freqs, d->floor_rel,
-                   d->d_labels + (size_t)first * d->nr * d->nf * 2, d->d_stats + (size_t)first * 6};
+                   d->d_labels + (size_t)first * d->nr * d->nf * 2, d->d_lmax + (size_t)first * d->nr,
+                   d->d_stats + (size_t)first * 6};
     if (M::launch_labels(ctx->stream, a)) return sfail(ctx, GFK_ECUDA, "label kernel refused");
     ctx->launches++;
     SG_CUDA(ctx, cudaGetLastError());
@@ -474,6 +496,8 @@ int gfk_net_create(gfk_ctx* ctx, const gfk_net_config* cfg, gfk_net** out) {
     if (cfg->nsoil_scalars < 1 || cfg->nsoil_scalars > M::kMaxSoil || cfg->batch < 128 || cfg->batch % 128 ||
         cfg->batch > (1 << 20))
         return sfail(ctx, GFK_EARG, "network: batch must be a positive multiple of 128 (<= 2^20)");
+    if (cfg->loss_mode != GFK_LOSS_PLAIN && cfg->loss_mode != GFK_LOSS_COMPLEX)
+        return sfail(ctx, GFK_EARG, "network: unknown loss mode %d", cfg->loss_mode);
     cudaSetDevice(ctx->device);
     if (M::prepare_gemm()) return sfail(ctx, GFK_ECUDA, "tensor-core GEMM kernels could not be configured");
     gfk_net* n = new gfk_net();
@@ -527,6 +551,7 @@ int gfk_net_create(gfk_ctx* ctx, const gfk_net_config* cfg, gfk_net** out) {
     A(&n->X, (size_t)n->B * M::kIn);
     A(&n->XT, (size_t)n->B * M::kIn);
     A(&n->Y, (size_t)n->B * 2);
+    A(&n->Cw, (size_t)n->B * 2);
     for (int l = 0; l < kLayers; l++) {
         NetLayer& L = n->L[l];
         A(&L.wb, (size_t)L.out * L.in);
@@ -676,15 +701,15 @@ int gfk_net_train(gfk_net* n, gfk_dataset* d, const int32_t* train, int32_t ntra
     return check_status(n);
 }
 
-int gfk_net_predict(gfk_net* n, const double* scalars, int32_t ns, const double* ranges, int32_t nr,
-                    const double* freqs, int32_t nf, double* out, int32_t on_device) {
+int gfk_net_predict(gfk_net* n, const double* scalars, const double* times, int32_t ns, const double* ranges,
+                    int32_t nr, const double* freqs, int32_t nf, double* out, int32_t on_device) {
     if (!n || !scalars || !ranges || !freqs || !out || ns < 0 || nr < 1 || nf < 1) return GFK_EARG;
     gfk_ctx* ctx = n->ctx;
     if (!n->scales) return sfail(ctx, GFK_EARG, "network scales are not set");
     if (ns == 0) return GFK_OK;
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
-    const std::vector<float> tab = soil_table(scalars, ns, n->cfg.nsoil_scalars);
+    const std::vector<float> tab = soil_table(scalars, times, ns, n->cfg.nsoil_scalars);
     float* d_soil = nullptr;
     double *d_r = nullptr, *d_f = nullptr;
     cd* d_G = nullptr;
@@ -719,9 +744,10 @@ int gfk_net_evaluate(gfk_net* n, gfk_dataset* d, const int32_t* soils, int32_t n
             return sfail(ctx, GFK_EARG, "evaluation soil %d is not a filled soil", soils[i]);
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
-    std::vector<float> tab((size_t)ns * M::kScalars);
+    std::vector<float> tab((size_t)ns * M::kSoilStride);
     for (int i = 0; i < ns; i++)
-        std::copy_n(d->soilfeat.begin() + (size_t)soils[i] * M::kScalars, M::kScalars, tab.begin() + (size_t)i * M::kScalars);
+        std::copy_n(d->soilfeat.begin() + (size_t)soils[i] * M::kSoilStride, M::kSoilStride,
+                    tab.begin() + (size_t)i * M::kSoilStride);
     float* d_soil = nullptr;
     int* d_ids = nullptr;
     cd* d_G = nullptr;
@@ -786,7 +812,7 @@ int gfk_net_fourier(gfk_net* n, float* host, int32_t set) {
     return GFK_OK;
 }
 
-int gfk_net_probe(gfk_net* n, const float* X, const float* Y, float* grad, float loss[2]) {
+int gfk_net_probe(gfk_net* n, const float* X, const float* Y, const float* coeffs, float* grad, float loss[2]) {
     if (!n || !X || !Y || !grad || !loss) return GFK_EARG;
     gfk_ctx* ctx = n->ctx;
     cudaSetDevice(ctx->device);
@@ -802,6 +828,12 @@ int gfk_net_probe(gfk_net* n, const float* X, const float* Y, float* grad, float
     SG_CUDA(ctx, cudaMemcpyAsync(n->X, xb.data(), xb.size() * 2, cudaMemcpyHostToDevice, s));
     SG_CUDA(ctx, cudaMemcpyAsync(n->XT, xt.data(), xt.size() * 2, cudaMemcpyHostToDevice, s));
     SG_CUDA(ctx, cudaMemcpyAsync(n->Y, Y, (size_t)B * 2 * 4, cudaMemcpyHostToDevice, s));
+    std::vector<float> cw((size_t)B * 2);
+    for (int b = 0; b < B; b++) {
+        cw[2 * b] = coeffs ? coeffs[2 * b] : 1.0f;
+        cw[2 * b + 1] = coeffs ? coeffs[2 * b + 1] : (std::isnan(Y[2 * b + 1]) ? 0.0f : n->cfg.phase_weight);
+    }
+    SG_CUDA(ctx, cudaMemcpyAsync(n->Cw, cw.data(), cw.size() * 4, cudaMemcpyHostToDevice, s));
     SG_TRY(enqueue_fwd_bwd(n));
     M::launch_grad_flat(s, n->adam, n->nparam, n->gflat);
     ctx->launches++;
@@ -811,14 +843,11 @@ int gfk_net_probe(gfk_net* n, const float* X, const float* Y, float* grad, float
     SG_CUDA(ctx, cudaMemcpyAsync(grad, n->gflat, n->nparam * 4, cudaMemcpyDeviceToHost, s));
     SG_CUDA(ctx, cudaMemcpyAsync(lp.data(), n->lpart, lp.size() * 4, cudaMemcpyDeviceToHost, s));
     SG_CUDA(ctx, cudaStreamSynchronize(s));
-    double s0 = 0, s1 = 0, c = 0;
-    for (int b = 0; b < nblk; b++) {
-        s0 += lp[4 * b];
-        s1 += lp[4 * b + 1];
-        c += lp[4 * b + 2];
-    }
-    loss[0] = (float)(s0 / B);
-    loss[1] = (float)(c > 0 ? s1 / c : 0.0);
+    double sm[4] = {0, 0, 0, 0};
+    for (int b = 0; b < nblk; b++)
+        for (int q = 0; q < 4; q++) sm[q] += lp[4 * b + q];
+    loss[0] = (float)(sm[2] > 0 ? sm[0] / sm[2] : 0.0);
+    loss[1] = (float)(sm[3] > 0 ? sm[1] / sm[3] : 0.0);
     return check_status(n);
 }
 

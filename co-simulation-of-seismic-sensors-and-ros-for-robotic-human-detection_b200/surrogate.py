@@ -75,7 +75,16 @@ def to_scalars(params):
     return out
 
 
-def from_sobol(p8, h3=1.0):
+def travel_times(params):
+    """Vertical S and P travel times of the three finite layers (s): the
+    network's resonance features, [h1/vs1, h2/vs2, h3/vs3, h1/vp1, h2/vp2, h3/vp3]."""
+    p = np.asarray(params, dtype=np.float64)
+    vs1, r1, _, h1, vs2, r2, _, h2, vs3, h3, _ = p.T
+    return np.ascontiguousarray(np.stack([h1 / vs1, h2 / vs2, h3 / vs3, h1 / (r1 * vs1), h2 / (r2 * vs2),
+                                          h3 / (DEEP_VPVS * vs3)], axis=1))
+
+
+def from_sobol(p8, h3=0.2):
     """Sobol rows (vs1, vpvs1, qs1, vs2, vpvs2, qs2, h1, vs_hs) as family rows."""
     p8 = np.asarray(p8, dtype=np.float64)
     vs1, r1, q1, vs2, r2, q2, h1, vsh = p8.T
@@ -150,12 +159,14 @@ class Dataset:
         self.grid = grid or LabelGrid()
         self.params = np.ascontiguousarray(params, dtype=np.float64)
         self.scalars = np.ascontiguousarray(to_scalars(self.params))
+        self.times = travel_times(self.params)
         self.floor_rel = floor_rel
         h = ctypes.c_void_p()
         r = np.ascontiguousarray(self.grid.ranges, dtype=np.float64)
         f = np.ascontiguousarray(self.grid.freqs, dtype=np.float64)
         self.engine.check(N.lib().gfk_dataset_create(self.engine.ctx, NPARAM, len(self.params), _dp(self.scalars),
-                                                     _dp(r), len(r), _dp(f), len(f), floor_rel, ctypes.byref(h)))
+                                                     _dp(self.times), _dp(r), len(r), _dp(f), len(f), floor_rel,
+                                                     ctypes.byref(h)))
         self.p = h
         self.engine._plans.add(self)
         self.solve_ms = 0.0
@@ -208,12 +219,15 @@ class NetConfig:
     weight_decay: float = 0.0
     phase_weight: float = 1.0
     fourier_sigma: float = 8.0
+    loss_mode: int = N.LOSS_COMPLEX
+    weight_floor: float = 1e-4
+    phase_cap: float = 1e4
     seed: int = 1
 
     def c(self):
         return N.GfkNetConfig(NPARAM, self.batch, self.warmup_steps, self.total_steps, self.lr_max, self.lr_min,
                               self.beta1, self.beta2, self.eps, self.weight_decay, self.phase_weight,
-                              self.fourier_sigma, self.seed)
+                              self.fourier_sigma, self.loss_mode, self.weight_floor, self.phase_cap, 0, self.seed)
 
 
 class Net:
@@ -244,9 +258,9 @@ class Net:
         self.engine.check(N.lib().gfk_net_params(self.p, _fp(v), len(v), 1))
 
     def fourier(self):
-        out = np.zeros(2 * 56, dtype=np.float32)
+        out = np.zeros(2 * N.NET_FOURIER, dtype=np.float32)
         self.engine.check(N.lib().gfk_net_fourier(self.p, _fp(out), 0))
-        return out.reshape(56, 2)
+        return out.reshape(N.NET_FOURIER, 2)
 
     def set_fourier(self, b):
         b = np.ascontiguousarray(b, dtype=np.float32).ravel()
@@ -273,13 +287,15 @@ class Net:
         self.steps_done += steps
         return loss
 
-    def probe(self, X, Y):
-        """One forward/backward pass on a given batch: (gradient, loss[2])."""
+    def probe(self, X, Y, C=None):
+        """One forward/backward pass on a given batch with loss coefficients
+        C [batch][2] (None: 1 and phase_weight): (gradient, loss[2])."""
         X = np.ascontiguousarray(X, dtype=np.float32)
         Y = np.ascontiguousarray(Y, dtype=np.float32)
+        Cp = None if C is None else _fp(np.ascontiguousarray(C, dtype=np.float32))
         grad = np.zeros(self.nparam, dtype=np.float32)
         loss = np.zeros(2, dtype=np.float32)
-        self.engine.check(N.lib().gfk_net_probe(self.p, _fp(X), _fp(Y), _fp(grad), _fp(loss)))
+        self.engine.check(N.lib().gfk_net_probe(self.p, _fp(X), _fp(Y), Cp, _fp(grad), _fp(loss)))
         return grad, loss
 
     # -- inference ----------------------------------------------------------
@@ -287,14 +303,15 @@ class Net:
         """G [soil, freq, range] for family rows `params`; written to device
         memory instead when out_device_ptr is given."""
         sc = np.ascontiguousarray(to_scalars(params))
+        tt = travel_times(params)
         r = np.ascontiguousarray(ranges, dtype=np.float64)
         f = np.ascontiguousarray(freqs, dtype=np.float64)
         if out_device_ptr is not None:
-            self.engine.check(N.lib().gfk_net_predict(self.p, _dp(sc), len(sc), _dp(r), len(r), _dp(f), len(f),
-                                                      ctypes.c_void_p(out_device_ptr), 1))
+            self.engine.check(N.lib().gfk_net_predict(self.p, _dp(sc), _dp(tt), len(sc), _dp(r), len(r), _dp(f),
+                                                      len(f), ctypes.c_void_p(out_device_ptr), 1))
             return None
         out = np.zeros((len(sc), len(f), len(r), 2))
-        self.engine.check(N.lib().gfk_net_predict(self.p, _dp(sc), len(sc), _dp(r), len(r), _dp(f), len(f),
+        self.engine.check(N.lib().gfk_net_predict(self.p, _dp(sc), _dp(tt), len(sc), _dp(r), len(r), _dp(f), len(f),
                                                   out.ctypes.data_as(ctypes.c_void_p), 0))
         return out[..., 0] + 1j * out[..., 1]
 
@@ -362,5 +379,5 @@ def train_ensemble(ds, train, members=4, steps=40000, config=None, engine=None, 
     return nets
 
 
-__all__ = ["PARAMS", "NPARAM", "soil_of", "draw", "from_unit", "to_scalars", "from_sobol", "LabelGrid", "Dataset",
+__all__ = ["PARAMS", "NPARAM", "soil_of", "draw", "from_unit", "to_scalars", "travel_times", "from_sobol", "LabelGrid", "Dataset",
            "NetConfig", "Net", "solve_media", "split_soils", "train_ensemble"]

@@ -277,14 +277,20 @@ int gfk_trace_metrics(gfk_ctx *ctx, const double *d_G, int64_t stride, int32_t n
 
 /* ---- surrogate network ---------------------------------------------------- */
 /* No counterpart in the reference (it has no learned component). A small
- * network maps (soil scalars, range, frequency) to the vertical displacement
- * spectrum as t0 = log|G| and t1 = -phi/(w r), phi the phase unwrapped along
- * range like internal/bank/interp.go:66-102: 128 input features (the soil
- * scalars, range and frequency, their logarithms and 56 Fourier pairs of
- * (range, frequency)), five SiLU layers of width 512 and a 2-wide FP32 output
- * layer. BF16 weights and activations, FP32 accumulation, FP32 master weights
- * and AdamW moments; every step runs libgfk's own forward, backward and
- * optimiser kernels and is replayed as one CUDA graph.
+ * network maps (soil, range, frequency) to the vertical displacement spectrum
+ * as t0 = log|G| and t1 = -phi/(w r), phi the phase unwrapped along range like
+ * internal/bank/interp.go:66-102: 128 input features, five SiLU layers of
+ * width 512 and a 2-wide FP32 output layer. BF16 weights and activations,
+ * FP32 accumulation, FP32 master weights and AdamW moments; every step runs
+ * libgfk's own forward, backward and optimiser kernels and is replayed as
+ * one CUDA graph.
+ *
+ * A soil is given as up to GFK_NET_MAX_SOIL scalars, already mapped to
+ * [-1, 1] by the caller, plus GFK_NET_TIMES vertical travel times in seconds
+ * (thickness / Vs and thickness / Vp of up to three layers; 0 where unused):
+ * the features carry sin, cos(2 pi f T) and log(f T) of each, which place the
+ * layer resonances. The other features are range and frequency and 47
+ * Fourier pairs of them.
  *
  * A data set holds the labels of nsoil soils over one range and frequency
  * grid in device memory, filled from device banks the solver produced. */
@@ -292,8 +298,19 @@ typedef struct gfk_dataset gfk_dataset;
 typedef struct gfk_net gfk_net;
 
 #define GFK_NET_MAX_SOIL 11
+#define GFK_NET_TIMES 6
 #define GFK_NET_WIDTH 512
 #define GFK_NET_INPUTS 128
+
+/* Loss per sample, on the standardised errors e0 (log-amplitude) and e1
+ * (phase slowness): c0 e0^2 + c1 e1^2 with
+ *   GFK_LOSS_PLAIN:   c0 = 1, c1 = phase_weight;
+ *   GFK_LOSS_COMPLEX: c0 = w, c1 = phase_weight w min((w_f r std1/std0)^2,
+ *                     phase_cap), w = max(|G|^2 / max_f |G(r, .)|^2,
+ *                     weight_floor) — the squared error of G itself relative
+ *                     to the spectral peak at that range, phase in radians.
+ * c1 = 0 where the phase is not learnt. */
+enum gfk_loss_mode { GFK_LOSS_PLAIN = 0, GFK_LOSS_COMPLEX = 1 };
 
 typedef struct {
     int32_t nsoil_scalars;  /* soil scalars per soil, <= GFK_NET_MAX_SOIL */
@@ -302,18 +319,22 @@ typedef struct {
     int32_t total_steps;    /* ... to lr_min at this step */
     float lr_max, lr_min;
     float beta1, beta2, eps, weight_decay;
-    float phase_weight;     /* loss weight of the phase target */
+    float phase_weight;
     float fourier_sigma;    /* std of the Fourier frequencies, cycles per domain */
+    int32_t loss_mode;      /* enum gfk_loss_mode */
+    float weight_floor;     /* GFK_LOSS_COMPLEX: smallest amplitude weight */
+    float phase_cap;        /* GFK_LOSS_COMPLEX: cap on the phase error's scale */
+    int32_t _pad;
     uint64_t seed;          /* initial weights, Fourier frequencies, batches */
 } gfk_net_config;
 
-/* Soil scalars are given already mapped to [-1, 1] by the caller. Labels are
- * built from banks with an amplitude floor floor_rel times the soil's largest
- * |G|: t0 is clamped at the floor, and a cell's phase is not learnt once its
- * unwrapping chain has met a cell below it. nr <= 128. */
+/* Labels are built from banks with an amplitude floor floor_rel times the
+ * soil's largest |G|: t0 is clamped at the floor, and a cell's phase is not
+ * learnt once its unwrapping chain has met a cell below it. nr <= 128.
+ * soil_times: [nsoil][GFK_NET_TIMES] or NULL (all zero). */
 int gfk_dataset_create(gfk_ctx *ctx, int32_t nsoil_scalars, int32_t nsoil, const double *soil_scalars,
-                       const double *ranges_m, int32_t nr, const double *freqs_hz, int32_t nf,
-                       double floor_rel, gfk_dataset **out);
+                       const double *soil_times, const double *ranges_m, int32_t nr, const double *freqs_hz,
+                       int32_t nf, double floor_rel, gfk_dataset **out);
 /* Labels of soils [first_soil, first_soil + nsoil) from the device bank d_G
  * [nsoil][nf][nr] (re, im) pairs (gfk_plan_result_device of a batch plan). */
 int gfk_dataset_fill(gfk_dataset *ds, const double *d_G, int32_t first_soil, int32_t nsoil);
@@ -331,14 +352,16 @@ int gfk_net_create(gfk_ctx *ctx, const gfk_net_config *cfg, gfk_net **out);
 int gfk_net_set_scales(gfk_net *net, double r_lo, double r_hi, double f_lo, double f_hi,
                        const float mean_std[4]);
 /* `steps` optimiser steps on batches drawn uniformly from the cells of the
- * listed soils. loss (optional, host [steps][2]) receives each step's mean
- * squared error of the two standardised targets. */
+ * listed soils. loss (optional, host [steps][2]) receives each step's
+ * coefficient-weighted mean squared errors of the two standardised targets. */
 int gfk_net_train(gfk_net *net, gfk_dataset *ds, const int32_t *train_soils, int32_t ntrain,
                   int32_t steps, float *loss);
 /* G for ns soils at every (frequency, range) pair: out[2 ((s nf + j) nr + i)]
- * (re, im). out is device memory when out_on_device is nonzero. */
-int gfk_net_predict(gfk_net *net, const double *soil_scalars, int32_t ns, const double *ranges_m,
-                    int32_t nr, const double *freqs_hz, int32_t nf, double *out, int32_t out_on_device);
+ * (re, im). out is device memory when out_on_device is nonzero. soil_times
+ * as in gfk_dataset_create. */
+int gfk_net_predict(gfk_net *net, const double *soil_scalars, const double *soil_times, int32_t ns,
+                    const double *ranges_m, int32_t nr, const double *freqs_hz, int32_t nf, double *out,
+                    int32_t out_on_device);
 /* Held-out error against the data set's labels for the listed soils, over the
  * data set's grid: out = {cells, sum e0^2, phase cells, sum e1^2,
  * sum (e1 w r)^2, sum |G_pred - G|^2, sum |G|^2}. */
@@ -347,13 +370,16 @@ int64_t gfk_net_param_count(const gfk_net *net);
 /* Get (set = 0) or set (set != 0) the FP32 master parameters, n floats:
  * W1 [512][128], b1, W2..W5 [512][512] and their biases, W6 [2][512], b6 [2]. */
 int gfk_net_params(gfk_net *net, float *host, int64_t n, int32_t set);
-/* Get or set the 56 x 2 Fourier frequencies. */
+/* Get or set the 47 x 2 Fourier frequencies. */
 int gfk_net_fourier(gfk_net *net, float *host, int32_t set);
 /* One forward and backward pass on a given batch without an update, for
  * gradient checks: X host [batch][128] features, Y host [batch][2]
- * standardised targets (NaN: no phase term). grad receives the full gradient
- * of the loss (layout of gfk_net_params), loss the two mean squared errors. */
-int gfk_net_probe(gfk_net *net, const float *X, const float *Y, float *grad, float loss[2]);
+ * standardised targets (NaN: no phase term), coeffs host [batch][2] loss
+ * coefficients (c0, c1) or NULL for (1, phase_weight). grad receives the
+ * gradient of (1/batch) sum c0 e0^2 + c1 e1^2 (layout of gfk_net_params),
+ * loss the two coefficient-weighted mean squared errors. */
+int gfk_net_probe(gfk_net *net, const float *X, const float *Y, const float *coeffs, float *grad,
+                  float loss[2]);
 int gfk_net_destroy(gfk_net *net);
 
 #ifdef __cplusplus

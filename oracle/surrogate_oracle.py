@@ -18,7 +18,11 @@ import math
 
 import numpy as np
 
-WIDTH, INPUTS, LAYERS, FOURIER, SCALARS = 512, 128, 5, 56, 16
+WIDTH, INPUTS, LAYERS, SCALARS, TIMES = 512, 128, 5, 16, 6
+TIME_FEAT = SCALARS                      # sin, cos(2 pi f T_q)
+LOG_TIME_FEAT = TIME_FEAT + 2 * TIMES    # (ln(f T_q) + 2) / 3 clamped to [-2, 2]
+FOURIER_FEAT = LOG_TIME_FEAT + TIMES     # Fourier pairs of (range, frequency)
+FOURIER = (INPUTS - FOURIER_FEAT) // 2
 
 
 def bf16(x):
@@ -79,24 +83,33 @@ def labels(G, ranges, freqs, floor_rel):
 
 # ---------------------------------------------------------------- features --
 
-def features(scalars, r, f, dom, fourier):
-    """Input rows for points (soil scalars [n][<=11], r [n], f [n]); dom =
-    (r_lo, r_hi, f_lo, f_hi); fourier [56][2]."""
+def features(scalars, times, r, f, dom, fourier):
+    """Input rows for points (soil scalars [n][<=11], travel times [n][6],
+    r [n], f [n]); dom = (r_lo, r_hi, f_lo, f_hi); fourier [47][2]."""
     scalars = np.atleast_2d(scalars)
+    times = np.atleast_2d(times)
+    r = np.asarray(r, dtype=np.float64)
+    f = np.asarray(f, dtype=np.float64)
     n = len(r)
     r_lo, r_hi, f_lo, f_hi = dom
-    ur = (np.asarray(r) - r_lo) / (r_hi - r_lo)
-    uf = (np.asarray(f) - f_lo) / (f_hi - f_lo)
+    ur = (r - r_lo) / (r_hi - r_lo)
+    uf = (f - f_lo) / (f_hi - f_lo)
     X = np.zeros((n, INPUTS))
     X[:, :scalars.shape[1]] = scalars
     X[:, 11] = 2 * ur - 1
     X[:, 12] = 2 * uf - 1
-    X[:, 13] = 2 * np.log(np.asarray(r) / r_lo) / math.log(r_hi / r_lo) - 1
-    X[:, 14] = 2 * np.log(np.asarray(f) / f_lo) / math.log(f_hi / f_lo) - 1
+    X[:, 13] = 2 * np.log(r / r_lo) / math.log(r_hi / r_lo) - 1
+    X[:, 14] = 2 * np.log(f / f_lo) / math.log(f_hi / f_lo) - 1
+    ft = f[:, None] * times
+    X[:, TIME_FEAT:LOG_TIME_FEAT:2] = np.sin(2 * math.pi * ft)
+    X[:, TIME_FEAT + 1:LOG_TIME_FEAT:2] = np.cos(2 * math.pi * ft)
+    with np.errstate(divide="ignore"):
+        lt = np.where(ft > 0, (np.log(np.where(ft > 0, ft, 1.0)) + 2) / 3, -2.0)
+    X[:, LOG_TIME_FEAT:FOURIER_FEAT] = np.clip(lt, -2, 2)
     B = np.asarray(fourier, dtype=np.float64).reshape(FOURIER, 2)
     arg = 2 * math.pi * (ur[:, None] * B[None, :, 0] + uf[:, None] * B[None, :, 1])
-    X[:, SCALARS::2] = np.sin(arg)
-    X[:, SCALARS + 1::2] = np.cos(arg)
+    X[:, FOURIER_FEAT::2] = np.sin(arg)
+    X[:, FOURIER_FEAT + 1::2] = np.cos(arg)
     return X
 
 
@@ -151,19 +164,28 @@ def forward(p, X, emulate=True):
     return y, cache
 
 
-def backward(p, X, Y, phase_weight=1.0, emulate=True):
-    """(gradient in the flat parameter layout, (mse0, mse1)) for targets Y
-    [B][2] (NaN phase: no phase term)."""
+def coefficients(Y, phase_weight=1.0):
+    """The plain loss's coefficients: (1, phase_weight), 0 where no phase."""
+    Y = np.asarray(Y, dtype=np.float64)
+    return np.stack([np.ones(len(Y)), np.where(np.isnan(Y[:, 1]), 0.0, phase_weight)], axis=1)
+
+
+def backward(p, X, Y, C=None, emulate=True):
+    """(gradient in the flat parameter layout, (weighted mse0, weighted mse1))
+    of (1/B) sum_b c0 e0^2 + c1 e1^2 for targets Y [B][2] (NaN phase: no
+    phase term) and coefficients C [B][2] (None: plain, weight 1)."""
     layers, w6o, b6o, n = layout()
     Ws, bs, W6, b6 = unpack(p)
     rnd = bf16 if emulate else (lambda a: np.asarray(a, dtype=np.float64))
     y, c = forward(p, X, emulate)
     B = len(X)
     Y = np.asarray(Y, dtype=np.float64)
-    m = ~np.isnan(Y[:, 1])
+    C = coefficients(Y) if C is None else np.asarray(C, dtype=np.float64)
+    m = ~np.isnan(Y[:, 1]) & (C[:, 1] > 0)
     e0 = y[:, 0] - Y[:, 0]
     e1 = np.where(m, y[:, 1] - np.where(m, Y[:, 1], 0.0), 0.0)
-    d = np.stack([2 * e0 / B, 2 * phase_weight * e1 / B], axis=1)
+    c1 = np.where(m, C[:, 1], 0.0)
+    d = np.stack([2 * C[:, 0] * e0 / B, 2 * c1 * e1 / B], axis=1)
     g = np.zeros(n)
     h5 = c["h"]
     g[w6o:w6o + 2 * WIDTH] = (d.T @ h5).ravel()
@@ -177,19 +199,31 @@ def backward(p, X, Y, phase_weight=1.0, emulate=True):
         g[w:w + WIDTH * fi] = (dz.T @ c["in"][l]).ravel()
         g[b:b + WIDTH] = dz.sum(axis=0)
         dh = dz @ c["Wb"][l]
-    mse0 = float(np.mean(e0 ** 2))
-    mse1 = float(np.sum(e1 ** 2) / max(m.sum(), 1))
+    mse0 = float(np.sum(C[:, 0] * e0 ** 2) / max(C[:, 0].sum(), 1e-300))
+    mse1 = float(np.sum(c1 * e1 ** 2) / max(c1.sum(), 1e-300))
     return g, (mse0, mse1)
 
 
-def loss(p, X, Y, phase_weight=1.0):
-    """The training loss (1/B) sum [e0^2 + w m e1^2] in FP64 without rounding."""
+def loss(p, X, Y, C=None):
+    """The training loss (1/B) sum c0 e0^2 + c1 e1^2 in FP64 without rounding."""
     y, _ = forward(p, X, emulate=False)
     Y = np.asarray(Y, dtype=np.float64)
-    m = ~np.isnan(Y[:, 1])
+    C = coefficients(Y) if C is None else np.asarray(C, dtype=np.float64)
+    m = ~np.isnan(Y[:, 1]) & (C[:, 1] > 0)
     e0 = y[:, 0] - Y[:, 0]
     e1 = np.where(m, y[:, 1] - np.where(m, Y[:, 1], 0.0), 0.0)
-    return float(np.mean(e0 ** 2 + phase_weight * e1 ** 2))
+    return float(np.mean(C[:, 0] * e0 ** 2 + np.where(m, C[:, 1], 0.0) * e1 ** 2))
+
+
+def loss_coefficients(labels_t0, labels_t1, lmax, f, r, mean_std, phase_weight=1.0, weight_floor=1e-4,
+                      phase_cap=1e4):
+    """The complex loss's coefficients (k_batch, loss mode 1) for cells with
+    labels (t0, t1), log max_f |G| at their range, frequency and range."""
+    s0, s1 = mean_std[1], mean_std[3]
+    w = np.maximum(np.exp(2 * (np.asarray(labels_t0) - lmax)), weight_floor)
+    wr = 2 * math.pi * np.asarray(f) * np.asarray(r) * (s1 / s0)
+    c1 = np.where(np.isnan(labels_t1), 0.0, phase_weight * w * np.minimum(wr * wr, phase_cap))
+    return np.stack([w, c1], axis=1)
 
 
 def adam_step(p, m, v, g, t, lr, beta1=0.9, beta2=0.999, eps=1e-8, wd=0.0):

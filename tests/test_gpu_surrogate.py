@@ -45,9 +45,11 @@ def test_gradients_match_oracle(pkg, eng):
     X = rng.uniform(-1, 1, (256, 128)).astype(np.float32)
     Y = rng.normal(size=(256, 2)).astype(np.float32)
     Y[::7, 1] = np.nan
-    g_gpu, loss = net.probe(X, Y)
-    g_emu, (m0, m1) = SO.backward(p, X, Y, phase_weight=net.config.phase_weight, emulate=True)
-    g_ref, _ = SO.backward(p, X, Y, phase_weight=net.config.phase_weight, emulate=False)
+    C = rng.uniform(0.05, 2.0, (256, 2)).astype(np.float32)  # complex-loss-like per-sample weights
+    C[::7, 1] = 0.0
+    g_gpu, loss = net.probe(X, Y, C)
+    g_emu, (m0, m1) = SO.backward(p, X, Y, C, emulate=True)
+    g_ref, _ = SO.backward(p, X, Y, C, emulate=False)
     assert abs(loss[0] - m0) <= 2e-3 * m0 and abs(loss[1] - m1) <= 2e-3 * m1
     layers, w6, b6, n = SO.layout()
     segs = [(w, w + SO.WIDTH * fi) for (w, _, fi) in layers] + [(b, b + SO.WIDTH) for (_, b, _) in layers]
@@ -72,10 +74,11 @@ def test_predict_matches_oracle_forward(pkg, eng):
     p = net.params().astype(np.float64)
     B = net.fourier()
     sc = sur.to_scalars(params)
+    tt = sur.travel_times(params)
     for s in range(3):
         rr, ff = np.meshgrid(ranges, freqs)
-        X = SO.features(np.repeat(sc[s:s + 1], rr.size, axis=0), rr.ravel(), ff.ravel(),
-                        (1.0, 64.0, 500 / 512, 500.0), B)
+        X = SO.features(np.repeat(sc[s:s + 1], rr.size, axis=0), np.repeat(tt[s:s + 1], rr.size, axis=0),
+                        rr.ravel(), ff.ravel(), (1.0, 64.0, 500 / 512, 500.0), B)
         y, _ = SO.forward(p, X, emulate=True)
         t0 = y[:, 0] * ms[1] + ms[0]
         t1 = y[:, 1] * ms[3] + ms[2]

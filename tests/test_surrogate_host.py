@@ -40,7 +40,8 @@ def test_oracle_gradient_matches_finite_differences():
     X = rng.uniform(-1, 1, (6, SO.INPUTS))
     Y = rng.normal(size=(6, 2))
     Y[2, 1] = np.nan  # a row without a phase term
-    g, _ = SO.backward(p, X, Y, phase_weight=0.7, emulate=False)
+    C = rng.uniform(0.1, 3.0, (6, 2))  # per-sample loss coefficients
+    g, _ = SO.backward(p, X, Y, C, emulate=False)
     layers, w6, b6, n = SO.layout()
     picks = [layers[0][0] + 5, layers[0][1] + 3, layers[2][0] + 1000, layers[4][0] + 77, layers[4][1] + 9,
              w6 + 3, w6 + SO.WIDTH + 11, b6, b6 + 1]
@@ -49,7 +50,7 @@ def test_oracle_gradient_matches_finite_differences():
         pp, pm = p.copy(), p.copy()
         pp[i] += h
         pm[i] -= h
-        fd = (SO.loss(pp, X, Y, 0.7) - SO.loss(pm, X, Y, 0.7)) / (2 * h)
+        fd = (SO.loss(pp, X, Y, C) - SO.loss(pm, X, Y, C)) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)) + 1e-9, (i, fd, g[i])
 
 
@@ -136,12 +137,18 @@ def test_scalars_and_features(pkg):
     lo = np.array([[p[1] for p in sur.PARAMS]])
     hi = np.array([[p[2] for p in sur.PARAMS]])
     assert np.allclose(sur.to_scalars(lo), -1) and np.allclose(sur.to_scalars(hi), 1)
-    B = np.random.default_rng(5).normal(0, 8, (56, 2))
-    X = SO.features(sur.to_scalars(lo), np.array([1.0]), np.array([500.0]), (1.0, 64.0, 500 / 512, 500.0), B)
-    assert X.shape == (1, 128)
+    B = np.random.default_rng(5).normal(0, 8, (SO.FOURIER, 2))
+    T = sur.travel_times(lo)
+    X = SO.features(sur.to_scalars(lo), T, np.array([1.0]), np.array([500.0]), (1.0, 64.0, 500 / 512, 500.0), B)
+    assert X.shape == (1, 128) and SO.FOURIER == 47
     assert X[0, 11] == -1 and X[0, 12] == 1 and X[0, 13] == -1 and X[0, 14] == 1 and X[0, 15] == 0
-    assert np.allclose(X[0, 16::2], np.sin(2 * np.pi * B[:, 1]))
-    assert np.allclose(X[0, 17::2], np.cos(2 * np.pi * B[:, 1]))
+    ft = 500.0 * T[0]
+    assert np.allclose(X[0, 16:28:2], np.sin(2 * np.pi * ft)) and np.allclose(X[0, 17:28:2], np.cos(2 * np.pi * ft))
+    assert np.allclose(X[0, 28:34], np.clip((np.log(ft) + 2) / 3, -2, 2))
+    assert np.allclose(X[0, 34::2], np.sin(2 * np.pi * B[:, 1]))
+    assert np.allclose(X[0, 35::2], np.cos(2 * np.pi * B[:, 1]))
+    # the first soil's S travel time through layer 1 is h1 / vs1
+    assert np.isclose(T[0, 0], lo[0, 3] / lo[0, 0]) and np.isclose(T[0, 5], lo[0, 9] / (2 * lo[0, 8]))
 
 
 def test_draw_and_split(pkg):
