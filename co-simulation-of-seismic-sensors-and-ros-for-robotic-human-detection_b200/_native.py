@@ -33,7 +33,7 @@ EXPORTS = [
     "gfk_plan_launches_per_execute", "gfk_plan_tuning", "gfk_plan_kernel_times", "gfk_plan_destroy",
     "gfk_plan_use_graph", "gfk_batch_create",
     "gfk_bank_pack", "gfk_bank_write", "gfk_vertical_displacement_multi_noalloc",
-    "gfk_trace_metrics",
+    "gfk_trace_metrics", "gfk_bank_tables", "gfk_bank_impulse_responses",
     "gfk_dataset_create", "gfk_dataset_fill", "gfk_dataset_stats", "gfk_dataset_labels", "gfk_dataset_destroy",
     "gfk_net_create", "gfk_net_set_scales", "gfk_net_train", "gfk_net_predict", "gfk_net_evaluate",
     "gfk_net_param_count", "gfk_net_params", "gfk_net_fourier", "gfk_net_probe", "gfk_net_destroy",
@@ -120,6 +120,9 @@ def lib():
         "gfk_bank_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, P(ctypes.c_float), i64]),
         "gfk_vertical_displacement_multi_noalloc": (ctypes.c_int, [P(GfkMedium), P(GfkSolve), P(d), i32, d,
                                                                    GfkIntegration, P(d), vp]),
+        "gfk_bank_tables": (ctypes.c_int, [vp, P(f32), i32, i32, P(d), P(d)]),
+        "gfk_bank_impulse_responses": (ctypes.c_int, [vp, P(f32), i32, i32, d, d, d, i32, P(d), i32, P(d), i32, i32,
+                                                      P(d)]),
         "gfk_trace_metrics": (ctypes.c_int, [vp, vp, i64, i32, i32, P(d), i32, d, d, i32, i32, P(d), P(d)]),
         "gfk_dataset_create": (ctypes.c_int, [vp, i32, i32, P(d), P(d), P(d), i32, P(d), i32, d, P(vp)]),
         "gfk_dataset_fill": (ctypes.c_int, [vp, vp, i32, i32]),

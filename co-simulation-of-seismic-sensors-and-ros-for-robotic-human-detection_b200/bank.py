@@ -194,6 +194,47 @@ class Bank:
     def size_bytes(self):
         return 4 * self.data.size
 
+    def _payload(self):
+        return np.ascontiguousarray(self.data, dtype=np.float32)
+
+    def tables(self, engine=None):
+        """Bank.prepare (internal/bank/interp.go:66-102) on the GPU: the FP64
+        log-magnitude and range-unwrapped phase tables, [count, bins] each."""
+        from .fk import default_engine
+        eng = engine or default_engine()
+        c, b = self.header.ranges.count, self.header.bins()
+        lm = np.zeros((c, b))
+        ph = np.zeros((c, b))
+        pl = self._payload()
+        eng.check(N.lib().gfk_bank_tables(eng.ctx, pl.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), c, b,
+                                          lm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                          ph.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return lm, ph
+
+    def impulse_responses(self, ranges, length, sensor=None, velocity=True, engine=None):
+        """Causal impulse responses at the given ranges, as internal/sensing
+        builds them from a bank (sensing.go:196-204): Bank.Response at every
+        bin, times i w (velocity) and the sensor's complex response per bin
+        (`sensor`, length bins, or None), through dsp.CausalImpulseResponseAt
+        with the bank's transform size. [len(ranges), length] on the GPU."""
+        from .fk import default_engine
+        eng = engine or default_engine()
+        h = self.header
+        r = np.ascontiguousarray(ranges, dtype=np.float64)
+        out = np.zeros((len(r), int(length)))
+        sp = None
+        if sensor is not None:
+            sc = np.asarray(sensor, dtype=np.complex128)
+            sa = np.ascontiguousarray(np.stack([sc.real, sc.imag], axis=1).ravel())
+            sp = sa.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        pl = self._payload()
+        eng.check(N.lib().gfk_bank_impulse_responses(
+            eng.ctx, pl.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), h.ranges.count, h.bins(),
+            float(h.ranges.min_m), float(h.ranges.max_m), float(h.sample_rate_hz), int(h.samples),
+            r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r), sp, 1 if velocity else 0, int(length),
+            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
     def write(self, path):
         """bank.Write (format.go:215-240), through libgfk's gfk_bank_write."""
         self.header.validate()

@@ -1,0 +1,263 @@
+// gfk_consume.cu — bank consumption on the GPU: the interpolation tables of
+// Bank.prepare, Bank.Response between grid ranges, and the causal impulse
+// responses a sensor engine builds from them.
+//
+//   tables     internal/bank/interp.go:66-102 — per bin, walking the range
+//              axis: log|v| (-1e308 for an exact zero) and the phase unwrapped
+//              by folding each step into (-pi, pi]; FP64 from the FP32 payload.
+//   response   internal/bank/interp.go:29-54 with format.go:295-309's bracket:
+//              linear in log-magnitude and in unwrapped phase between the two
+//              bracketing ranges; zero where either end is an exact zero.
+//   impulse    internal/dsp/dsp.go:232-261 (CausalImpulseResponseAt) at the
+//              bank's own transform size, fed as internal/sensing does
+//              (sensing.go:196-204, propagation.go:84-104): velocity i w u(r, f)
+//              times the sensor's response, tapered above 0.8 Nyquist,
+//              inverse-transformed (1/n), the first `length` samples kept.
+//
+// One thread per bin builds the tables (the unwrap is sequential in range);
+// one block per query range builds its spectrum in shared memory and runs the
+// n-point FFT there (gfk_fft.cuh), n = the bank's Samples <= 4096.
+#include <cmath>
+#include <vector>
+
+#include "../../include/gfk.h"
+#include "gfk_ctx.h"
+#include "gfk_fft.cuh"
+#include "gfk_kernels.cuh"
+
+namespace gfk {
+namespace consume {
+
+constexpr double kNegInf = -1e308;  // interp.go:56
+constexpr int kThreads = 256;
+constexpr int kMaxSamples = 4096;
+
+__global__ void k_tables(const float* __restrict__ data, int count, int bins, double* __restrict__ logmag,
+                         double* __restrict__ phase) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= bins) return;
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    double prev = 0.0, unwrapped = 0.0;
+    for (int i = 0; i < count; i++) {
+        const size_t j = (size_t)i * bins + k;
+        const double re = data[2 * j], im = data[2 * j + 1];
+        const double mag = hypot(re, im);
+        if (mag == 0.0) {
+            logmag[j] = kNegInf;
+            phase[j] = unwrapped;
+            continue;
+        }
+        logmag[j] = log(mag);
+        const double w = atan2(im, re);
+        if (i == 0) {
+            unwrapped = w;
+        } else {
+            double d = w - prev;
+            d -= two_pi * round(d / two_pi);  // halves away from zero, as Go's math.Round
+            unwrapped += d;
+        }
+        prev = w;
+        phase[j] = unwrapped;
+    }
+}
+
+struct ImpulseArgs {
+    const double* logmag;
+    const double* phase;
+    int count, bins, n, length;
+    const int* lo;          // [nq] lower bracketing range index
+    const double* frac;     // [nq]
+    const cd* sensor;       // [bins] or null
+    int velocity;
+    double fs;
+    const cd* tw;           // [n/2]
+    double* out;            // [nq][length]
+};
+
+__global__ void __launch_bounds__(kThreads) k_impulse(ImpulseArgs a) {
+    extern __shared__ cd buf[];  // [2][n]
+    cd* x = buf;
+    cd* y = buf + a.n;
+    const int q = blockIdx.x;
+    const int n = a.n;
+    const int lo = a.lo[q];
+    const int hi = a.count == 1 ? lo : lo + 1;
+    const double frac = a.frac[q];
+    const double nyq = a.fs / 2, taper_from = 0.8 * nyq;
+    const double pi = 3.14159265358979323846;
+    for (int k = threadIdx.x; k <= n / 2; k += blockDim.x) {
+        cd h = mk(0.0);
+        const double f = k * a.fs / n;
+        if (k > 0 && k < a.bins) {
+            const size_t i0 = (size_t)lo * a.bins + k, i1 = (size_t)hi * a.bins + k;
+            if (a.logmag[i0] != kNegInf && a.logmag[i1] != kNegInf) {
+                const double lm = a.logmag[i0] + frac * (a.logmag[i1] - a.logmag[i0]);
+                const double ph = a.phase[i0] + frac * (a.phase[i1] - a.phase[i0]);
+                double sn, cs;
+                sincos(ph, &sn, &cs);
+                const double m = exp(lm);
+                h = mk(m * cs, m * sn);
+                if (a.velocity) h = mk(0.0, 2.0 * pi * f) * h;
+                if (a.sensor) h = h * a.sensor[k];
+            }
+            if (f > taper_from) h = h * (0.5 * (1.0 + cos(pi * (f - taper_from) / (nyq - taper_from))));
+        }
+        if (k == 0 || k == n / 2) h.im = 0.0;  // the real transform reads only their real parts
+        x[k] = mk(h.re, -h.im);                // conj of the Hermitian extension
+        if (k > 0 && k < n / 2) x[n - k] = h;
+    }
+    __syncthreads();
+    const cd* r = fft_pow2(x, y, n, a.tw);
+    for (int t = threadIdx.x; t < a.length; t += blockDim.x) a.out[(size_t)q * a.length + t] = r[t].re / n;
+}
+
+}  // namespace consume
+}  // namespace gfk
+
+namespace {
+
+int cfail(gfk_ctx* ctx, int status, const char* msg) {
+    if (ctx) ctx->last_error = msg;
+    return status;
+}
+
+#define CS_CUDA(ctx, call)                                                                         \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            if (ctx) (ctx)->last_error = std::string(#call ": ") + cudaGetErrorString(e_);         \
+            return e_ == cudaErrorMemoryAllocation ? GFK_ENOMEM : GFK_ECUDA;                        \
+        }                                                                                          \
+    } while (0)
+
+// Device copies of a payload and its tables, freed together.
+struct Tables {
+    gfk_ctx* ctx = nullptr;
+    float* data = nullptr;
+    double *logmag = nullptr, *phase = nullptr;
+    ~Tables() {
+        if (!ctx) return;
+        if (data) cudaFreeAsync(data, ctx->stream);
+        if (logmag) cudaFreeAsync(logmag, ctx->stream);
+        if (phase) cudaFreeAsync(phase, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+    }
+};
+
+int build_tables(gfk_ctx* ctx, const float* payload, int count, int bins, Tables& t) {
+    const size_t cells = (size_t)count * bins;
+    t.ctx = ctx;
+    CS_CUDA(ctx, cudaMallocAsync((void**)&t.data, cells * 2 * sizeof(float), ctx->stream));
+    CS_CUDA(ctx, cudaMallocAsync((void**)&t.logmag, cells * sizeof(double), ctx->stream));
+    CS_CUDA(ctx, cudaMallocAsync((void**)&t.phase, cells * sizeof(double), ctx->stream));
+    CS_CUDA(ctx, cudaMemcpyAsync(t.data, payload, cells * 2 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    gfk::consume::k_tables<<<(bins + 127) / 128, 128, 0, ctx->stream>>>(t.data, count, bins, t.logmag, t.phase);
+    ctx->launches++;
+    CS_CUDA(ctx, cudaGetLastError());
+    return GFK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gfk_bank_tables(gfk_ctx* ctx, const float* payload, int32_t count, int32_t bins, double* logmag,
+                    double* phase) {
+    if (!ctx || !payload || !logmag || !phase) return GFK_EARG;
+    if (count < 1 || bins < 1) return cfail(ctx, GFK_EARG, "bank: empty payload");
+    cudaSetDevice(ctx->device);
+    Tables t;
+    const int st = build_tables(ctx, payload, count, bins, t);
+    if (st) return st;
+    const size_t cells = (size_t)count * bins;
+    CS_CUDA(ctx, cudaMemcpyAsync(logmag, t.logmag, cells * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CS_CUDA(ctx, cudaMemcpyAsync(phase, t.phase, cells * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GFK_OK;
+}
+
+int gfk_bank_impulse_responses(gfk_ctx* ctx, const float* payload, int32_t count, int32_t bins, double min_m,
+                               double max_m, double fs_hz, int32_t samples, const double* ranges, int32_t nq,
+                               const double* sensor, int32_t velocity, int32_t length, double* out) {
+    if (!ctx || !payload || !ranges || !out) return GFK_EARG;
+    if (count < 1 || nq < 0) return cfail(ctx, GFK_EARG, "bank: empty payload");
+    if (samples < 2 || (samples & (samples - 1)) || bins != samples / 2 + 1)
+        return cfail(ctx, GFK_EARG, "bank: samples must be a power of two with bins = samples/2 + 1");
+    if (samples > gfk::consume::kMaxSamples)
+        return cfail(ctx, GFK_ELIMIT, "bank: impulse responses are built for samples <= 4096");
+    if (length <= 0) return cfail(ctx, GFK_EARG, "dsp: impulse response length must be positive");
+    if (!(fs_hz > 0)) return cfail(ctx, GFK_EARG, "dsp: sample rate must be positive");
+    if (samples < length) return cfail(ctx, GFK_EARG, "dsp: transform size is shorter than the samples to keep");
+    if (nq == 0) return GFK_OK;
+    // format.go:295-309 bracket, on the host
+    std::vector<int> lo(nq);
+    std::vector<double> frac(nq);
+    const double spacing = count > 1 ? (max_m - min_m) / (count - 1) : 0.0;
+    for (int q = 0; q < nq; q++) {
+        const double r = ranges[q];
+        if (!(r >= min_m && r <= max_m)) {
+            char buf[160];
+            snprintf(buf, sizeof buf, "bank: range %g m is outside the bank's %g to %g m", r, min_m, max_m);
+            return cfail(ctx, GFK_EARG, buf);
+        }
+        if (count == 1) {
+            lo[q] = 0;
+            frac[q] = 0.0;
+            continue;
+        }
+        const double x = (r - min_m) / spacing;
+        int l = (int)std::floor(x);
+        if (l >= count - 1) {
+            lo[q] = count - 2;
+            frac[q] = 1.0;
+        } else {
+            lo[q] = l;
+            frac[q] = x - l;
+        }
+    }
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    Tables t;
+    int st = build_tables(ctx, payload, count, bins, t);
+    if (st) return st;
+    std::vector<double> tw(samples);
+    for (int m = 0; m < samples / 2; m++) {
+        const double a = -2.0 * M_PI * m / samples;
+        tw[2 * m] = std::cos(a);
+        tw[2 * m + 1] = std::sin(a);
+    }
+    struct Buf {
+        gfk_ctx* ctx;
+        void* p = nullptr;
+        ~Buf() {
+            if (p) cudaFreeAsync(p, ctx->stream);
+        }
+    } d_lo{ctx}, d_frac{ctx}, d_tw{ctx}, d_sensor{ctx}, d_out{ctx};
+    CS_CUDA(ctx, cudaMallocAsync(&d_lo.p, nq * sizeof(int), s));
+    CS_CUDA(ctx, cudaMallocAsync(&d_frac.p, nq * sizeof(double), s));
+    CS_CUDA(ctx, cudaMallocAsync(&d_tw.p, samples * sizeof(double), s));
+    CS_CUDA(ctx, cudaMallocAsync(&d_out.p, (size_t)nq * length * sizeof(double), s));
+    CS_CUDA(ctx, cudaMemcpyAsync(d_lo.p, lo.data(), nq * sizeof(int), cudaMemcpyHostToDevice, s));
+    CS_CUDA(ctx, cudaMemcpyAsync(d_frac.p, frac.data(), nq * sizeof(double), cudaMemcpyHostToDevice, s));
+    CS_CUDA(ctx, cudaMemcpyAsync(d_tw.p, tw.data(), samples * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (sensor) {
+        CS_CUDA(ctx, cudaMallocAsync(&d_sensor.p, (size_t)bins * 2 * sizeof(double), s));
+        CS_CUDA(ctx, cudaMemcpyAsync(d_sensor.p, sensor, (size_t)bins * 2 * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    const size_t smem = (size_t)2 * samples * sizeof(cd);
+    if (smem > 48 * 1024)
+        CS_CUDA(ctx, cudaFuncSetAttribute(gfk::consume::k_impulse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+    gfk::consume::ImpulseArgs a{t.logmag, t.phase, count, bins, samples, length,
+                                static_cast<const int*>(d_lo.p), static_cast<const double*>(d_frac.p),
+                                static_cast<const cd*>(d_sensor.p), velocity, fs_hz,
+                                static_cast<const cd*>(d_tw.p), static_cast<double*>(d_out.p)};
+    gfk::consume::k_impulse<<<nq, gfk::consume::kThreads, smem, s>>>(a);
+    ctx->launches++;
+    CS_CUDA(ctx, cudaGetLastError());
+    CS_CUDA(ctx, cudaMemcpyAsync(out, d_out.p, (size_t)nq * length * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CS_CUDA(ctx, cudaStreamSynchronize(s));
+    return GFK_OK;
+}
+
+}  // extern "C"

@@ -10,11 +10,10 @@
 // (internal/sweep/sweep.go:128-169): the peak |y| and the magnitude-weighted
 // centroid of |rfft(y)| over the band bins [k_lo, k_hi].
 //
-// Both transforms are n = 1024 complex radix-2 Stockham FFTs in FP64 in
-// shared memory (the autosort formulation of Govindaraju et al., SC 2008:
-// butterfly j reads x[j], x[j + n/2] and writes y[2 Ns (j / Ns) + j % Ns]
-// and that + Ns, twiddle e^{-2 pi i (j % Ns) / (2 Ns)}). The inverse
-// transform of the Hermitian spectrum is Re(FFT(conj(Y~))) / n.
+// Both transforms are n = 1024 complex radix-2 FFTs in FP64 in shared memory
+// (gfk_fft.cuh). The inverse transform of the Hermitian spectrum is
+// Re(FFT(conj(Y~))) / n.
+#include "gfk_fft.cuh"
 #include "gfk_kernels.cuh"
 #include "gfk_mlp.cuh"
 
@@ -22,27 +21,6 @@ namespace gfk {
 namespace trace {
 
 constexpr int kThreads = 256;
-
-__device__ void fft1024(cd* x, cd* y, const cd* __restrict__ tw) {
-    // x holds the input; the result ends in x (10 stages, even count).
-    cd* src = x;
-    cd* dst = y;
-    for (int ns = 1; ns < kN; ns <<= 1) {
-        for (int j = threadIdx.x; j < kN / 2; j += blockDim.x) {
-            const int k = j & (ns - 1);
-            const cd w = tw[k * (kN / (2 * ns))];
-            const cd a0 = src[j];
-            const cd a1 = src[j + kN / 2] * w;
-            const int d = ((j - k) << 1) + k;
-            dst[d] = a0 + a1;
-            dst[d + ns] = a0 - a1;
-        }
-        __syncthreads();
-        cd* t = src;
-        src = dst;
-        dst = t;
-    }
-}
 
 __global__ void __launch_bounds__(kThreads) k_metrics(const cd* __restrict__ G, long long stride, int nbins,
                                                       const cd* __restrict__ S, const cd* __restrict__ tw, double fs,
@@ -61,19 +39,19 @@ __global__ void __launch_bounds__(kThreads) k_metrics(const cd* __restrict__ G, 
         if (k > 0 && k < kN / 2) buf[0][kN - k] = Y;
     }
     __syncthreads();
-    fft1024(buf[0], buf[1], tw);
+    const cd* y = fft_pow2(buf[0], buf[1], kN, tw);  // 10 stages: the result is in buf[0]
     // y_t = Re / n e^{w_I t}; keep y as the real input of the second transform
     double pk = 0.0;
     for (int t = tid; t < kN; t += blockDim.x) {
-        const double yt = buf[0][t].re * (1.0 / kN) * exp(wi * t / fs);
+        const double yt = y[t].re * (1.0 / kN) * exp(wi * t / fs);
         pk = fmax(pk, fabs(yt));
         buf[0][t] = mk(yt);
     }
     __syncthreads();
-    fft1024(buf[0], buf[1], tw);
+    const cd* Yc = fft_pow2(buf[0], buf[1], kN, tw);
     double num = 0.0, den = 0.0;
     for (int k = k_lo + tid; k <= k_hi; k += blockDim.x) {
-        const double a = hypot(buf[0][k].re, buf[0][k].im);
+        const double a = hypot(Yc[k].re, Yc[k].im);
         num += a * (k * fs / kN);
         den += a;
     }

@@ -259,6 +259,30 @@ int gfk_bank_pack(const double *spectra, int32_t nf, int32_t nr,
 int gfk_bank_write(const char *path, const char *header_json,
                    const float *payload, int64_t nfloats);
 
+/* ---- bank consumption (internal/bank/interp.go, internal/dsp/dsp.go) ----- */
+/* Bank.prepare (internal/bank/interp.go:66-102): the FP64 log-magnitude and
+ * range-unwrapped phase tables of a bank payload, float32 (re, im) pairs
+ * [count][bins] (range-major, as in the file). An exact zero has
+ * log-magnitude -1e308 and keeps the running phase. Host arrays in and out,
+ * count*bins doubles each. */
+int gfk_bank_tables(gfk_ctx *ctx, const float *payload, int32_t count, int32_t bins,
+                    double *logmag, double *phase);
+/* The causal impulse responses a sensor engine builds from a bank
+ * (internal/sensing/sensing.go:196-204 with propagation.go:84-104): at each of
+ * nq ranges, Bank.Response (interp.go:29-54, bracket format.go:295-309) on
+ * every bin k = 1..samples/2, times i 2 pi f_k when velocity is nonzero, times
+ * sensor[k] (host, bins complex (re, im) pairs) when sensor is not NULL, fed to
+ * dsp.CausalImpulseResponseAt (dsp.go:232-261) with the transform size
+ * `samples` (the bank's): tapered above 0.8 Nyquist, inverse real transform
+ * scaled 1/samples, first `length` samples kept. The grid is
+ * [min_m, max_m] with `count` ranges; bins must be samples/2 + 1, samples a
+ * power of two <= 4096 (GFK_ELIMIT above). A range outside the grid is
+ * GFK_EARG with the reference's message. out: host [nq][length] doubles. */
+int gfk_bank_impulse_responses(gfk_ctx *ctx, const float *payload, int32_t count, int32_t bins,
+                               double min_m, double max_m, double fs_hz, int32_t samples,
+                               const double *ranges_m, int32_t nq, const double *sensor,
+                               int32_t velocity, int32_t length, double *out);
+
 /* ---- sweep metrics of geophone traces ------------------------------------ */
 /* For each of ns soils, the geophone trace synthesised from its displacement
  * spectrum and its two sweep metrics (internal/sweep/sweep.go:128-169 Measure:

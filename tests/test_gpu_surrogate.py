@@ -151,11 +151,18 @@ def test_training_reduces_loss_and_beats_mean(pkg, eng):
     params = sur.draw(40, 31)
     ds = sur.Dataset(params, grid, engine=eng).fill(batch_soils=40)
     train, held = sur.split_soils(40, 0.1, 1)
-    net = sur.Net(sur.NetConfig(batch=1024, warmup_steps=50, total_steps=600, lr_max=2e-3, seed=9), eng)
+    net = sur.Net(sur.NetConfig(batch=1024, warmup_steps=50, total_steps=600, lr_max=2e-3, seed=9,
+                                loss_mode=pkg._native.LOSS_PLAIN), eng)
     net.scales_from(ds)
     loss = net.train(ds, train, 600)
     assert np.isfinite(loss).all()
     assert loss[-50:, 0].mean() < 0.2 * loss[:50, 0].mean()
+    # the complex (energy-weighted) loss trains as well
+    cnet = sur.Net(sur.NetConfig(batch=1024, warmup_steps=50, total_steps=600, lr_max=2e-3, seed=9), eng)
+    cnet.scales_from(ds)
+    closs = cnet.train(ds, train, 600)
+    assert np.isfinite(closs).all() and closs[-50:].sum(axis=1).mean() < 0.2 * closs[:50].sum(axis=1).mean()
+    cnet.close()
     # the constant predictor (t = mean) has RMS s0 on log-amplitude
     m0, s0, _, _, _ = ds.stats()
     assert net.evaluate(ds, train)["rms_log_amp"] / s0 < 0.3
