@@ -20,6 +20,7 @@ PLAIN_FP64 = 0
 SPLIT_INT8 = 1
 LOSS_PLAIN = 0
 LOSS_COMPLEX = 1
+LOSS_AMPLITUDE = 2
 NET_TIMES = 6
 NET_FOURIER = 47
 
@@ -33,7 +34,7 @@ EXPORTS = [
     "gfk_plan_launches_per_execute", "gfk_plan_tuning", "gfk_plan_kernel_times", "gfk_plan_destroy",
     "gfk_plan_use_graph", "gfk_batch_create",
     "gfk_bank_pack", "gfk_bank_write", "gfk_vertical_displacement_multi_noalloc",
-    "gfk_trace_metrics", "gfk_bank_tables", "gfk_bank_impulse_responses",
+    "gfk_trace_metrics", "gfk_ensemble_gate", "gfk_scatter_rows", "gfk_bank_tables", "gfk_bank_impulse_responses",
     "gfk_dataset_create", "gfk_dataset_fill", "gfk_dataset_stats", "gfk_dataset_labels", "gfk_dataset_destroy",
     "gfk_net_create", "gfk_net_set_scales", "gfk_net_train", "gfk_net_predict", "gfk_net_evaluate",
     "gfk_net_param_count", "gfk_net_params", "gfk_net_fourier", "gfk_net_probe", "gfk_net_destroy",
@@ -120,6 +121,8 @@ def lib():
         "gfk_bank_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, P(ctypes.c_float), i64]),
         "gfk_vertical_displacement_multi_noalloc": (ctypes.c_int, [P(GfkMedium), P(GfkSolve), P(d), i32, d,
                                                                    GfkIntegration, P(d), vp]),
+        "gfk_ensemble_gate": (ctypes.c_int, [vp, P(vp), i32, i64, i32, i32, P(d), d, vp, P(ctypes.c_uint8), P(d)]),
+        "gfk_scatter_rows": (ctypes.c_int, [vp, vp, i64, P(i64), i64, vp]),
         "gfk_bank_tables": (ctypes.c_int, [vp, P(f32), i32, i32, P(d), P(d)]),
         "gfk_bank_impulse_responses": (ctypes.c_int, [vp, P(f32), i32, i32, d, d, d, i32, P(d), i32, P(d), i32, i32,
                                                       P(d)]),

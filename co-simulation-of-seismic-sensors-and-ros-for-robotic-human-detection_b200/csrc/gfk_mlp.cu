@@ -317,7 +317,11 @@ __global__ void __launch_bounds__(kIn) k_batch(BatchArgs a) {
             a.Y[2 * b] = (L[0] - a.y_mean0) / a.y_std0;
             a.Y[2 * b + 1] = (L[1] - a.y_mean1) / a.y_std1;  // NaN stays NaN
             float c0 = 1.0f, c1 = ph ? a.phase_weight : 0.0f;
-            if (a.loss_mode == 1) {
+            if (a.loss_mode == 2) {
+                const float w = fmaxf(__expf(L[0] - a.lmax[(size_t)soil * a.nr + ir]), a.weight_floor);
+                c0 = w;
+                c1 = ph ? a.phase_weight * w : 0.0f;
+            } else if (a.loss_mode == 1) {
                 const float w = fmaxf(__expf(2.0f * (L[0] - a.lmax[(size_t)soil * a.nr + ir])), a.weight_floor);
                 const float wr = static_cast<float>(2.0 * 3.14159265358979323846 * a.freqs[jf] * a.ranges[ir]) *
                                  (a.y_std1 / a.y_std0);

@@ -79,7 +79,9 @@ struct FeatureDomain {
 //   mode 0: c0 = 1, c1 = phase_weight (0 where the phase is not learnt);
 //   mode 1 (complex): c0 = w, c1 = phase_weight w min((w_f r s1/s0)^2, cap),
 //   w = max(|G|^2 / max_f |G(r, .)|^2, weight_floor): the squared error of G
-//   relative to the soil's spectral peak at that range, phase in radians.
+//   relative to the soil's spectral peak at that range, phase in radians;
+//   mode 2 (amplitude-weighted): c0 = v, c1 = phase_weight v,
+//   v = max(|G| / max_f |G(r, .)|, weight_floor).
 struct BatchArgs {
     const float* labels;   // [nsoil][nr][nf][2]: log|G|, -phi/(w r) (NaN: phase not learnt)
     const float* lmax;     // [nsoil][nr]: log max_f |G|
@@ -197,5 +199,27 @@ constexpr int kN = 1024;
 void launch_metrics(cudaStream_t s, const cd* G, long long stride, int ns, int nbins, const cd* S,
                     const cd* twiddle, double fs, double omega_imag, int k_lo, int k_hi, double* peak,
                     double* centroid);
+
+// Ensemble gate, one block per soil: mean[s][k] = mean over members of
+// G_e[s stride + k]; flag[s][k] = 1 where max_e |G_e - mean| |S[k+1]| exceeds
+// threshold * max_k |mean S[k+1]| (the ensemble's disagreement on that row's
+// share of the recorded trace, relative to the trace spectrum's peak);
+// spread[s] = max_k of that ratio.
+constexpr int kMaxMembers = 16;
+struct GateArgs {
+    const cd* members[kMaxMembers];
+    int E;
+    long long stride;
+    int ns, nbins;
+    const cd* S;
+    double threshold;
+    cd* mean;
+    unsigned char* flag;
+    double* spread;
+};
+void launch_gate(cudaStream_t s, const GateArgs& a);
+// dst[index[i]] = src[i * src_stride] for i < n.
+void launch_scatter(cudaStream_t s, const cd* src, long long src_stride, const long long* index, long long n,
+                    cd* dst);
 }  // namespace trace
 }  // namespace gfk

@@ -383,6 +383,62 @@ int gfk_trace_metrics(gfk_ctx* ctx, const double* d_G, int64_t stride, int32_t n
     return GFK_OK;
 }
 
+int gfk_ensemble_gate(gfk_ctx* ctx, const double* const* d_members, int32_t E, int64_t stride, int32_t ns,
+                      int32_t nbins, const double* shaping, double threshold, double* d_mean, uint8_t* flags,
+                      double* spread) {
+    if (!ctx || !d_members || !shaping || !d_mean || !flags || !spread) return GFK_EARG;
+    if (E < 1 || E > gfk::trace::kMaxMembers || ns < 0 || nbins < 1 || stride < nbins)
+        return sfail(ctx, GFK_EARG, "ensemble gate: bad sizes");
+    if (ns == 0) return GFK_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    gfk::trace::GateArgs a{};
+    for (int e = 0; e < E; e++) a.members[e] = reinterpret_cast<const cd*>(d_members[e]);
+    a.E = E;
+    a.stride = stride;
+    a.ns = ns;
+    a.nbins = nbins;
+    a.threshold = threshold;
+    a.mean = reinterpret_cast<cd*>(d_mean);
+    cd* d_S = nullptr;
+    unsigned char* d_flag = nullptr;
+    double* d_spread = nullptr;
+    SG_TRY(salloc(ctx, &d_S, (size_t)nbins + 1));
+    SG_TRY(salloc(ctx, &d_flag, (size_t)ns * nbins));
+    SG_TRY(salloc(ctx, &d_spread, (size_t)ns));
+    SG_CUDA(ctx, cudaMemcpyAsync(d_S, shaping, sizeof(cd) * (nbins + 1), cudaMemcpyHostToDevice, s));
+    a.S = d_S;
+    a.flag = d_flag;
+    a.spread = d_spread;
+    gfk::trace::launch_gate(s, a);
+    ctx->launches++;
+    SG_CUDA(ctx, cudaGetLastError());
+    SG_CUDA(ctx, cudaMemcpyAsync(flags, d_flag, (size_t)ns * nbins, cudaMemcpyDeviceToHost, s));
+    SG_CUDA(ctx, cudaMemcpyAsync(spread, d_spread, sizeof(double) * ns, cudaMemcpyDeviceToHost, s));
+    cudaFreeAsync(d_S, s);
+    cudaFreeAsync(d_flag, s);
+    cudaFreeAsync(d_spread, s);
+    SG_CUDA(ctx, cudaStreamSynchronize(s));
+    return GFK_OK;
+}
+
+int gfk_scatter_rows(gfk_ctx* ctx, const double* d_src, int64_t src_stride, const int64_t* index, int64_t n,
+                     double* d_dst) {
+    if (!ctx || !d_src || !index || !d_dst || n < 0 || src_stride < 1) return GFK_EARG;
+    if (n == 0) return GFK_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    long long* d_idx = nullptr;
+    SG_TRY(salloc(ctx, &d_idx, (size_t)n));
+    SG_CUDA(ctx, cudaMemcpyAsync(d_idx, index, sizeof(long long) * n, cudaMemcpyHostToDevice, s));
+    gfk::trace::launch_scatter(s, reinterpret_cast<const cd*>(d_src), src_stride, d_idx, n, reinterpret_cast<cd*>(d_dst));
+    ctx->launches++;
+    SG_CUDA(ctx, cudaGetLastError());
+    cudaFreeAsync(d_idx, s);
+    SG_CUDA(ctx, cudaStreamSynchronize(s));
+    return GFK_OK;
+}
+
 int gfk_dataset_create(gfk_ctx* ctx, int32_t np, int32_t nsoil, const double* scalars, const double* times,
                        const double* ranges, int32_t nr, const double* freqs, int32_t nf, double floor_rel,
                        gfk_dataset** out) {
@@ -496,7 +552,7 @@ int gfk_net_create(gfk_ctx* ctx, const gfk_net_config* cfg, gfk_net** out) {
     if (cfg->nsoil_scalars < 1 || cfg->nsoil_scalars > M::kMaxSoil || cfg->batch < 128 || cfg->batch % 128 ||
         cfg->batch > (1 << 20))
         return sfail(ctx, GFK_EARG, "network: batch must be a positive multiple of 128 (<= 2^20)");
-    if (cfg->loss_mode != GFK_LOSS_PLAIN && cfg->loss_mode != GFK_LOSS_COMPLEX)
+    if (cfg->loss_mode != GFK_LOSS_PLAIN && cfg->loss_mode != GFK_LOSS_COMPLEX && cfg->loss_mode != GFK_LOSS_AMPLITUDE)
         return sfail(ctx, GFK_EARG, "network: unknown loss mode %d", cfg->loss_mode);
     cudaSetDevice(ctx->device);
     if (M::prepare_gemm()) return sfail(ctx, GFK_ECUDA, "tensor-core GEMM kernels could not be configured");

@@ -74,6 +74,55 @@ __global__ void __launch_bounds__(kThreads) k_metrics(const cd* __restrict__ G, 
     }
 }
 
+__global__ void __launch_bounds__(kThreads) k_gate(GateArgs a) {
+    __shared__ double red[kThreads];
+    const int s = blockIdx.x, tid = threadIdx.x;
+    double pk = 0.0;
+    for (int k = tid; k < a.nbins; k += blockDim.x) {
+        cd m = mk(0.0);
+        for (int e = 0; e < a.E; e++) m = m + a.members[e][(size_t)s * a.stride + k];
+        m = m * (1.0 / a.E);
+        a.mean[(size_t)s * a.nbins + k] = m;
+        pk = fmax(pk, cabs_(m * a.S[k + 1]));
+    }
+    red[tid] = pk;
+    __syncthreads();
+    for (int w = kThreads / 2; w > 0; w >>= 1) {
+        if (tid < w) red[tid] = fmax(red[tid], red[tid + w]);
+        __syncthreads();
+    }
+    const double peak = red[0];
+    __syncthreads();
+    double worst = 0.0;
+    for (int k = tid; k < a.nbins; k += blockDim.x) {
+        const cd m = a.mean[(size_t)s * a.nbins + k];
+        double d = 0.0;
+        for (int e = 0; e < a.E; e++) d = fmax(d, cabs_(a.members[e][(size_t)s * a.stride + k] - m));
+        const double ratio = peak > 0.0 ? d * cabs_(a.S[k + 1]) / peak : 0.0;
+        a.flag[(size_t)s * a.nbins + k] = ratio > a.threshold ? 1 : 0;
+        worst = fmax(worst, ratio);
+    }
+    red[tid] = worst;
+    __syncthreads();
+    for (int w = kThreads / 2; w > 0; w >>= 1) {
+        if (tid < w) red[tid] = fmax(red[tid], red[tid + w]);
+        __syncthreads();
+    }
+    if (tid == 0) a.spread[s] = red[0];
+}
+
+__global__ void k_scatter(const cd* src, long long src_stride, const long long* index, long long n, cd* dst) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) dst[index[i]] = src[i * src_stride];
+}
+
+void launch_gate(cudaStream_t s, const GateArgs& a) { k_gate<<<a.ns, kThreads, 0, s>>>(a); }
+
+void launch_scatter(cudaStream_t s, const cd* src, long long src_stride, const long long* index, long long n,
+                    cd* dst) {
+    k_scatter<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, src_stride, index, n, dst);
+}
+
 void launch_metrics(cudaStream_t s, const cd* G, long long stride, int ns, int nbins, const cd* S, const cd* twiddle,
                     double fs, double omega_imag, int k_lo, int k_hi, double* peak, double* centroid) {
     k_metrics<<<ns, kThreads, 0, s>>>(G, stride, nbins, S, twiddle, fs, omega_imag, k_lo, k_hi, peak, centroid);

@@ -410,30 +410,116 @@ def spread(values):
     return (v.max(axis=0) - v.min(axis=0)) / np.maximum(np.abs(v.mean(axis=0)), 1e-300)
 
 
-def run_surrogate(engine, nets, n=16384, seed=0, setup=None, threshold=0.01, batch_soils=20000):
-    """The Sobol run with the surrogate answering: every network of the
-    ensemble predicts each soil's metrics; where the ensemble's relative
-    spread of either metric exceeds `threshold` the soil is re-solved by the
-    plain GPU f-k path, whose answer replaces the ensemble mean."""
+def _solve_rows(params, bins_per_soil, setup, engine, batch_soils, nk=NK, kmax=KMAX, formulation=N.DUNKIN):
+    """Yields (plan, soil indices, bin lists) for the listed rows of each
+    soil: one batch plan per group of soils, each soil with its own bins."""
+    freqs = setup.freqs()
+    opt = Integration(nk, 0.0, kmax)
+    soils = [i for i, b in enumerate(bins_per_soil) if len(b)]
+    for b0 in range(0, len(soils), batch_soils):
+        group = soils[b0:b0 + batch_soils]
+        media = [Medium(soil_of(params[i]), formulation=formulation, omega_imag=setup.omega_imag, engine=engine)
+                 for i in group]
+        plan = Batch(media, [freqs[bins_per_soil[i]] for i in group], [setup.r], opt, engine=engine)
+        try:
+            plan.execute()
+            status = plan.statuses()
+            if (status != 0).any():
+                raise RuntimeError(f"fallback row {int(np.nonzero(status)[0][0])}: status "
+                                   f"{N.STATUS_NAMES[int(status[np.nonzero(status)[0][0]])]}")
+            yield plan, group
+        finally:
+            plan.close()
+
+
+def run_surrogate(engine, nets, n=16384, seed=0, setup=None, threshold=0.01, batch_soils=20000, gate="rows",
+                  chunk_soils=32768):
+    """The Sobol run with the surrogate answering and the plain GPU f-k solve
+    as fallback and judge.
+
+    gate="rows": every network predicts each soil's spectrum at the sensor;
+    the ensemble mean answers, except on the rows (soil, bin) where the
+    members disagree by more than `threshold` of the soil's trace-spectrum
+    peak (gfk_ensemble_gate), which the f-k solve recomputes in place
+    (gfk_scatter_rows); metrics then run on the merged device spectra.
+    gate="soil": each network's metrics are computed; where the ensemble's
+    relative spread of either metric exceeds `threshold` the whole soil is
+    re-solved and its plain metrics replace the ensemble mean."""
+    import torch  # device buffers only
+
+    from .surrogate import from_sobol
     setup = setup or TraceSetup()
     k = len(PARAMS)
     t0 = time.perf_counter()
     u = saltelli(n, k, seed)
     params = unit_to_params(u)
-    peaks, cens = ensemble_metrics(nets, params, setup, engine)
-    t1 = time.perf_counter()
-    peak, cen = peaks.mean(axis=0), cens.mean(axis=0)
-    sp = np.maximum(spread(peaks), spread(cens))
-    fb = np.nonzero(sp > threshold)[0]
-    gpu_s = 0.0
-    if len(fb):
-        pk, ce, gpu_s = solve_metrics(params[fb], setup, engine, batch_soils)
-        peak[fb], cen[fb] = pk, ce
-    t2 = time.perf_counter()
+    nb = len(setup.freqs())
+    if gate == "soil":
+        peaks, cens = ensemble_metrics(nets, params, setup, engine)
+        t1 = time.perf_counter()
+        peak, cen = peaks.mean(axis=0), cens.mean(axis=0)
+        sp = np.maximum(spread(peaks), spread(cens))
+        fb = np.nonzero(sp > threshold)[0]
+        gpu_s = 0.0
+        if len(fb):
+            pk, ce, gpu_s = solve_metrics(params[fb], setup, engine, batch_soils)
+            peak[fb], cen[fb] = pk, ce
+        t2 = time.perf_counter()
+        res = _result(n, k, peak, cen, {})
+        res.seconds = {"surrogate": t1 - t0, "fallback_wall": t2 - t1, "fallback_gpu": gpu_s,
+                       "total": time.perf_counter() - t0, "soils": len(params), "fallback_soils": int(len(fb)),
+                       "fallback_fraction": len(fb) / len(params), "members": len(nets), "threshold": threshold,
+                       "gate": gate}
+        res.metrics["spread"] = sp
+        return res
+
+    p11 = from_sobol(params)
+    Sc = shaping(setup)
+    S = np.ascontiguousarray(np.stack([Sc.real, Sc.imag], axis=1).ravel())
+    dev = f"cuda:{engine.device}"
+    cs = min(chunk_soils, len(p11))
+    bufs = [torch.empty(cs * nb * 2, dtype=torch.float64, device=dev) for _ in nets]
+    mean = torch.empty(cs * nb * 2, dtype=torch.float64, device=dev)
+    ptrs = (ctypes.c_void_p * len(nets))(*[b.data_ptr() for b in bufs])
+    peak = np.zeros(len(p11))
+    cen = np.zeros(len(p11))
+    spread_s = np.zeros(len(p11))
+    t_pred = t_fb = gpu_s = 0.0
+    rows_fb = 0
+    soils_fb = 0
+    for c0 in range(0, len(p11), cs):
+        chunk = p11[c0:c0 + cs]
+        m = len(chunk)
+        ta = time.perf_counter()
+        for net, b in zip(nets, bufs):
+            net.predict(chunk, [setup.r], setup.freqs(), out_device_ptr=b.data_ptr())
+        flags = np.zeros((m, nb), dtype=np.uint8)
+        sp = np.zeros(m)
+        engine.check(N.lib().gfk_ensemble_gate(
+            engine.ctx, ptrs, len(nets), nb, m, nb, S.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), threshold,
+            ctypes.c_void_p(mean.data_ptr()), flags.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+            sp.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        tb = time.perf_counter()
+        t_pred += tb - ta
+        bins = [np.nonzero(flags[i])[0] for i in range(m)]
+        rows_fb += int(flags.sum())
+        soils_fb += int((flags.sum(axis=1) > 0).sum())
+        for plan, group in _solve_rows(params[c0:c0 + m], bins, setup, engine, batch_soils):
+            idx = np.ascontiguousarray(np.concatenate([g * nb + bins[g] for g in group]).astype(np.int64))
+            engine.check(N.lib().gfk_scatter_rows(engine.ctx, ctypes.c_void_p(plan.result_device_ptr()), 1,
+                                                  idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), len(idx),
+                                                  ctypes.c_void_p(mean.data_ptr())))
+            a, b_, c_ = plan.kernel_times()
+            gpu_s += (a + b_ + c_) * 1e-3
+        pk, ce = metrics_device(engine, mean.data_ptr(), nb, m, setup)
+        peak[c0:c0 + m], cen[c0:c0 + m], spread_s[c0:c0 + m] = pk, ce, sp
+        t_fb += time.perf_counter() - tb
+    del bufs, mean
     res = _result(n, k, peak, cen, {})
-    t3 = time.perf_counter()
-    res.seconds = {"surrogate": t1 - t0, "fallback_wall": t2 - t1, "fallback_gpu": gpu_s, "post": t3 - t2,
-                   "total": t3 - t0, "soils": len(params), "fallback_soils": int(len(fb)),
-                   "fallback_fraction": len(fb) / len(params), "members": len(nets), "threshold": threshold}
-    res.metrics["spread"] = sp
+    total = time.perf_counter() - t0
+    res.seconds = {"surrogate": t_pred, "fallback_wall": t_fb, "fallback_gpu": gpu_s, "total": total,
+                   "soils": len(params), "fallback_soils": soils_fb, "fallback_rows": rows_fb,
+                   "fallback_fraction": rows_fb / (len(params) * nb), "members": len(nets), "threshold": threshold,
+                   "gate": gate}
+    res.metrics["spread"] = spread_s
     return res

@@ -299,6 +299,23 @@ int gfk_trace_metrics(gfk_ctx *ctx, const double *d_G, int64_t stride, int32_t n
                       const double *shaping, int32_t n, double fs_hz, double omega_imag,
                       int32_t k_lo, int32_t k_hi, double *peak, double *centroid);
 
+/* ---- ensemble gate for surrogate answers ---------------------------------- */
+/* No counterpart in the reference. For E predicted spectra of ns soils
+ * (device arrays of (re, im) pairs, soil s's bins k = 1..nbins at
+ * d_members[e][2 (s stride + k - 1)]): d_mean (device, [ns][nbins] pairs)
+ * receives their mean; flags (host, [ns][nbins] bytes) marks the rows whose
+ * ensemble disagreement, weighted by the trace shaping |S_k| (the factors of
+ * gfk_trace_metrics, n/2 + 1 = nbins + 1 pairs, host), exceeds threshold times
+ * the peak of |mean S| over the soil's bins; spread (host, ns) receives each
+ * soil's largest such ratio. E <= 16. */
+int gfk_ensemble_gate(gfk_ctx *ctx, const double *const *d_members, int32_t E, int64_t stride,
+                      int32_t ns, int32_t nbins, const double *shaping, double threshold,
+                      double *d_mean, uint8_t *flags, double *spread);
+/* d_dst[2 index[i]] <- d_src[2 i src_stride] (re, im pairs), i < n; index host,
+ * the pointers device memory. Puts solved rows back into a spectrum buffer. */
+int gfk_scatter_rows(gfk_ctx *ctx, const double *d_src, int64_t src_stride, const int64_t *index,
+                     int64_t n, double *d_dst);
+
 /* ---- surrogate network ---------------------------------------------------- */
 /* No counterpart in the reference (it has no learned component). A small
  * network maps (soil, range, frequency) to the vertical displacement spectrum
@@ -332,9 +349,11 @@ typedef struct gfk_net gfk_net;
  *   GFK_LOSS_COMPLEX: c0 = w, c1 = phase_weight w min((w_f r std1/std0)^2,
  *                     phase_cap), w = max(|G|^2 / max_f |G(r, .)|^2,
  *                     weight_floor) — the squared error of G itself relative
- *                     to the spectral peak at that range, phase in radians.
+ *                     to the spectral peak at that range, phase in radians;
+ *   GFK_LOSS_AMPLITUDE: c0 = v, c1 = phase_weight v, v = max(|G| / max_f
+ *                     |G(r, .)|, weight_floor).
  * c1 = 0 where the phase is not learnt. */
-enum gfk_loss_mode { GFK_LOSS_PLAIN = 0, GFK_LOSS_COMPLEX = 1 };
+enum gfk_loss_mode { GFK_LOSS_PLAIN = 0, GFK_LOSS_COMPLEX = 1, GFK_LOSS_AMPLITUDE = 2 };
 
 typedef struct {
     int32_t nsoil_scalars;  /* soil scalars per soil, <= GFK_NET_MAX_SOIL */

@@ -38,7 +38,8 @@ def solved_bank(pkg, eng):
     h = pkg.Header(pkg.Provenance("gfk-b200 dunkin", "test"), stack, 1000.0, 1024,
                    pkg.RangeGrid(1.0, 12.75, 48), "vertical", "m/N")
     med = pkg.Medium(stack, formulation=pkg.DUNKIN, engine=eng)
-    return pkg.build_bank(med, h, 200.0, pkg.Integration(4096, 0.0, 52.36), check_range_sampling=False)
+    b, _ = pkg.build_bank(med, h, 200.0, pkg.Integration(4096, 0.0, 52.36), check_range_sampling=False)
+    return b
 
 
 def golden(pkg, name):

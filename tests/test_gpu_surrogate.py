@@ -172,17 +172,25 @@ def test_training_reduces_loss_and_beats_mean(pkg, eng):
 
 
 def test_surrogate_sobol_plumbing(pkg, eng):
-    """End to end with an untrained two-member ensemble: every soil the
-    ensemble disagrees on is re-solved, and those soils' metrics equal the
-    plain run's exactly."""
+    """End to end with an untrained two-member ensemble. Soil gate: every
+    soil the ensemble disagrees on is re-solved and those soils' metrics
+    equal the plain run's. Row gate: with a zero threshold every row is
+    re-solved in place and all metrics equal the plain run's; with an
+    unreachable one nothing is, and no solver row runs."""
     sob, sur = pkg.sobol, pkg.surrogate
     nets = [sur.Net(sur.NetConfig(batch=256, seed=s), eng) for s in (1, 2)]
     for n_ in nets:
         n_.set_scales(1.0, 64.0, 500 / 512, 500.0, [-22.0, 2.0, 0.006, 0.002])
-    res = sob.run_surrogate(eng, nets, n=8, seed=2, threshold=0.01)
     plain = sob.run_plain(eng, n=8, seed=2)
+    res = sob.run_surrogate(eng, nets, n=8, seed=2, threshold=0.01, gate="soil")
     fb = np.nonzero(res.metrics["spread"] > 0.01)[0]
     assert res.seconds["fallback_soils"] == len(fb) and len(fb) > 0
     assert np.allclose(res.metrics["peak"][fb], plain.metrics["peak"][fb], rtol=1e-12)
+    rows = sob.run_surrogate(eng, nets, n=8, seed=2, threshold=0.0, gate="rows")
+    assert rows.seconds["fallback_fraction"] == 1.0
+    assert np.allclose(rows.metrics["peak"], plain.metrics["peak"], rtol=1e-12)
+    assert np.allclose(rows.metrics["centroid"], plain.metrics["centroid"], rtol=1e-12)
+    none = sob.run_surrogate(eng, nets, n=8, seed=2, threshold=1e30, gate="rows")
+    assert none.seconds["fallback_rows"] == 0 and np.isfinite(none.metrics["peak"]).all()
     for n_ in nets:
         n_.close()
