@@ -211,7 +211,7 @@ class NetConfig:
     batch: int = 8192
     warmup_steps: int = 500
     total_steps: int = 40000
-    lr_max: float = 1e-3
+    lr_max: float = 3e-4
     lr_min: float = 1e-5
     beta1: float = 0.9
     beta2: float = 0.999
@@ -219,8 +219,8 @@ class NetConfig:
     weight_decay: float = 0.0
     phase_weight: float = 1.0
     fourier_sigma: float = 8.0
-    loss_mode: int = N.LOSS_COMPLEX
-    weight_floor: float = 1e-4
+    loss_mode: int = N.LOSS_AMPLITUDE
+    weight_floor: float = 0.1
     phase_cap: float = 1e4
     seed: int = 1
 

@@ -174,7 +174,7 @@ def test_training_reduces_loss_and_beats_mean(pkg, eng):
 def test_surrogate_sobol_plumbing(pkg, eng):
     """End to end with an untrained two-member ensemble. Soil gate: every
     soil the ensemble disagrees on is re-solved and those soils' metrics
-    equal the plain run's. Row gate: with a zero threshold every row is
+    equal the plain run's. Row gate: with a negative threshold every row is
     re-solved in place and all metrics equal the plain run's; with an
     unreachable one nothing is, and no solver row runs."""
     sob, sur = pkg.sobol, pkg.surrogate
@@ -186,7 +186,7 @@ def test_surrogate_sobol_plumbing(pkg, eng):
     fb = np.nonzero(res.metrics["spread"] > 0.01)[0]
     assert res.seconds["fallback_soils"] == len(fb) and len(fb) > 0
     assert np.allclose(res.metrics["peak"][fb], plain.metrics["peak"][fb], rtol=1e-12)
-    rows = sob.run_surrogate(eng, nets, n=8, seed=2, threshold=0.0, gate="rows")
+    rows = sob.run_surrogate(eng, nets, n=8, seed=2, threshold=-1.0, gate="rows")
     assert rows.seconds["fallback_fraction"] == 1.0
     assert np.allclose(rows.metrics["peak"], plain.metrics["peak"], rtol=1e-12)
     assert np.allclose(rows.metrics["centroid"], plain.metrics["centroid"], rtol=1e-12)
