@@ -12,7 +12,8 @@ from .bank import (Bank, Header, Provenance, RangeGrid, build_bank, open_bank, r
 from . import workloads
 from . import sobol
 from . import surrogate
+from . import disp
 
 __all__ = ["Batch", "Engine", "FkError", "Grid", "Integration", "Layer", "MAX_LAYER_PHASE", "Medium", "Plan", "SLS",
            "Stack", "default_engine", "uniform", "Bank", "Header", "Provenance", "RangeGrid", "build_bank",
-           "open_bank", "range_nyquist", "workloads", "sobol", "surrogate", "DUNKIN", "REFERENCE_DIRECT", "PLAIN_FP64", "SPLIT_INT8"]
+           "open_bank", "range_nyquist", "workloads", "sobol", "surrogate", "disp", "DUNKIN", "REFERENCE_DIRECT", "PLAIN_FP64", "SPLIT_INT8"]

@@ -259,6 +259,31 @@ int gfk_bank_pack(const double *spectra, int32_t nf, int32_t nr,
 int gfk_bank_write(const char *path, const char *header_json,
                    const float *payload, int64_t nfloats);
 
+/* ---- Rayleigh dispersion (internal/propmat, internal/disp) ---------------- */
+/* disp.Search (internal/disp/disp.go:30-54): samples <= 0 uses 2000 (at most
+ * 16384), tolerance <= 0 uses 1e-10. */
+typedef struct gfk_search {
+    int32_t samples;
+    int32_t _pad;
+    double tolerance;
+} gfk_search;
+/* disp.Modes (internal/disp/disp.go:68-103) at nf frequencies: every Rayleigh
+ * phase velocity of the lossless stack (Vp, Vs, density and thicknesses; Q is
+ * ignored, as propmat's secular function is real), slowest first, found by
+ * scanning propmat.SecularAtVelocity (internal/propmat/propmat.go:265-320) on
+ * the disp.Bounds interval and bisecting each sign change. velocities:
+ * [nf][max_modes] host doubles, counts: [nf] modes found. GFK_ESTACK for a
+ * stack layer.Stack.Validate refuses, GFK_EARG for a non-positive frequency,
+ * GFK_ELIMIT (counts still filled, velocities truncated) when a frequency has
+ * more than max_modes (<= 64) modes. */
+int gfk_dispersion_modes(gfk_ctx *ctx, const gfk_medium *m, const double *freqs_hz, int32_t nf,
+                         gfk_search opt, int32_t max_modes, double *velocities, int32_t *counts);
+/* propmat.SecularAtVelocity at n (frequency, phase velocity) pairs: out[i] the
+ * normalised secular value, ok[i] 0 where the reference returns an error or a
+ * non-finite value (phase velocity not below the half-space's Vs). */
+int gfk_secular(gfk_ctx *ctx, const gfk_medium *m, const double *freqs_hz, const double *velocities,
+                int64_t n, double *out, int32_t *ok);
+
 /* ---- bank consumption (internal/bank/interp.go, internal/dsp/dsp.go) ----- */
 /* Bank.prepare (internal/bank/interp.go:66-102): the FP64 log-magnitude and
  * range-unwrapped phase tables of a bank payload, float32 (re, im) pairs

@@ -19,6 +19,9 @@ Writes:
                         40-3000 digits (oracle/mp_direct.py) for a grid of
                         media, wavenumbers and frequencies, both Qp conventions
                         and with a complex frequency offset
+  dispersion/*.json     the reference's disba dispersion goldens
+                        (testdata/dispersion/*.json: disba 0.7.0
+                        PhaseDispersion, Rayleigh), copied byte for byte
 """
 import hashlib
 import json
@@ -117,7 +120,15 @@ def mp_surface_responses():
     (HERE / "surface_response_mp.json").write_text(json.dumps(out, indent=1))
 
 
+def dispersion_fixtures():
+    out = HERE / "dispersion"
+    out.mkdir(exist_ok=True)
+    for src in sorted((REF / "testdata" / "dispersion").glob("*.json")):
+        shutil.copyfile(src, out / src.name)
+
+
 if __name__ == "__main__":
+    dispersion_fixtures()
     bank_fixtures()
     known_answers()
     mp_surface_responses()
