@@ -297,44 +297,59 @@ __global__ void k_step_begin(TrainScalars* ts) {
     ts->bc2 = static_cast<float>(1.0 - pow(static_cast<double>(ts->beta2), static_cast<double>(t)));
 }
 
-// 32 samples per block, one feature per thread.
+// 32 samples per block: one thread per sample draws the cell and builds its
+// scalars and targets, then one thread per feature fills the 32 rows.
 __global__ void __launch_bounds__(kIn) k_batch(BatchArgs a) {
     __shared__ bf16 tile[32][kIn + 2];
+    __shared__ PointScalars ps[32];
+    __shared__ int soil_of[32];
     const long long t = a.ts->step;
     const int b0 = blockIdx.x * 32;
     const int j = threadIdx.x;
-    for (int i = 0; i < 32; i++) {
-        const int b = b0 + i;
+    if (j < 32) {
+        const int b = b0 + j;
         const unsigned long long h = mix64(a.seed ^ mix64(static_cast<unsigned long long>(t) * a.B + b));
         const int soil = a.train[pick(h, a.ntrain)];
         const unsigned long long h2 = mix64(h);
         const int ir = pick(h2, a.nr), jf = pick(h2 >> 32, a.nf);
-        const PointScalars p = point_scalars(a.ranges[ir], a.freqs[jf], a.dom);
-        tile[i][j] = __float2bfloat16_rn(feature(j, a.soilfeat + (size_t)soil * kSoilStride, p, a.fourier));
-        if (j == 0) {
-            const float* L = a.labels + (((size_t)soil * a.nr + ir) * a.nf + jf) * 2;
-            const bool ph = !isnan(L[1]);
-            a.Y[2 * b] = (L[0] - a.y_mean0) / a.y_std0;
-            a.Y[2 * b + 1] = (L[1] - a.y_mean1) / a.y_std1;  // NaN stays NaN
-            float c0 = 1.0f, c1 = ph ? a.phase_weight : 0.0f;
-            if (a.loss_mode == 2) {
-                const float w = fmaxf(__expf(L[0] - a.lmax[(size_t)soil * a.nr + ir]), a.weight_floor);
-                c0 = w;
-                c1 = ph ? a.phase_weight * w : 0.0f;
-            } else if (a.loss_mode == 1) {
-                const float w = fmaxf(__expf(2.0f * (L[0] - a.lmax[(size_t)soil * a.nr + ir])), a.weight_floor);
-                const float wr = static_cast<float>(2.0 * 3.14159265358979323846 * a.freqs[jf] * a.ranges[ir]) *
-                                 (a.y_std1 / a.y_std0);
-                c0 = w;
-                c1 = ph ? a.phase_weight * w * fminf(wr * wr, a.phase_cap) : 0.0f;
-            }
-            a.C[2 * b] = c0;
-            a.C[2 * b + 1] = c1;
+        ps[j] = point_scalars(a.ranges[ir], a.freqs[jf], a.dom);
+        soil_of[j] = soil;
+        const float* L = a.labels + (((size_t)soil * a.nr + ir) * a.nf + jf) * 2;
+        const bool ph = !isnan(L[1]);
+        a.Y[2 * b] = (L[0] - a.y_mean0) / a.y_std0;
+        a.Y[2 * b + 1] = (L[1] - a.y_mean1) / a.y_std1;  // NaN stays NaN
+        float c0 = 1.0f, c1 = ph ? a.phase_weight : 0.0f;
+        if (a.loss_mode == 2) {
+            const float w = fmaxf(__expf(L[0] - a.lmax[(size_t)soil * a.nr + ir]), a.weight_floor);
+            c0 = w;
+            c1 = ph ? a.phase_weight * w : 0.0f;
+        } else if (a.loss_mode == 1) {
+            const float w = fmaxf(__expf(2.0f * (L[0] - a.lmax[(size_t)soil * a.nr + ir])), a.weight_floor);
+            const float wr = static_cast<float>(2.0 * 3.14159265358979323846 * a.freqs[jf] * a.ranges[ir]) *
+                             (a.y_std1 / a.y_std0);
+            c0 = w;
+            c1 = ph ? a.phase_weight * w * fminf(wr * wr, a.phase_cap) : 0.0f;
         }
+        a.C[2 * b] = c0;
+        a.C[2 * b + 1] = c1;
     }
     __syncthreads();
+    for (int i = 0; i < 32; i++)
+        tile[i][j] = __float2bfloat16_rn(feature(j, a.soilfeat + (size_t)soil_of[i] * kSoilStride, ps[i], a.fourier));
+    __syncthreads();
     for (int i = 0; i < 32; i++) a.X[(size_t)(b0 + i) * kIn + j] = tile[i][j];
-    for (int i = 0; i < 32; i++) a.XT[(size_t)j * a.B + b0 + i] = tile[i][j];
+    // X^T: thread j writes its feature's 32 consecutive samples (64 bytes)
+    uint32_t w[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        __nv_bfloat162 v;
+        v.x = tile[2 * i][j];
+        v.y = tile[2 * i + 1][j];
+        w[i] = *reinterpret_cast<uint32_t*>(&v);
+    }
+    uint4* d = reinterpret_cast<uint4*>(a.XT + (size_t)j * a.B + b0);
+#pragma unroll
+    for (int i = 0; i < 4; i++) d[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
 }
 
 // ------------------------------------------------------------------ head --
@@ -484,21 +499,22 @@ __global__ void __launch_bounds__(256) k_bias_grad(BiasPtrs d, int B, float* gb)
 
 // ------------------------------------------------------------------ adam --
 
-__device__ __forceinline__ int seg_of(const AdamArgs& a, long long i) {
-    int s = 0;
-    while (s + 1 < a.nseg && i >= a.seg[s + 1].off) s++;
-    return s;
+// Grids are (blocks over the largest segment, segments): a block works inside
+// one segment, whose descriptor it reads from device memory.
+__device__ __forceinline__ float seg_grad(const AdamSeg& g, long long j) {
+    float grad = 0.0f;
+    for (int q = 0; q < g.nsrc; q++) grad += g.src[q * g.stride + j];
+    return grad;
 }
 
 // AdamW (Loshchilov & Hutter 2019) on the FP32 master copy, gradients summed
-// from their partials in a fixed order; refreshes the BF16 copies W and W^T.
-__global__ void k_adam(AdamArgs a, long long nparam) {
-    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-    if (i >= nparam) return;
-    const AdamSeg& g = a.seg[seg_of(a, i)];
-    const long long j = i - g.off;
-    float grad = 0.0f;
-    for (int q = 0; q < g.nsrc; q++) grad += g.src[q * g.stride + j];
+// from their partials in a fixed order; refreshes the BF16 copy W.
+__global__ void k_adam(AdamArgs a) {
+    const AdamSeg g = a.dseg[blockIdx.y];
+    const long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (j >= g.n) return;
+    const long long i = g.off + j;
+    const float grad = seg_grad(g, j);
     const TrainScalars* ts = a.ts;
     const float b1 = ts->beta1, b2 = ts->beta2;
     const float m = b1 * a.m[i] + (1.0f - b1) * grad;
@@ -508,34 +524,33 @@ __global__ void k_adam(AdamArgs a, long long nparam) {
     float p = a.p[i];
     p -= ts->lr * ((m / ts->bc1) / (sqrtf(v / ts->bc2) + a.eps) + a.weight_decay * p);
     a.p[i] = p;
-    if (g.wb) {
-        const int r = static_cast<int>(j / g.cols), c = static_cast<int>(j % g.cols);
-        const bf16 pb = __float2bfloat16_rn(p);
-        g.wb[j] = pb;
-        g.wt[(size_t)c * g.rows + r] = pb;
-    }
+    if (g.wb) g.wb[j] = __float2bfloat16_rn(p);
 }
 
-__global__ void k_sync_weights(AdamArgs a, long long nparam) {
-    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-    if (i >= nparam) return;
-    const AdamSeg& g = a.seg[seg_of(a, i)];
+// W^T from W for every weight segment, 32 x 32 tiles through shared memory.
+__global__ void k_transpose_w(AdamArgs a) {
+    __shared__ bf16 t[32][33];
+    const AdamSeg g = a.dseg[blockIdx.z];
     if (!g.wb) return;
-    const long long j = i - g.off;
-    const int r = static_cast<int>(j / g.cols), c = static_cast<int>(j % g.cols);
-    const bf16 pb = __float2bfloat16_rn(a.p[i]);
-    g.wb[j] = pb;
-    g.wt[(size_t)c * g.rows + r] = pb;
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    if (c0 >= g.cols || r0 >= g.rows) return;
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) t[y][threadIdx.x] = g.wb[(size_t)(r0 + y) * g.cols + c0 + threadIdx.x];
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) g.wt[(size_t)(c0 + y) * g.rows + r0 + threadIdx.x] = t[threadIdx.x][y];
 }
 
-__global__ void k_grad_flat(AdamArgs a, long long nparam, float* out) {
-    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-    if (i >= nparam) return;
-    const AdamSeg& g = a.seg[seg_of(a, i)];
-    const long long j = i - g.off;
-    float grad = 0.0f;
-    for (int q = 0; q < g.nsrc; q++) grad += g.src[q * g.stride + j];
-    out[i] = grad;
+__global__ void k_sync_weights(AdamArgs a) {
+    const AdamSeg g = a.dseg[blockIdx.y];
+    const long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (j >= g.n || !g.wb) return;
+    g.wb[j] = __float2bfloat16_rn(a.p[g.off + j]);
+}
+
+__global__ void k_grad_flat(AdamArgs a, float* out) {
+    const AdamSeg g = a.dseg[blockIdx.y];
+    const long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (j >= g.n) return;
+    out[g.off + j] = seg_grad(g, j);
 }
 
 // One warp: fixed-order sums of the head kernel's loss partials; each slot
@@ -830,16 +845,35 @@ void launch_bias_grad(cudaStream_t s, const bf16* const* dZT, int layers, int B,
     k_bias_grad<<<dim3(kWidth, layers), 256, 0, s>>>(d, B, gb);
 }
 
-void launch_adam(cudaStream_t s, const AdamArgs& a, long long nparam) {
-    k_adam<<<(unsigned)((nparam + 255) / 256), 256, 0, s>>>(a, nparam);
+namespace {
+long long max_seg(const AdamArgs& a) {
+    long long m = 1;
+    for (int s = 0; s < a.nseg; s++) m = a.seg[s].n > m ? a.seg[s].n : m;
+    return m;
+}
+void launch_transposes(cudaStream_t s, const AdamArgs& a) {
+    int rows = 32, cols = 32;
+    for (int q = 0; q < a.nseg; q++)
+        if (a.seg[q].wb) {
+            rows = a.seg[q].rows > rows ? a.seg[q].rows : rows;
+            cols = a.seg[q].cols > cols ? a.seg[q].cols : cols;
+        }
+    k_transpose_w<<<dim3(cols / 32, rows / 32, a.nseg), dim3(32, 8), 0, s>>>(a);
+}
+}  // namespace
+
+void launch_adam(cudaStream_t s, const AdamArgs& a, long long) {
+    k_adam<<<dim3((unsigned)((max_seg(a) + 255) / 256), a.nseg), 256, 0, s>>>(a);
+    launch_transposes(s, a);
 }
 
-void launch_sync_weights(cudaStream_t s, const AdamArgs& a, long long nparam) {
-    k_sync_weights<<<(unsigned)((nparam + 255) / 256), 256, 0, s>>>(a, nparam);
+void launch_sync_weights(cudaStream_t s, const AdamArgs& a, long long) {
+    k_sync_weights<<<dim3((unsigned)((max_seg(a) + 255) / 256), a.nseg), 256, 0, s>>>(a);
+    launch_transposes(s, a);
 }
 
-void launch_grad_flat(cudaStream_t s, const AdamArgs& a, long long nparam, float* out) {
-    k_grad_flat<<<(unsigned)((nparam + 255) / 256), 256, 0, s>>>(a, nparam, out);
+void launch_grad_flat(cudaStream_t s, const AdamArgs& a, long long, float* out) {
+    k_grad_flat<<<dim3((unsigned)((max_seg(a) + 255) / 256), a.nseg), 256, 0, s>>>(a, out);
 }
 
 void launch_loss_hist(cudaStream_t s, const float* lpart, int nblk, int B, const TrainScalars* ts, float* hist,

@@ -127,13 +127,16 @@ struct AdamSeg {
 constexpr int kMaxSegs = 16;
 struct AdamArgs {
     int nseg;
-    AdamSeg seg[kMaxSegs];
+    AdamSeg seg[kMaxSegs];  // host copy
+    const AdamSeg* dseg;    // the same table in device memory, read by the kernels
     float* p;             // FP32 master parameters
     float* m;
     float* v;
     float eps, weight_decay;
     const TrainScalars* ts;
 };
+// AdamW over every segment (one grid row per segment), then the BF16
+// transposes W^T of the weight segments (32 x 32 shared-memory tiles).
 void launch_adam(cudaStream_t s, const AdamArgs& a, long long nparam);
 // bf16 copies of every weight segment from the master parameters.
 void launch_sync_weights(cudaStream_t s, const AdamArgs& a, long long nparam);

@@ -122,6 +122,7 @@ struct gfk_net {
     bf16 *X = nullptr, *XT = nullptr;
     float* Y = nullptr;
     bf16 *Z[kLayers] = {}, *H[kLayers] = {}, *HT[kLayers] = {}, *dZ[kLayers] = {}, *dZT[kLayers] = {};
+    M::AdamSeg* d_seg = nullptr;
     float *Cw = nullptr, *gpart = nullptr, *lpart = nullptr, *gb = nullptr, *hist = nullptr, *gflat = nullptr;
     int* d_status = nullptr;
     int* d_train = nullptr;
@@ -169,6 +170,7 @@ void net_free(gfk_net* n) {
                     &n->hist, &n->gflat, &n->iT};
     for (float** q : fl) sfree(c, *q);
     sfree(c, n->d_ts);
+    sfree(c, n->d_seg);
     sfree(c, n->X);
     sfree(c, n->XT);
     sfree(c, n->iX);
@@ -270,7 +272,7 @@ int enqueue_step(gfk_net* n, const gfk_dataset* d) {
     SG_TRY(enqueue_fwd_bwd(n));
     M::launch_loss_hist(s, n->lpart, n->B / M::kHeadRows, n->B, n->d_ts, n->hist, kHistCap);
     M::launch_adam(s, n->adam, n->nparam);
-    n->ctx->launches += 2;
+    n->ctx->launches += 3;
     return GFK_OK;
 }
 
@@ -647,6 +649,12 @@ int gfk_net_create(gfk_ctx* ctx, const gfk_net_config* cfg, gfk_net** out) {
     ad.eps = cfg->eps;
     ad.weight_decay = cfg->weight_decay;
     ad.ts = n->d_ts;
+    if (salloc(ctx, &n->d_seg, (size_t)M::kMaxSegs) != GFK_OK) {
+        net_free(n);
+        delete n;
+        return GFK_ENOMEM;
+    }
+    ad.dseg = n->d_seg;
 
     M::TrainScalars ts{};
     ts.step = 0;
@@ -663,8 +671,9 @@ int gfk_net_create(gfk_ctx* ctx, const gfk_net_config* cfg, gfk_net** out) {
     cudaMemsetAsync(n->d_status, 0, 4, s);
     cudaMemcpyAsync(n->d_ts, &ts, sizeof ts, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(n->d_four, n->four.data(), n->four.size() * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(n->d_seg, ad.seg, sizeof(M::AdamSeg) * ad.nseg, cudaMemcpyHostToDevice, s);
     M::launch_sync_weights(s, n->adam, n->nparam);
-    ctx->launches++;
+    ctx->launches += 2;
     if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
         net_free(n);
         delete n;
@@ -732,7 +741,7 @@ int gfk_net_train(gfk_net* n, gfk_dataset* d, const int32_t* train, int32_t ntra
         n->graph_train.assign(train, train + ntrain);
     }
     // launches per replayed step, counted from the step's own enqueue
-    const int64_t per_step = 2 + kLayers + 1 + (kLayers - 1) + kLayers + 1 + 2;
+    const int64_t per_step = 2 + kLayers + 1 + (kLayers - 1) + kLayers + 1 + 3;
     std::vector<float> h(kHistCap * 2);
     for (int done = 0; done < steps;) {
         const int blk = std::min(kHistCap, steps - done);
@@ -846,7 +855,7 @@ int gfk_net_params(gfk_net* n, float* host, int64_t cnt, int32_t set) {
     if (set) {
         SG_CUDA(ctx, cudaMemcpyAsync(n->d_p, host, cnt * 4, cudaMemcpyHostToDevice, s));
         M::launch_sync_weights(s, n->adam, n->nparam);
-        ctx->launches++;
+        ctx->launches += 2;
     } else {
         SG_CUDA(ctx, cudaMemcpyAsync(host, n->d_p, cnt * 4, cudaMemcpyDeviceToHost, s));
     }
