@@ -13,7 +13,8 @@ from . import workloads
 from . import sobol
 from . import surrogate
 from . import disp
+from . import fdtd
 
 __all__ = ["Batch", "Engine", "FkError", "Grid", "Integration", "Layer", "MAX_LAYER_PHASE", "Medium", "Plan", "SLS",
            "Stack", "default_engine", "uniform", "Bank", "Header", "Provenance", "RangeGrid", "build_bank",
-           "open_bank", "range_nyquist", "workloads", "sobol", "surrogate", "disp", "DUNKIN", "REFERENCE_DIRECT", "PLAIN_FP64", "SPLIT_INT8"]
+           "open_bank", "range_nyquist", "workloads", "sobol", "surrogate", "disp", "fdtd", "DUNKIN", "REFERENCE_DIRECT", "PLAIN_FP64", "SPLIT_INT8"]

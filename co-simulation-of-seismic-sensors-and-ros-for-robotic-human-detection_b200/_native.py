@@ -34,7 +34,7 @@ EXPORTS = [
     "gfk_plan_launches_per_execute", "gfk_plan_tuning", "gfk_plan_kernel_times", "gfk_plan_destroy",
     "gfk_plan_use_graph", "gfk_batch_create",
     "gfk_bank_pack", "gfk_bank_write", "gfk_vertical_displacement_multi_noalloc",
-    "gfk_dispersion_modes", "gfk_secular",
+    "gfk_dispersion_modes", "gfk_secular", "gfk_fdtd_grid", "gfk_fdtd_run",
     "gfk_trace_metrics", "gfk_ensemble_gate", "gfk_scatter_rows", "gfk_bank_tables", "gfk_bank_impulse_responses",
     "gfk_dataset_create", "gfk_dataset_fill", "gfk_dataset_stats", "gfk_dataset_labels", "gfk_dataset_destroy",
     "gfk_net_create", "gfk_net_set_scales", "gfk_net_train", "gfk_net_predict", "gfk_net_evaluate",
@@ -65,6 +65,13 @@ class GfkGrid(ctypes.Structure):
 class GfkSolve(ctypes.Structure):
     _fields_ = [("formulation", ctypes.c_int32), ("quadrature", ctypes.c_int32), ("guard", ctypes.c_int32),
                 ("_pad", ctypes.c_int32), ("omega_imag", ctypes.c_double)]
+
+
+class GfkFdtdModel(ctypes.Structure):
+    _fields_ = [("medium", GfkMedium), ("max_range_m", ctypes.c_double), ("depth_m", ctypes.c_double),
+                ("spacing_m", ctypes.c_double), ("pml_cells", ctypes.c_int32), ("_pad", ctypes.c_int32),
+                ("pml_reflection", ctypes.c_double), ("dominant_freq_hz", ctypes.c_double),
+                ("courant", ctypes.c_double)]
 
 
 class GfkSearch(ctypes.Structure):
@@ -126,6 +133,8 @@ def lib():
         "gfk_bank_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, P(ctypes.c_float), i64]),
         "gfk_vertical_displacement_multi_noalloc": (ctypes.c_int, [P(GfkMedium), P(GfkSolve), P(d), i32, d,
                                                                    GfkIntegration, P(d), vp]),
+        "gfk_fdtd_grid": (ctypes.c_int, [P(GfkFdtdModel), P(d), P(i32), P(i32)]),
+        "gfk_fdtd_run": (ctypes.c_int, [vp, P(GfkFdtdModel), P(d), i32, P(d), i32, i32, P(d), P(d), P(d)]),
         "gfk_dispersion_modes": (ctypes.c_int, [vp, P(GfkMedium), P(d), i32, GfkSearch, i32, P(d), P(i32)]),
         "gfk_secular": (ctypes.c_int, [vp, P(GfkMedium), P(d), P(d), i64, P(d), P(i32)]),
         "gfk_ensemble_gate": (ctypes.c_int, [vp, P(vp), i32, i64, i32, i32, P(d), d, vp, P(ctypes.c_uint8), P(d)]),

@@ -9,7 +9,7 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libgfk.so"
 SOURCES = ["gfk_kernels.cu", "gfk_quad_tc.cu", "gfk_host.cu", "gfk_noalloc.cu", "gfk_mlp.cu", "gfk_trace.cu",
-           "gfk_surrogate.cu", "gfk_consume.cu", "gfk_disp.cu"]
+           "gfk_surrogate.cu", "gfk_consume.cu", "gfk_disp.cu", "gfk_fdtd.cu"]
 HEADERS = ["gfk_math.cuh", "gfk_solver.cuh", "gfk_kernels.cuh", "gfk_tc.cuh", "gfk_mlp.cuh", "gfk_ctx.h",
            "gfk_fft.cuh"]
 

@@ -259,6 +259,39 @@ int gfk_bank_pack(const double *spectra, int32_t nf, int32_t nr,
 int gfk_bank_write(const char *path, const char *header_json,
                    const float *payload, int64_t nfloats);
 
+/* ---- finite-difference validator (internal/fdtd) ------------------------ */
+/* fdtd.Model (internal/fdtd/model.go:30-100): the stack (medium.layers), the
+ * optional standard linear solid (medium.sls_tau_sigma/eps; zero: elastic),
+ * its reference frequency (medium.ref_freq_hz, <= 0: 30 Hz), the domain and
+ * the grid; pml_cells <= 0: 20, pml_reflection <= 0: 1e-4, dominant_freq_hz
+ * <= 0: from the slowest velocity, courant <= 0: 0.5. */
+typedef struct gfk_fdtd_model {
+    gfk_medium medium;
+    double max_range_m;
+    double depth_m;
+    double spacing_m;
+    int32_t pml_cells;
+    int32_t _pad;
+    double pml_reflection;
+    double dominant_freq_hz;
+    double courant;
+} gfk_fdtd_model;
+/* New's grid (fdtd.go:45-64): the time step and the cell counts including
+ * the absorbing layers. Host only. */
+int gfk_fdtd_grid(const gfk_fdtd_model *m, double *dt, int32_t *nr, int32_t *nz);
+/* fdtd.Run (internal/fdtd/run.go:78-127): `steps` steps of the axisymmetric
+ * velocity-stress scheme driven by a vertical surface force (force[n] newtons
+ * at step n, zero past nforce), recording the free-surface vertical velocity
+ * (fdtd.go:330-345) at the grid columns nearest `ranges` into traces
+ * [nrcv][steps] (host). snapped (host, nrcv, may be NULL) receives the column
+ * ranges; meta (host, 5): dt, t0 (= dt/2, the velocities' time offset), the
+ * largest particle speed seen, nr, nz. GFK_ENONFINITE with the reference's
+ * message when the run diverges; GFK_EARG for a receiver outside the
+ * interior or non-positive steps, spacing or domain. */
+int gfk_fdtd_run(gfk_ctx *ctx, const gfk_fdtd_model *m, const double *force, int32_t nforce,
+                 const double *ranges_m, int32_t nrcv, int32_t steps, double *traces, double *snapped,
+                 double *meta);
+
 /* ---- Rayleigh dispersion (internal/propmat, internal/disp) ---------------- */
 /* disp.Search (internal/disp/disp.go:30-54): samples <= 0 uses 2000 (at most
  * 16384), tolerance <= 0 uses 1e-10. */
