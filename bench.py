@@ -325,6 +325,61 @@ def run_sobol(args, gfk, torch, rank, world, local):
         print(json.dumps(out))
 
 
+def run_fdtd(args, gfk, torch, rank, world, local):
+    """The finite-difference validator on a grid far larger than L2: a lossy
+    (SLS, Q 25 at 30 Hz) two-layer model 60 m x 40 m at 2 cm spacing
+    (3021 x 2021 cells with the absorbing layers), K time steps after W
+    warm-up steps, two kernels per step."""
+    F = gfk.fdtd
+    eng = gfk.Engine(local)
+    st = gfk.Stack([gfk.Layer(2.0, 350.0, 140.0, 1600.0, 0, 0), gfk.Layer(0.0, 800.0, 320.0, 2000.0, 0, 0)])
+    md = F.Model(st, relax=gfk.SLS.fit(25.0, 30.0), ref_freq=30, max_range=60, depth=40, spacing=0.02,
+                 dominant_freq=25)
+    dt, nr, nz = md.grid()
+    force = F.ricker(1000, 25, dt, args.warmup + args.steps)
+    F.run(F.Shot(md, force, [5.0], max(args.warmup, 3)), engine=eng)  # warm the allocator and kernels
+    barrier(world)
+    t0 = time.perf_counter()
+    res = F.run(F.Shot(md, force, [5.0, 20.0], args.steps), engine=eng)
+    dt_wall = time.perf_counter() - t0  # run() returns after the stream is synchronised
+    t = allmax(dt_wall, world)
+    cells = nr * nz
+    # algorithmic bytes per cell-step (lossy interior): velocities read 6 fields, write 2;
+    # stresses read 10 (4 stresses, 2 velocities, 4 memory variables), write 8
+    bytes_per = (6 + 2 + 10 + 8) * 8
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import fdtd_oracle as FO
+        sim = FO.Sim([(2.0, 350.0, 140.0, 1600.0), (0.0, 800.0, 320.0, 2000.0)], FO.SLS.fit(25.0, 30.0), 30,
+                     60, 40, 0.02, dominant_freq=25)
+        sim.force = force
+        c0 = time.perf_counter()
+        ns = 0
+        while time.perf_counter() - c0 < 10.0:
+            sim.do_step()
+            ns += 1
+        cs = time.perf_counter() - c0
+        cpu = {"value": cells * ns / cs, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+               "sample": f"{ns} steps of the same grid through the numpy restatement (oracle/fdtd_oracle.py)"}
+    eng.close()
+    if rank == 0:
+        ms = 1e3 * t / args.steps
+        ach = cells * bytes_per / (ms * 1e-3) / 1e9
+        peak = (measured_peaks() or {}).get("hbm_gbs")
+        out = {"metric": "FDTD cell-updates/s (axisymmetric velocity-stress, SLS, C-PML)",
+               "value": cells * args.steps * world / t, "unit": "cell-updates/s", "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "gpu_launches": 2 * args.steps + (args.steps + 255) // 256,
+               "config": {"workload": f"fdtd: 2-layer lossy soil 60 m x 40 m at 2 cm ({nr} x {nz} cells), "
+                                      "Ricker 25 Hz vertical force, 2 receivers", "inputs_vs_l2": "fields, memory variables and C-PML state 0.9 GB > L2"},
+               "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                            "frac": ach / peak if peak else None, "traffic": None},
+               "cpu_baseline": cpu, "peak_speed": res.peak}
+        print(json.dumps(out))
+
+
 def run_train(args, gfk, torch, rank, world, local):
     """Surrogate training throughput: labels for --sur-soils family soils
     from the batched FP64 solver, then W warm-up and K timed AdamW steps of
@@ -448,7 +503,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--freq-stride", type=int, default=1,
                     help="profiling only: keep every n-th frequency (a smaller case of the same kernels)")
-    ap.add_argument("--workload", default="graded", choices=["graded", "batched", "sobol", "surrogate", "train"],
+    ap.add_argument("--workload", default="graded", choices=["graded", "batched", "sobol", "surrogate", "train", "fdtd"],
                     help="graded: the 10-layer graded soil (default); batched: seeded uneven soils; "
                          "sobol: the all-plain Sobol run")
     ap.add_argument("--sobol-n", type=int, default=16384, help="sobol workload: Saltelli base size N")
@@ -481,6 +536,8 @@ def main():
         return run_surrogate(args, gfk, torch, rank, world, local)
     if args.workload == "train":
         return run_train(args, gfk, torch, rank, world, local)
+    if args.workload == "fdtd":
+        return run_fdtd(args, gfk, torch, rank, world, local)
     wl = gfk.workloads.graded_soil()
     if args.freq_stride > 1:
         wl.freqs = wl.freqs[::args.freq_stride].copy()

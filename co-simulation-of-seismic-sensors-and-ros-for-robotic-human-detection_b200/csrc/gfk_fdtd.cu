@@ -15,7 +15,9 @@
 // contiguous): the velocity kernel also writes the prescribed surface
 // traction for this step, and the stress kernel also records the receivers
 // (their velocities are final by then). The arithmetic of every cell is the
-// reference's, in the same order; FP64 throughout. Every 256 steps a max-speed
+// reference's, in the same order, except that divisions by the spacing, the
+// radius and the density are multiplications by precomputed reciprocals (the
+// same values to a rounding); FP64 throughout. Every 256 steps a max-speed
 // reduction checks for divergence, as Run does.
 #include <cmath>
 #include <complex>
@@ -36,8 +38,12 @@ struct Args {
     double dr, dz, dt, src_area;
     bool lossy;
     double mem_decay, mem_drive;
-    // materials per row
+    // materials per row; the time step over the densities, precomputed
     const double *rho, *lamU, *muU, *rhoZ, *muZ;
+    const double *dt_rho, *dt_rhoZ;
+    // reciprocal spacings and radii: 1 / dr, 1 / dz, 1 / ((i + 1/2) dr), 1 / (i dr)
+    double idr, idz;
+    const double *ir_half, *ir_int;
     // C-PML profiles (a, b) and the first damped index of each
     const double *aRi, *bRi, *aRh, *bRh, *aZi, *bZi, *aZh, *bZh;
     int fRi, fRh, fZi, fZh;
@@ -72,29 +78,28 @@ __global__ void k_velocities(Args s, double surface_traction) {
     const int k = j * nr + i;
     // radial velocity
     {
-        double dtrr = (s.trr[k + 1] - s.trr[k]) / s.dr;
+        double dtrr = (s.trr[k + 1] - s.trr[k]) * s.idr;
         if (i >= s.fRh) dtrr += cpml(&s.psiTrrR[k], s.aRh[i], s.bRh[i], dtrr);
-        double dtrz = j == 0 ? 2 * s.trz[k] / s.dz : (s.trz[k] - s.trz[k - nr]) / s.dz;
+        double dtrz = j == 0 ? 2 * s.trz[k] * s.idz : (s.trz[k] - s.trz[k - nr]) * s.idz;
         if (j >= s.fZi) dtrz += cpml(&s.psiTrzZ[k], s.aZi[j], s.bZi[j], dtrz);
-        const double hoop =
-            0.5 * ((s.trr[k] - s.tqq[k]) + (s.trr[k + 1] - s.tqq[k + 1])) / ((double(i) + 0.5) * s.dr);
-        s.vr[k] += s.dt / s.rho[j] * (dtrr + dtrz + hoop);
+        const double hoop = 0.5 * ((s.trr[k] - s.tqq[k]) + (s.trr[k + 1] - s.tqq[k + 1])) * s.ir_half[i];
+        s.vr[k] += s.dt_rho[j] * (dtrr + dtrz + hoop);
     }
     // vertical velocity
     {
         const double tzz_k = k == 0 ? surface_traction : s.tzz[k];
         if (k == 0) s.tzz[0] = surface_traction;  // fdtd.go:144
-        double dtzz = (s.tzz[k + nr] - tzz_k) / s.dz;
+        double dtzz = (s.tzz[k + nr] - tzz_k) * s.idz;
         if (j >= s.fZh) dtzz += cpml(&s.psiTzzZ[k], s.aZh[j], s.bZh[j], dtzz);
         double radial;
         if (i == 0) {
-            radial = 4 * s.trz[k] / s.dr;
+            radial = 4 * s.trz[k] * s.idr;
         } else {
-            double d = (s.trz[k] - s.trz[k - 1]) / s.dr;
+            double d = (s.trz[k] - s.trz[k - 1]) * s.idr;
             if (i >= s.fRi) d += cpml(&s.psiTrzR[k], s.aRi[i], s.bRi[i], d);
-            radial = d + 0.5 * (s.trz[k] + s.trz[k - 1]) / (double(i) * s.dr);
+            radial = d + 0.5 * (s.trz[k] + s.trz[k - 1]) * s.ir_int[i];
         }
-        s.vz[k] += s.dt / s.rhoZ[j] * (dtzz + radial);
+        s.vz[k] += s.dt_rhoZ[j] * (dtzz + radial);
     }
 }
 
@@ -126,11 +131,11 @@ __global__ void k_stresses(Args s, double dTdt, int step) {
     // normal stresses
     double dvr, vrr;
     if (i == 0) {
-        dvr = 2 * s.vr[k] / s.dr;
+        dvr = 2 * s.vr[k] * s.idr;
         vrr = dvr;
     } else {
-        dvr = (s.vr[k] - s.vr[k - 1]) / s.dr;
-        vrr = 0.5 * (s.vr[k] + s.vr[k - 1]) / (double(i) * s.dr);
+        dvr = (s.vr[k] - s.vr[k - 1]) * s.idr;
+        vrr = 0.5 * (s.vr[k] + s.vr[k - 1]) * s.ir_int[i];
     }
     if (i >= s.fRi) dvr += cpml(&s.psiVrR[k], s.aRi[i], s.bRi[i], dvr);
     double dvz;
@@ -138,7 +143,7 @@ __global__ void k_stresses(Args s, double dTdt, int step) {
         const double applied = i == 0 ? dTdt : 0.0;
         dvz = (applied - lam * (dvr + vrr)) / lam2mu;
     } else {
-        dvz = (s.vz[k] - s.vz[k - nr]) / s.dz;
+        dvz = (s.vz[k] - s.vz[k - nr]) * s.idz;
         if (j >= s.fZi) dvz += cpml(&s.psiVzZ[k], s.aZi[j], s.bZi[j], dvz);
     }
     const double err = lam2mu * dvr + lam * (vrr + dvz);
@@ -159,9 +164,9 @@ __global__ void k_stresses(Args s, double dTdt, int step) {
     }
     // shear stress
     if (i < nr - 1 && j < s.nz - 1) {
-        double dvzdr = (s.vz[k + 1] - s.vz[k]) / s.dr;
+        double dvzdr = (s.vz[k + 1] - s.vz[k]) * s.idr;
         if (i >= s.fRh) dvzdr += cpml(&s.psiVzR[k], s.aRh[i], s.bRh[i], dvzdr);
-        double dvrdz = (s.vr[k + nr] - s.vr[k]) / s.dz;
+        double dvrdz = (s.vr[k + nr] - s.vr[k]) * s.idz;
         if (j >= s.fZh) dvrdz += cpml(&s.psiVrZ[k], s.aZh[j], s.bZh[j], dvrdz);
         const double e = s.muZ[j] * (dvzdr + dvrdz);
         if (s.lossy)
@@ -399,6 +404,21 @@ int gfk_fdtd_run(gfk_ctx* ctx, const gfk_fdtd_model* md, const double* force, in
         a.mem_decay = (1 - g.dt / (2 * tau)) / den;
         a.mem_drive = (g.dt * kappa / tau) / den;
     }
+    std::vector<double> dtr(nz), dtrz(nz), irh(nr), iri(nr, 0.0);
+    for (int j = 0; j < nz; j++) {
+        dtr[j] = g.dt / rho[j];
+        dtrz[j] = g.dt / rhoZ[j];
+    }
+    for (int i = 0; i < nr; i++) {
+        irh[i] = 1.0 / ((i + 0.5) * h);
+        if (i > 0) iri[i] = 1.0 / (i * h);
+    }
+    a.idr = 1.0 / h;
+    a.idz = 1.0 / h;
+    a.dt_rho = up(dtr);
+    a.dt_rhoZ = up(dtrz);
+    a.ir_half = up(irh);
+    a.ir_int = up(iri);
     a.rho = up(rho);
     a.lamU = up(lamU);
     a.muU = up(muU);
