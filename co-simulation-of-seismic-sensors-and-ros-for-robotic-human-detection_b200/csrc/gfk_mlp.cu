@@ -39,7 +39,9 @@ constexpr int STAGE_BYTES = 2 * BOX * TILE;    // 32768
 constexpr int STAGES = 3;
 constexpr int THREADS = 192;
 constexpr int TMEM_COLS = BN;                  // 128 FP32 accumulator columns
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256 + BN * 4;
+constexpr int kTileLd = BN + 8;  // BF16 row pitch of the epilogue's staging tiles (272 bytes)
+static_assert(2 * BM * kTileLd * 2 <= STAGES * STAGE_BYTES, "staging tiles alias the pipeline stages");
 
 // Instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = 128.
 __host__ __device__ inline uint32_t idesc_bf16_128x128() {
@@ -55,7 +57,9 @@ __host__ __device__ inline uint32_t idesc_bf16_128x128() {
     return id.desc_;
 }
 
-__device__ __forceinline__ float sigmoid_(float z) { return 1.0f / (1.0f + __expf(-z)); }
+// Hardware exponential and approximate reciprocal (no IEEE division): the
+// results are rounded to BF16 (8-bit mantissa) right after.
+__device__ __forceinline__ float sigmoid_(float z) { return __fdividef(1.0f, 1.0f + __expf(-z)); }
 
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
     __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
@@ -82,6 +86,7 @@ __global__ void __launch_bounds__(THREADS, 2)
     uint64_t* accf = empty + STAGES;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 1);
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+    float* bias_s = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES + 256);  // [BN]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
@@ -161,11 +166,23 @@ __global__ void __launch_bounds__(THREADS, 2)
             tc_commit(accf);
         }
     } else {
+        // epilogue, phase 1 (warps 2-5): TMEM -> registers -> elementwise work;
+        // BF16 results go to a shared-memory tile (the pipeline stages are free
+        // once every MMA has completed), FP32 gradient partials straight out
+        // the tile's bias columns, read once while the MMAs run
+        if (MODE == kFwdTrain || MODE == kFwdInfer) {
+            bias_s[threadIdx.x - 64] = a.bias[n0 + threadIdx.x - 64];
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+        }
         const bool ok = mbar_wait(accf, 0);
+        if (!ok) *(volatile int*)abort_flag = 1;  // the tile stays unwritten: no stores below
         tc_fence_after();
         const int q = warp & 3;
-        const int row = m0 + q * 32 + lane;
+        const int rl = q * 32 + lane;
+        const int row = m0 + rl;
         const bool row_ok = ok && !*(volatile int*)abort_flag;
+        bf16* tileO = reinterpret_cast<bf16*>(smem);
+        bf16* tileZ = tileO + BM * kTileLd;
 #pragma unroll 1
         for (int j = 0; j < BN / 32; j++) {
             uint32_t v[32];
@@ -186,11 +203,11 @@ __global__ void __launch_bounds__(THREADS, 2)
                 float zv[32];
 #pragma unroll
                 for (int c = 0; c < 32; c++) {
-                    zv[c] = __uint_as_float(v[c]) + a.bias[nb + c];
+                    zv[c] = __uint_as_float(v[c]) + bias_s[j * 32 + c];
                     y[c] = zv[c] * sigmoid_(zv[c]);
                 }
                 if (MODE == kFwdTrain) {
-                    uint4* zd = reinterpret_cast<uint4*>(a.zout + (size_t)row * a.N + nb);
+                    uint4* zd = reinterpret_cast<uint4*>(tileZ + rl * kTileLd + j * 32);
 #pragma unroll
                     for (int c = 0; c < 4; c++)
                         zd[c] = make_uint4(pack2(zv[8 * c], zv[8 * c + 1]), pack2(zv[8 * c + 2], zv[8 * c + 3]),
@@ -207,20 +224,46 @@ __global__ void __launch_bounds__(THREADS, 2)
                     y[c] = __uint_as_float(v[c]) * (sg * (1.0f + zv[c] * (1.0f - sg)));
                 }
             }
-            uint4* od = reinterpret_cast<uint4*>(a.out + (size_t)row * a.N + nb);
+            uint4* od = reinterpret_cast<uint4*>(tileO + rl * kTileLd + j * 32);
 #pragma unroll
             for (int c = 0; c < 4; c++)
                 od[c] = make_uint4(pack2(y[8 * c], y[8 * c + 1]), pack2(y[8 * c + 2], y[8 * c + 3]),
                                    pack2(y[8 * c + 4], y[8 * c + 5]), pack2(y[8 * c + 6], y[8 * c + 7]));
-            if (MODE != kFwdInfer && a.outT) {
-#pragma unroll
-                for (int c = 0; c < 32; c++) a.outT[(size_t)(nb + c) * a.M + row] = __float2bfloat16_rn(y[c]);
-            }
         }
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    // phase 2 (all warps): coalesced stores of the tile, its transpose and Z
+    if (MODE != kWgrad && !*(volatile int*)abort_flag) {
+        const bf16* tileO = reinterpret_cast<const bf16*>(smem);
+        const bf16* tileZ = tileO + BM * kTileLd;
+        for (int c = threadIdx.x; c < BM * (BN / 8); c += THREADS) {
+            const int r = c / (BN / 8), c8 = (c % (BN / 8)) * 8;
+            const size_t g = (size_t)(m0 + r) * a.N + n0 + c8;
+            *reinterpret_cast<uint4*>(a.out + g) = *reinterpret_cast<const uint4*>(tileO + r * kTileLd + c8);
+            if (MODE == kFwdTrain)
+                *reinterpret_cast<uint4*>(a.zout + g) = *reinterpret_cast<const uint4*>(tileZ + r * kTileLd + c8);
+        }
+        if (MODE != kFwdInfer && a.outT) {
+            // 32 bytes (16 rows) of one transposed row per thread; lanes run
+            // over columns, so the shared-memory column reads do not conflict
+            for (int c = threadIdx.x; c < BN * (BM / 16); c += THREADS) {
+                const int n = c % BN, r16 = (c / BN) * 16;
+                uint32_t w[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    __nv_bfloat162 v2;
+                    v2.x = tileO[(r16 + 2 * e) * kTileLd + n];
+                    v2.y = tileO[(r16 + 2 * e + 1) * kTileLd + n];
+                    w[e] = *reinterpret_cast<uint32_t*>(&v2);
+                }
+                uint4* d = reinterpret_cast<uint4*>(a.outT + (size_t)(n0 + n) * a.M + m0 + r16);
+                d[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                d[1] = make_uint4(w[4], w[5], w[6], w[7]);
+            }
+        }
+    }
     if (threadIdx.x == 0 && *(volatile int*)abort_flag && a.status) atomicOr(a.status, kStTimeout);
     if (warp == 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
