@@ -37,7 +37,7 @@ EXPORTS = [
     "gfk_dispersion_modes", "gfk_secular", "gfk_fdtd_grid", "gfk_fdtd_run",
     "gfk_trace_metrics", "gfk_ensemble_gate", "gfk_scatter_rows", "gfk_bank_tables", "gfk_bank_impulse_responses",
     "gfk_dataset_create", "gfk_dataset_fill", "gfk_dataset_stats", "gfk_dataset_labels", "gfk_dataset_destroy",
-    "gfk_net_create", "gfk_net_set_scales", "gfk_net_train", "gfk_net_predict", "gfk_net_evaluate",
+    "gfk_net_create", "gfk_net_set_scales", "gfk_net_train", "gfk_net_train_ranges", "gfk_net_predict", "gfk_net_evaluate",
     "gfk_net_param_count", "gfk_net_params", "gfk_net_fourier", "gfk_net_probe", "gfk_net_destroy",
 ]
 
@@ -151,6 +151,7 @@ def lib():
         "gfk_net_create": (ctypes.c_int, [vp, P(GfkNetConfig), P(vp)]),
         "gfk_net_set_scales": (ctypes.c_int, [vp, d, d, d, d, P(f32)]),
         "gfk_net_train": (ctypes.c_int, [vp, vp, P(i32), i32, i32, P(f32)]),
+        "gfk_net_train_ranges": (ctypes.c_int, [vp, vp, P(i32), i32, i32, i32, i32, P(f32)]),
         "gfk_net_predict": (ctypes.c_int, [vp, P(d), P(d), i32, P(d), i32, P(d), i32, vp, i32]),
         "gfk_net_evaluate": (ctypes.c_int, [vp, vp, P(i32), i32, P(d)]),
         "gfk_net_param_count": (i64, [vp]),

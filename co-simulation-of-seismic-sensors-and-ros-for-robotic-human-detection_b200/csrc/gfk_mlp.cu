@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(kIn) k_batch(BatchArgs a) {
         const unsigned long long h = mix64(a.seed ^ mix64(static_cast<unsigned long long>(t) * a.B + b));
         const int soil = a.train[pick(h, a.ntrain)];
         const unsigned long long h2 = mix64(h);
-        const int ir = pick(h2, a.nr), jf = pick(h2 >> 32, a.nf);
+        const int ir = a.ir0 + pick(h2, a.nir), jf = pick(h2 >> 32, a.nf);
         ps[j] = point_scalars(a.ranges[ir], a.freqs[jf], a.dom);
         soil_of[j] = soil;
         const float* L = a.labels + (((size_t)soil * a.nr + ir) * a.nf + jf) * 2;

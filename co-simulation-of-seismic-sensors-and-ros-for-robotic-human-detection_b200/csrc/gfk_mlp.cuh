@@ -88,6 +88,7 @@ struct BatchArgs {
     const float* soilfeat; // [nsoil][kSoilStride]
     const int* train;      // soils the batch draws from
     int ntrain, nr, nf, B;
+    int ir0, nir;          // ranges the batch draws from: [ir0, ir0 + nir)
     const double* ranges;  // [nr]
     const double* freqs;   // [nf]
     FeatureDomain dom;

@@ -127,6 +127,7 @@ struct gfk_net {
     int* d_status = nullptr;
     int* d_train = nullptr;
     int ntrain = 0;
+    int ir0 = 0, nir = 0;  // range window of the captured step
     const gfk_dataset* graph_ds = nullptr;
     std::vector<int> graph_train;
     cudaGraphExec_t gexec = nullptr;
@@ -248,6 +249,8 @@ int enqueue_step(gfk_net* n, const gfk_dataset* d) {
     b.ntrain = n->ntrain;
     b.nr = d->nr;
     b.nf = d->nf;
+    b.ir0 = n->ir0;
+    b.nir = n->nir;
     b.B = n->B;
     b.ranges = d->d_ranges;
     b.freqs = d->d_freqs;
@@ -696,15 +699,25 @@ int gfk_net_set_scales(gfk_net* n, double r_lo, double r_hi, double f_lo, double
     return GFK_OK;
 }
 
-int gfk_net_train(gfk_net* n, gfk_dataset* d, const int32_t* train, int32_t ntrain, int32_t steps, float* loss) {
+int gfk_net_train_ranges(gfk_net* n, gfk_dataset* d, const int32_t* train, int32_t ntrain, int32_t first_range,
+                         int32_t nranges, int32_t steps, float* loss) {
     if (!n || !d || !train || ntrain < 1 || steps < 0) return GFK_EARG;
     gfk_ctx* ctx = n->ctx;
     if (d->ctx != ctx) return sfail(ctx, GFK_EARG, "network and data set belong to different contexts");
     if (!n->scales) return sfail(ctx, GFK_EARG, "network scales are not set");
     if (d->nparam != n->cfg.nsoil_scalars) return sfail(ctx, GFK_EARG, "data set has a different soil scalar count");
+    if (first_range < 0 || nranges < 1 || first_range + nranges > d->nr)
+        return sfail(ctx, GFK_EARG, "training ranges [%d, %d) outside the data set's %d", first_range,
+                     first_range + nranges, d->nr);
     for (int i = 0; i < ntrain; i++)
         if (train[i] < 0 || train[i] >= d->nsoil || !d->filled[train[i]])
             return sfail(ctx, GFK_EARG, "training soil %d is not a filled soil of the data set", train[i]);
+    if (n->gexec && (n->ir0 != first_range || n->nir != nranges)) {  // the window is baked into the graph
+        cudaGraphExecDestroy(n->gexec);
+        n->gexec = nullptr;
+    }
+    n->ir0 = first_range;
+    n->nir = nranges;
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
     const bool same = n->gexec && n->graph_ds == d && n->graph_train.size() == (size_t)ntrain &&
@@ -764,6 +777,11 @@ int gfk_net_train(gfk_net* n, gfk_dataset* d, const int32_t* train, int32_t ntra
     }
     SG_CUDA(ctx, cudaGetLastError());
     return check_status(n);
+}
+
+int gfk_net_train(gfk_net* n, gfk_dataset* d, const int32_t* train, int32_t ntrain, int32_t steps, float* loss) {
+    if (!d) return GFK_EARG;
+    return gfk_net_train_ranges(n, d, train, ntrain, 0, d->nr, steps, loss);
 }
 
 int gfk_net_predict(gfk_net* n, const double* scalars, const double* times, int32_t ns, const double* ranges,

@@ -278,12 +278,15 @@ class Net:
                         [m0, s0, m1, s1])
 
     # -- training -----------------------------------------------------------
-    def train(self, ds, soils, steps):
-        """`steps` AdamW steps on cells of the given data set soils; returns
-        the per-step (amplitude, phase) mean squared errors."""
+    def train(self, ds, soils, steps, ranges=None):
+        """`steps` AdamW steps on cells of the given data set soils (and, if
+        given, only the data set's range indices [ranges[0], ranges[1]));
+        returns the per-step (amplitude, phase) mean squared errors."""
         soils = np.ascontiguousarray(soils, dtype=np.int32)
         loss = np.zeros((steps, 2), dtype=np.float32)
-        self.engine.check(N.lib().gfk_net_train(self.p, ds.p, _ip(soils), len(soils), int(steps), _fp(loss)))
+        r0, r1 = ranges if ranges is not None else (0, len(ds.grid.ranges))
+        self.engine.check(N.lib().gfk_net_train_ranges(self.p, ds.p, _ip(soils), len(soils), int(r0), int(r1 - r0),
+                                                       int(steps), _fp(loss)))
         self.steps_done += steps
         return loss
 
@@ -362,8 +365,9 @@ def split_soils(n, holdout=0.05, seed=0):
     return np.sort(perm[k:]).astype(np.int32), np.sort(perm[:k]).astype(np.int32)
 
 
-def train_ensemble(ds, train, members=4, steps=40000, config=None, engine=None, log=None):
-    """`members` networks differing in initial weights, Fourier frequencies and batches."""
+def train_ensemble(ds, train, members=4, steps=40000, config=None, engine=None, log=None, ranges=None):
+    """`members` networks differing in initial weights, Fourier frequencies and
+    batches; `ranges` restricts training to range indices [r0, r1)."""
     nets = []
     for m in range(members):
         cfg = NetConfig(**{**(config.__dict__ if config else {}), "seed": (config.seed if config else 1) + 7919 * m,
@@ -371,7 +375,7 @@ def train_ensemble(ds, train, members=4, steps=40000, config=None, engine=None, 
         net = Net(cfg, engine)
         net.scales_from(ds)
         t = time.perf_counter()
-        loss = net.train(ds, train, steps)
+        loss = net.train(ds, train, steps, ranges)
         if log:
             log(f"member {m}: {steps} steps in {time.perf_counter() - t:.1f} s, final loss "
                 f"{loss[-100:, 0].mean():.3e} / {loss[-100:, 1].mean():.3e}")

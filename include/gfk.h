@@ -457,6 +457,11 @@ int gfk_net_set_scales(gfk_net *net, double r_lo, double r_hi, double f_lo, doub
  * coefficient-weighted mean squared errors of the two standardised targets. */
 int gfk_net_train(gfk_net *net, gfk_dataset *ds, const int32_t *train_soils, int32_t ntrain,
                   int32_t steps, float *loss);
+/* As gfk_net_train, drawing only from the data set's ranges [first_range,
+ * first_range + nranges): a network that serves one sensor range (the Sobol
+ * workload's 10 m) spends its capacity there. */
+int gfk_net_train_ranges(gfk_net *net, gfk_dataset *ds, const int32_t *train_soils, int32_t ntrain,
+                         int32_t first_range, int32_t nranges, int32_t steps, float *loss);
 /* G for ns soils at every (frequency, range) pair: out[2 ((s nf + j) nr + i)]
  * (re, im). out is device memory when out_on_device is nonzero. soil_times
  * as in gfk_dataset_create. */

@@ -194,3 +194,42 @@ def test_surrogate_sobol_plumbing(pkg, eng):
     assert none.seconds["fallback_rows"] == 0 and np.isfinite(none.metrics["peak"]).all()
     for n_ in nets:
         n_.close()
+
+
+def test_ensemble_gate_and_scatter_match_numpy(pkg, eng):
+    """gfk_ensemble_gate (mean, trace-weighted spread flags, per-soil worst
+    ratio) and gfk_scatter_rows against numpy on random member spectra."""
+    import torch
+    sob = pkg.sobol
+    setup = sob.TraceSetup()
+    S = sob.shaping(setup)
+    rng = np.random.default_rng(9)
+    E, ns, nb = 3, 7, 512
+    G = (rng.normal(size=(E, ns, nb)) + 1j * rng.normal(size=(E, ns, nb))) * 1e-9
+    G[1:] = G[0] + 0.05 * (G[1:] - G[0])  # members close to each other
+    dev = [torch.from_numpy(np.stack([g.real, g.imag], axis=-1).ravel()).to("cuda:0") for g in G]
+    mean = torch.zeros(ns * nb * 2, dtype=torch.float64, device="cuda:0")
+    ptrs = (ctypes.c_void_p * E)(*[d.data_ptr() for d in dev])
+    Sh = np.ascontiguousarray(np.stack([S.real, S.imag], axis=1).ravel())
+    flags = np.zeros((ns, nb), dtype=np.uint8)
+    spread = np.zeros(ns)
+    thr = 0.02
+    eng.check(pkg._native.lib().gfk_ensemble_gate(
+        eng.ctx, ptrs, E, nb, ns, nb, Sh.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), thr,
+        ctypes.c_void_p(mean.data_ptr()), flags.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+        spread.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    m = G.mean(axis=0)
+    got = mean.cpu().numpy().reshape(ns, nb, 2)
+    assert np.allclose(got[..., 0] + 1j * got[..., 1], m, rtol=1e-14, atol=1e-30)
+    d = np.abs(G - m[None]).max(axis=0) * np.abs(S[1:])[None]
+    ratio = d / np.abs(m * S[1:][None]).max(axis=1, keepdims=True)
+    assert np.array_equal(flags.astype(bool), ratio > thr)
+    assert np.allclose(spread, ratio.max(axis=1), rtol=1e-12)
+    # scatter three rows back from a packed source
+    src = torch.from_numpy(np.array([1.0, 2.0, 3.0, 4.0, 5.0, 6.0])).to("cuda:0")
+    idx = np.array([5, 700, 3583], dtype=np.int64)
+    eng.check(pkg._native.lib().gfk_scatter_rows(eng.ctx, ctypes.c_void_p(src.data_ptr()), 1,
+                                                 idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), 3,
+                                                 ctypes.c_void_p(mean.data_ptr())))
+    out = mean.cpu().numpy().reshape(-1, 2)
+    assert np.array_equal(out[idx], [[1, 2], [3, 4], [5, 6]])
