@@ -124,6 +124,8 @@ int check_layer_phase(gfk_ctx* ctx, const gfk_medium* m, double f) {  // fk.go:2
     return GFK_OK;
 }
 
+int grid_for_bounds(const gfk_medium* m, double rmin, double rmax, double f, gfk_integration opt, gfk_grid* out);
+
 int grid_for(gfk_ctx* ctx, const gfk_medium* m, const double* ranges, int nr, double f, gfk_integration opt,
              gfk_grid* out) {  // fk.go:464-495
     if (nr <= 0 || !ranges) return fail(ctx, GFK_EARG, "fk: no ranges given");
@@ -134,6 +136,12 @@ int grid_for(gfk_ctx* ctx, const gfk_medium* m, const double* ranges, int nr, do
         rmin = std::min(rmin, ranges[i]);
         rmax = std::max(rmax, ranges[i]);
     }
+    return grid_for_bounds(m, rmin, rmax, f, opt, out);
+}
+
+// GridFor's rule once the range bounds are known (a plan computes them once
+// for all its frequencies).
+int grid_for_bounds(const gfk_medium* m, double rmin, double rmax, double f, gfk_integration opt, gfk_grid* out) {
     const double kbody = kTwoPi * f / slowest_vs(m);
     const double kmf = opt.kmax_factor > 0 ? opt.kmax_factor : 30;
     const double kmax = std::max(opt.kmax > 0 ? opt.kmax : kmf * kbody, 40 / rmin);
@@ -353,8 +361,11 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
     p->nf = (int)nf_total;
     p->nr = nr;
     const bool guard = s->guard || s->formulation == GFK_REFERENCE_DIRECT;
-    double rmin = INFINITY;
-    for (double r : p->ranges) rmin = std::min(rmin, r);
+    double rmin = INFINITY, rmax = 0;
+    for (double r : p->ranges) {
+        rmin = std::min(rmin, r);
+        rmax = std::max(rmax, r);
+    }
     p->host_status.assign(p->nf, GFK_OK);
     p->fd.assign(p->nf, gfk::FreqDesc{});
     p->freqs.assign(p->nf, 0.0);
@@ -409,7 +420,7 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
             gfk_grid g{0, 0, 0};
             if (!st && m && m->layers && m->count > 0) {
                 if (mode == kGridMulti) {
-                    st = grid_for(ctx, m, p->ranges.data(), nr, fr, opt, &g);
+                    st = grid_for_bounds(m, rmin, rmax, fr, opt, &g);  // ranges validated above
                 } else {  // Medium.VerticalDisplacement's own rule (fk.go:407-421)
                     const double kbody = kTwoPi * fr / slowest;
                     const double kmf = opt.kmax_factor > 0 ? opt.kmax_factor : 30;
