@@ -306,13 +306,21 @@ class Plan:
         self.engine.check(N.lib().gfk_plan_result_device(self.p, ctypes.byref(d)))
         return d.value
 
-    def download(self, raise_on_error=True):
-        out = np.zeros((len(self.freqs), 2 * len(self.ranges)))
+    def download(self, raise_on_error=True, out=None):
+        """([rows, ranges] complex128, per-row status). The rows land directly
+        in a complex array (its memory is the (re, im) pairs the ABI writes);
+        `out` may supply one (e.g. in pinned memory) to reuse."""
+        shape = (len(self.freqs), len(self.ranges))
+        if out is None:
+            out = np.empty(shape, dtype=np.complex128)
+        elif out.shape != shape or out.dtype != np.complex128 or not out.flags.c_contiguous:
+            raise FkError(N.EARG, f"download buffer must be a C-contiguous complex128 array of shape {shape}")
         status = np.zeros(len(self.freqs), dtype=np.int32)
-        st = N.lib().gfk_plan_download(self.p, _dp(out), status.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        st = N.lib().gfk_plan_download(self.p, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                       status.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
         if st and raise_on_error:
             self.engine.check(st)
-        return out[:, 0::2] + 1j * out[:, 1::2], status
+        return out, status
 
     def statuses(self):
         """Per-row status codes of the last execute, without moving the result."""
