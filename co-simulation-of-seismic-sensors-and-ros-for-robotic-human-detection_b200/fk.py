@@ -392,6 +392,56 @@ class Batch(Plan):
         """Splits a [sum nf, ...] result into one array per medium."""
         return np.split(rows, np.cumsum(self.counts)[:-1])
 
+    @classmethod
+    def from_layers(cls, layers, counts, freqs, ranges, opt=None, solve=None, engine=None, freqs_per_medium=None):
+        """A batch plan built straight from arrays, for sweeps over many soils:
+        layers [total entries, 6] (thickness, Vp, Vs, density, Qs, Qp; each
+        medium's entries consecutive, half-space last), counts [media]; every
+        medium solved at `freqs` unless `freqs_per_medium` (a list of arrays)
+        is given. solve: (formulation, quadrature, omega_imag); media take the
+        default reference frequency and Q."""
+        self = cls.__new__(cls)
+        self.p = None
+        self.engine = engine or default_engine()
+        lay = np.ascontiguousarray(layers, dtype=np.float64)
+        cnt = np.ascontiguousarray(counts, dtype=np.int32)
+        nm = len(cnt)
+        if lay.ndim != 2 or lay.shape[1] != 6 or int(cnt.sum()) != len(lay) or nm == 0:
+            raise FkError(N.EARG, "layers must be [sum(counts), 6] and counts non-empty")
+        starts = np.concatenate([[0], np.cumsum(cnt)[:-1]]).astype(np.uint64)
+        med_dt = np.dtype([("layers", np.uint64), ("count", np.int32), ("_pad", np.int32), ("ref", np.float64),
+                           ("dq", np.float64), ("ts", np.float64), ("te", np.float64)])
+        meds = np.zeros(nm, dtype=med_dt)
+        meds["layers"] = np.uint64(lay.ctypes.data) + starts * np.uint64(48)
+        meds["count"] = cnt
+        self.ranges = np.ascontiguousarray(ranges, dtype=np.float64)
+        if freqs_per_medium is None:
+            f = np.ascontiguousarray(freqs, dtype=np.float64)
+            self._freqs = [f] * nm
+            fptr = np.full(nm, f.ctypes.data, dtype=np.uint64)
+            nfs = np.full(nm, len(f), dtype=np.int32)
+        else:
+            self._freqs = [np.ascontiguousarray(x, dtype=np.float64) for x in freqs_per_medium]
+            if len(self._freqs) != nm:
+                raise FkError(N.EARG, "one frequency list per medium")
+            fptr = np.array([x.ctypes.data for x in self._freqs], dtype=np.uint64)
+            nfs = np.array([len(x) for x in self._freqs], dtype=np.int32)
+        self.freqs = np.concatenate(self._freqs) if self._freqs else np.zeros(0)
+        self.counts = nfs.astype(np.int64)
+        form, quad, wi = solve if solve is not None else (N.DUNKIN, N.PLAIN_FP64, 0.0)
+        sv = N.GfkSolve(int(form), int(quad), 0, 0, float(wi))
+        opt = opt or Integration()
+        h = ctypes.c_void_p()
+        st = N.lib().gfk_batch_create(self.engine.ctx, meds.ctypes.data_as(ctypes.POINTER(N.GfkMedium)), nm,
+                                      fptr.ctypes.data_as(ctypes.POINTER(ctypes.POINTER(ctypes.c_double))),
+                                      nfs.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(sv),
+                                      _dp(self.ranges), len(self.ranges), opt.c(), ctypes.byref(h))
+        del lay, meds
+        self.engine.check(st)
+        self.p = h
+        self.engine._plans.add(self)
+        return self
+
 
 # ----------------------------------------------------------------- plumbing --
 

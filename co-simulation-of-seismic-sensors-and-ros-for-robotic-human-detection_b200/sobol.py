@@ -107,6 +107,20 @@ def soil_of(p):
                   Layer(0.0, 2.0 * vsh, vsh, 2000.0, 40.0, 80.0)])
 
 
+def layer_table(params):
+    """soil_of for many rows at once: ([3 n, 6] layer entries, [n] counts),
+    the arrays Batch.from_layers takes."""
+    p = np.asarray(params, dtype=np.float64)
+    vs1, r1, q1, vs2, r2, q2, h1, vsh = p.T
+    n = len(p)
+    out = np.empty((n, 3, 6))
+    out[:, 0] = np.stack([h1, r1 * vs1, vs1, np.full(n, 1700.0), q1, 2 * q1], axis=1)
+    out[:, 1] = np.stack([np.full(n, 2.0), r2 * vs2, vs2, np.full(n, 1850.0), q2, 2 * q2], axis=1)
+    out[:, 2] = np.stack([np.zeros(n), 2.0 * vsh, vsh, np.full(n, 2000.0), np.full(n, 40.0), np.full(n, 80.0)],
+                         axis=1)
+    return out.reshape(3 * n, 6), np.full(n, 3, dtype=np.int32)
+
+
 # ------------------------------------------------------------------ source --
 
 @dataclass
@@ -329,9 +343,9 @@ def solve_metrics(params, setup, engine, batch_soils=20000, nk=NK, kmax=KMAX, fo
     gpu_s = 0.0
     for b0 in range(0, len(params), batch_soils):
         chunk = params[b0:b0 + batch_soils]
-        media = [Medium(soil_of(p), formulation=formulation, omega_imag=setup.omega_imag, engine=engine)
-                 for p in chunk]
-        plan = Batch(media, [freqs] * len(media), [setup.r], opt, engine=engine)
+        lay, cnt = layer_table(chunk)
+        plan = Batch.from_layers(lay, cnt, freqs, [setup.r], opt, (formulation, N.PLAIN_FP64, setup.omega_imag),
+                                 engine=engine)
         try:
             plan.execute()
             status = plan.statuses()
@@ -418,9 +432,9 @@ def _solve_rows(params, bins_per_soil, setup, engine, batch_soils, nk=NK, kmax=K
     soils = [i for i, b in enumerate(bins_per_soil) if len(b)]
     for b0 in range(0, len(soils), batch_soils):
         group = soils[b0:b0 + batch_soils]
-        media = [Medium(soil_of(params[i]), formulation=formulation, omega_imag=setup.omega_imag, engine=engine)
-                 for i in group]
-        plan = Batch(media, [freqs[bins_per_soil[i]] for i in group], [setup.r], opt, engine=engine)
+        lay, cnt = layer_table(params[group])
+        plan = Batch.from_layers(lay, cnt, None, [setup.r], opt, (formulation, N.PLAIN_FP64, setup.omega_imag),
+                                 engine=engine, freqs_per_medium=[freqs[bins_per_soil[i]] for i in group])
         try:
             plan.execute()
             status = plan.statuses()

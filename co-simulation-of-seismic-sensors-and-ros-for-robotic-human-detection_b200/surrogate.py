@@ -52,6 +52,20 @@ def soil_of(p):
                   Layer(0.0, DEEP_VPVS * vsh, vsh, DENSITY[3], DEEP_QS, 2 * DEEP_QS)])
 
 
+def layer_table(params):
+    """soil_of for many rows at once: ([4 n, 6] layer entries, [n] counts)."""
+    p = np.asarray(params, dtype=np.float64)
+    vs1, r1, q1, h1, vs2, r2, q2, h2, vs3, h3, vsh = p.T
+    n = len(p)
+    c = lambda x: np.full(n, x)
+    out = np.empty((n, 4, 6))
+    out[:, 0] = np.stack([h1, r1 * vs1, vs1, c(DENSITY[0]), q1, 2 * q1], axis=1)
+    out[:, 1] = np.stack([h2, r2 * vs2, vs2, c(DENSITY[1]), q2, 2 * q2], axis=1)
+    out[:, 2] = np.stack([h3, DEEP_VPVS * vs3, vs3, c(DENSITY[2]), c(DEEP_QS), c(2 * DEEP_QS)], axis=1)
+    out[:, 3] = np.stack([c(0.0), DEEP_VPVS * vsh, vsh, c(DENSITY[3]), c(DEEP_QS), c(2 * DEEP_QS)], axis=1)
+    return out.reshape(4 * n, 6), np.full(n, 4, dtype=np.int32)
+
+
 def draw(n, seed):
     """n soils uniform on the family's box (log-uniform where marked)."""
     u = np.random.default_rng(seed).random((n, NPARAM))
@@ -133,9 +147,9 @@ def solve_media(params, grid, engine, ranges=None, batch_soils=8192, each=None):
     ms = 0.0
     for b0 in range(0, len(params), batch_soils):
         chunk = params[b0:b0 + batch_soils]
-        media = [Medium(soil_of(p), formulation=N.DUNKIN, omega_imag=grid.omega_imag, quadrature=N.PLAIN_FP64,
-                        engine=engine) for p in chunk]
-        plan = Batch(media, [freqs] * len(media), ranges, opt, engine=engine)
+        lay, cnt = layer_table(chunk)
+        plan = Batch.from_layers(lay, cnt, freqs, ranges, opt, (N.DUNKIN, N.PLAIN_FP64, grid.omega_imag),
+                                 engine=engine)
         try:
             plan.execute()
             st = plan.statuses()

@@ -167,3 +167,16 @@ def test_adam_oracle_first_step():
     g = np.array([0.3, -1e-3, 2.0])
     q, m, v = SO.adam_step(p, np.zeros(3), np.zeros(3), g, 1, 1e-2)
     assert np.allclose(q, p - 1e-2 * np.sign(g), atol=1e-9)
+
+
+def test_layer_tables_equal_stacks(pkg):
+    """The vectorised layer tables the batch solves use equal the per-soil stacks."""
+    sob, sur = pkg.sobol, pkg.surrogate
+    p8 = sob.unit_to_params(np.random.default_rng(11).random((7, 8)))
+    lay, cnt = sob.layer_table(p8)
+    want = np.array([[l.thickness, l.vp, l.vs, l.density, l.qs, l.qp] for p in p8 for l in sob.soil_of(p)])
+    assert np.array_equal(lay, want) and (cnt == 3).all()
+    p11 = sur.draw(7, 12)
+    lay, cnt = sur.layer_table(p11)
+    want = np.array([[l.thickness, l.vp, l.vs, l.density, l.qs, l.qp] for p in p11 for l in sur.soil_of(p)])
+    assert np.array_equal(lay, want) and (cnt == 4).all()
