@@ -322,7 +322,8 @@ def run_sobol(args, gfk, torch, rank, world, local):
                                       "75 kg footstep through an SM-24-like geophone (10 Hz, 0.7)",
                           "soils": res.seconds["soils"], "rows": cells},
                "e2e": {"value": cells / wall, "unit": UNIT, "s_per_run": wall,
-                       "h2d_bytes_per_step": res.seconds["soils"] * 3 * 48, "d2h_bytes_per_step": cells * 16},
+                       "h2d_bytes_per_step": res.seconds["soils"] * 3 * 48 + 513 * 16,
+                       "d2h_bytes_per_step": res.seconds["soils"] * 2 * 8 + cells * 4},
                "sobol": {"S1": res.s1, "ST": res.st,
                          "seconds": {k: v for k, v in res.seconds.items() if k not in ("rows", "soils")}}}
         print(json.dumps(out))
