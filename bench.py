@@ -193,7 +193,7 @@ def run_reference(args):
         return
     import __graft_entry__
     gfk = __graft_entry__.load_package()
-    wl = gfk.workloads.graded_soil()
+    wl = gfk.workloads.single_soil() if args.workload == "single" else gfk.workloads.graded_soil()
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_baseline(gfk, wl, threads, target_s=2.0)
@@ -217,14 +217,19 @@ def run_reference(args):
 
 
 def config_of(wl, note):
-    return {"workload": f"{wl.name}: 10 finite 0.8 m layers (Vs 120->600 m/s, Vp=2Vs, rho 1600->2100, "
-                        f"Qs 10->60, Qp=2Qs) over a half-space; {len(wl.freqs)} bins 0-500 Hz (fs 1 kHz), "
+    if wl.name == "single_soil":
+        soil = ("0.5 m (Vs 150, Vp 300, rho 1700, Qs 15, Qp 30) and 2 m (250, 500, 1800, 25, 50) layers over a "
+                "half-space (400, 800, 2000, 40, 80)")
+        l2 = "L2 flushed (256 MiB write) between timed steps; the 32 MB integrand fits in L2"
+    else:
+        soil = ("10 finite 0.8 m layers (Vs 120->600 m/s, Vp=2Vs, rho 1600->2100, Qs 10->60, Qp=2Qs) over a "
+                "half-space")
+        l2 = "intermediates (537 MB integrand, 134 MB J0 table) exceed L2; L2 also flushed (256 MiB write) between timed steps"
+    return {"workload": f"{wl.name}: {soil}; {len(wl.freqs)} bins 0-500 Hz (fs 1 kHz), "
                         f"{wl.samples} wavenumbers to {wl.kmax:.1f} rad/m, {len(wl.ranges)} ranges "
                         f"{wl.ranges[0]:g}-{wl.ranges[-1]:g} m, w_I = pi/T",
             "soils": 1, "frequencies": len(wl.freqs), "wavenumbers": wl.samples, "ranges": len(wl.ranges),
-            "cells_per_step": wl.cells(), "l2": "intermediates (537 MB integrand, 134 MB J0 table) exceed L2; "
-                                                  "L2 also flushed (256 MiB write) between timed steps",
-            "note": note}
+            "cells_per_step": wl.cells(), "l2": l2, "note": note}
 
 
 def run_batched(args, gfk, torch, rank, world, local):
@@ -507,7 +512,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--freq-stride", type=int, default=1,
                     help="profiling only: keep every n-th frequency (a smaller case of the same kernels)")
-    ap.add_argument("--workload", default="graded", choices=["graded", "batched", "sobol", "surrogate", "train", "fdtd"],
+    ap.add_argument("--workload", default="graded", choices=["graded", "single", "batched", "sobol", "surrogate", "train",
+                                                              "fdtd"],
                     help="graded: the 10-layer graded soil (default); batched: seeded uneven soils; "
                          "sobol: the all-plain Sobol run")
     ap.add_argument("--sobol-n", type=int, default=16384, help="sobol workload: Saltelli base size N")
@@ -542,7 +548,7 @@ def main():
         return run_train(args, gfk, torch, rank, world, local)
     if args.workload == "fdtd":
         return run_fdtd(args, gfk, torch, rank, world, local)
-    wl = gfk.workloads.graded_soil()
+    wl = gfk.workloads.single_soil() if args.workload == "single" else gfk.workloads.graded_soil()
     if args.freq_stride > 1:
         wl.freqs = wl.freqs[::args.freq_stride].copy()
     eng = gfk.Engine(local)

@@ -8,7 +8,7 @@ step over the whole grid) and returns the surface traces.
 """
 import ctypes
 import math
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -30,8 +30,8 @@ class Model:
     dominant_freq: float = 0.0
     courant: float = 0.0
 
-    def c(self, holder):
-        return N.GfkFdtdModel(holder.c, float(self.max_range), float(self.depth), float(self.spacing),
+    def c(self, cmedium):
+        return N.GfkFdtdModel(cmedium, float(self.max_range), float(self.depth), float(self.spacing),
                               int(self.pml_cells), 0, float(self.pml_reflection), float(self.dominant_freq),
                               float(self.courant))
 
@@ -41,9 +41,8 @@ class Model:
     def grid(self):
         """(dt, nr, nz) of the simulation New builds (fdtd.go:45-64)."""
         with _c_medium(self._medium()) as cm:
-            holder = type("H", (), {"c": cm})
             dt, nr, nz = ctypes.c_double(), ctypes.c_int32(), ctypes.c_int32()
-            st = N.lib().gfk_fdtd_grid(ctypes.byref(self.c(holder)), ctypes.byref(dt), ctypes.byref(nr),
+            st = N.lib().gfk_fdtd_grid(ctypes.byref(self.c(cm)), ctypes.byref(dt), ctypes.byref(nr),
                                        ctypes.byref(nz))
         if st:
             raise FkError(st, f"fdtd: invalid model ({N.status_string(st)})")
@@ -114,8 +113,7 @@ def run(shot, engine=None):
     meta = np.zeros(5)
     dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     with _c_medium(shot.model._medium()) as cm:
-        holder = type("H", (), {"c": cm})
-        st = N.lib().gfk_fdtd_run(eng.ctx, ctypes.byref(shot.model.c(holder)), dp(force), len(force), dp(r), len(r),
+        st = N.lib().gfk_fdtd_run(eng.ctx, ctypes.byref(shot.model.c(cm)), dp(force), len(force), dp(r), len(r),
                                   int(shot.steps), dp(traces), dp(snapped), dp(meta))
     eng.check(st)
     return Result(meta[0], meta[1], [Trace(float(snapped[i]), traces[i]) for i in range(len(r))],

@@ -24,14 +24,13 @@ along range like internal/bank/interp.go:66-102 (see gfk_mlp.cu k_labels).
 """
 import ctypes
 import math
-import pathlib
 import time
 from dataclasses import dataclass, field
 
 import numpy as np
 
 from . import _native as N
-from .fk import Batch, FkError, Integration, Layer, Medium, Stack, default_engine
+from .fk import Batch, FkError, Integration, Layer, Stack, default_engine
 
 PARAMS = [
     ("vs1", 80.0, 600.0, True), ("vpvs1", 1.7, 3.0, False), ("qs1", 10.0, 60.0, False), ("h1", 0.2, 5.0, True),
