@@ -443,7 +443,11 @@ def run_surrogate(args, gfk, torch, rank, world, local):
     eng = gfk.Engine(local)
     log = (lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else (lambda m: None)
     t0 = time.perf_counter()
-    params = U.draw(args.sur_soils, 20240611)
+    if args.sur_family == "sobol":
+        # the Sobol soils' own 8-parameter box, as members of the 11-scalar family
+        params = U.from_sobol(S.unit_to_params(np.random.default_rng(20240611).random((args.sur_soils, 8))))
+    else:
+        params = U.draw(args.sur_soils, 20240611)
     ds = U.Dataset(params, U.LabelGrid(), floor_rel=1e-6, engine=eng).fill(batch_soils=8192)
     t_data = time.perf_counter() - t0
     m0, s0, m1, s1, frac = ds.stats()
@@ -452,7 +456,9 @@ def run_surrogate(args, gfk, torch, rank, world, local):
     train, held = U.split_soils(args.sur_soils, 0.05, 0)
     cfg = U.NetConfig(total_steps=args.sur_steps, lr_max=args.sur_lr, fourier_sigma=args.sur_sigma)
     t1 = time.perf_counter()
-    nets = U.train_ensemble(ds, train, members=args.members, steps=args.sur_steps, config=cfg, engine=eng, log=log)
+    ranges = tuple(int(x) for x in args.sur_ranges.split(",")) if args.sur_ranges else None
+    nets = U.train_ensemble(ds, train, members=args.members, steps=args.sur_steps, config=cfg, engine=eng, log=log,
+                            ranges=ranges)
     t_train = time.perf_counter() - t1
     evals = [n.evaluate(ds, held) for n in nets]
     for i, e in enumerate(evals):
@@ -489,7 +495,8 @@ def run_surrogate(args, gfk, torch, rank, world, local):
                "value": speed, "unit": "x", "n_gpus": world, "steps": 1, "warmup": 0,
                "ms_per_step": 1e3 * res_s.seconds["total"], "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
-               "config": {"workload": f"surrogate: {args.sur_soils} 3-layer soils x 64 ranges x 512 bins labels, "
+               "config": {"workload": f"surrogate: {args.sur_soils} 3-layer soils ({args.sur_family} box) x 64 ranges "
+                                      f"x 512 bins labels (training ranges {args.sur_ranges or 'all'}), "
                                       f"{args.members} x MLP 6x512 SiLU BF16 {args.sur_steps} steps batch 8192; "
                                       f"Sobol N={args.sobol_n} d=8 at 10 m; f-k fallback on the rows where the "
                                       f"ensemble spread exceeds {args.threshold:.0%} of the trace-spectrum peak"},
@@ -523,6 +530,10 @@ def main():
     ap.add_argument("--sur-lr", type=float, default=3e-4)
     ap.add_argument("--sur-sigma", type=float, default=8.0, help="Fourier feature frequency std")
     ap.add_argument("--members", type=int, default=4, help="surrogate ensemble size")
+    ap.add_argument("--sur-family", default="box", choices=["box", "sobol"],
+                    help="surrogate training soils: box = the 11-scalar family's box; sobol = the Sobol "
+                         "soils' 8-parameter box inside it")
+    ap.add_argument("--sur-ranges", default="", help="surrogate training range indices r0,r1 (default: all)")
     ap.add_argument("--threshold", type=float, default=0.01, help="ensemble spread above which soils fall back")
     ap.add_argument("--save-nets", default="", help="directory to save the trained members")
     ap.add_argument("--quadrature", default="split", choices=["split", "fp64"],

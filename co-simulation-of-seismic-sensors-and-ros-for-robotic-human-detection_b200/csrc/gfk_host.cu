@@ -220,6 +220,9 @@ struct gfk_plan {
     int8_t *d_A = nullptr, *d_B = nullptr;
     int* d_rowexp = nullptr;
     unsigned long long* d_rowmax = nullptr;
+    // split-K wavenumber sums for chunks too small to fill the SMs
+    int ksplit = 1;
+    cd* d_ksum = nullptr;  // [ksplit][rows of a chunk][nr] partial sums
     int32_t launches_per_exec = 0;
     int prop_variant = -1;       // Dunkin launch shape; -1 until the first execute tunes it
     std::vector<float> tune_ms;  // per variant, from the tuning run
@@ -245,7 +248,7 @@ void plan_free(gfk_plan* p) {
     if (p->gexec) cudaGraphExecDestroy(p->gexec);
     void* ptrs[] = {p->d_lp,  p->d_media, p->d_fd, p->d_ranges, p->d_W, p->d_lc,     p->d_wc2,
                     p->d_C,   p->d_rem,   p->d_G,  p->d_status, p->d_A, p->d_B,      p->d_rowexp,
-                    p->d_rowmax, p->d_partial};
+                    p->d_rowmax, p->d_partial, p->d_ksum};
     for (void* q : ptrs)
         if (q) cudaFreeAsync(q, s);
     for (auto& sg : p->segs) {
@@ -541,6 +544,16 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
         if (!st && cudaMemsetAsync(p->d_A, 0, (size_t)4 * p->Mp * p->Kp, ctx->stream) != cudaSuccess)
             st = fail(ctx, GFK_ECUDA, "clearing the slice planes failed");
     }
+    if (!st && p->shared && !p->fused) {
+        int max_cnf = 0;
+        for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
+            max_cnf = std::max(max_cnf, p->chunk_begin[c + 1] - p->chunk_begin[c]);
+        int ks = p->tc ? gfk::quad_tc_splits(2 * max_cnf, nr, p->Kp) : gfk::quad_gemm_splits(max_cnf, g_n, nr);
+        const int64_t per_split = (int64_t)max_cnf * nr;
+        while (ks > 1 && ks * per_split * (int64_t)sizeof(cd) > (int64_t(512) << 20)) ks--;
+        p->ksplit = ks;
+        if (ks > 1) st = dalloc(ctx, &p->d_ksum, (size_t)(ks * per_split));
+    }
     if (!st) st = h2d(ctx, p->d_lp, p->lp.data(), p->lp.size());
     if (!st) st = h2d(ctx, p->d_media, p->media.data(), p->media.size());
     if (!st) st = h2d(ctx, p->d_fd, p->fd.data(), p->fd.size());
@@ -556,6 +569,7 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
     for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
         if (p->chunk_begin[c + 1] > p->chunk_begin[c]) nchunks++;
     p->launches_per_exec = p->nf > 0 ? (p->tc ? 3 + 3 * nchunks : 2 + 2 * nchunks + (p->shared ? 1 : 0)) : 0;
+    if (p->nf > 0 && p->ksplit > 1) p->launches_per_exec += nchunks;
     if (p->fused) p->prop_variant = 0;  // one launch shape; nothing to tune
     *out = p;
     return GFK_OK;
@@ -661,12 +675,14 @@ int plan_enqueue(gfk_plan* p, bool timed) {
         if (p->tc) {
             gfk::launch_slice_rem(s, p->d_rem, p->g_n, p->Kp, p->Mp, cnf, p->d_rowmax, p->d_rowexp, p->d_A);
             if (gfk::launch_quad_tc(s, p->d_A, p->d_B, 2 * cnf, p->nr, p->Mp, p->Np, p->Kp, p->d_rowexp, p->col_exp,
-                                    p->d_C + fb, p->d_ranges, dk, p->d_G + (size_t)fb * p->nr, p->d_status + fb))
+                                    p->d_C + fb, p->d_ranges, dk, p->d_G + (size_t)fb * p->nr, p->d_status + fb,
+                                    p->ksplit, p->d_ksum))
                 return fail(ctx, GFK_ECUDA, "tensor-core quadrature launch setup failed");
-            ctx->launches += 1;
+            ctx->launches += 1 + (p->ksplit > 1 ? 1 : 0);
         } else if (p->shared) {
             gfk::launch_quad_gemm(s, p->d_rem, p->d_W, p->d_C + fb, p->d_ranges, cnf, p->g_n, p->nr, dk,
-                                  p->d_G + (size_t)fb * p->nr);
+                                  p->d_G + (size_t)fb * p->nr, p->ksplit, p->d_ksum);
+            ctx->launches += p->ksplit > 1 ? 1 : 0;
         } else {
             gfk::launch_quad_ragged(s, p->d_rem, p->d_C + fb, p->d_ranges, cnf, p->nr, p->d_fd + fb,
                                     p->d_G + (size_t)fb * p->nr);

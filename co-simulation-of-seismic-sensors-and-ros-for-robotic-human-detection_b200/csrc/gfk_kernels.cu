@@ -12,6 +12,8 @@
 //                   (internal/bank/format.go:185-193)
 #include "gfk_kernels.cuh"
 
+#include <algorithm>
+
 namespace gfk {
 
 // ------------------------------------------------------------ constants --
@@ -336,7 +338,8 @@ constexpr int QBM = 64, QBN = 64, QBK = 16;
 
 __global__ __launch_bounds__(256) void k_quad_gemm(const cd* __restrict__ rem, const double* __restrict__ W,
                                                    const cd* __restrict__ C, const double* __restrict__ ranges,
-                                                   int nf, int nk, int nr, double dk, cd* __restrict__ G) {
+                                                   int nf, int nk, int nr, double dk, cd* __restrict__ G,
+                                                   cd* __restrict__ part) {
     __shared__ __align__(16) cd sA[2][QBK][QBM];
     __shared__ __align__(16) double sB[2][QBK][QBN];
     const int tid = threadIdx.x;
@@ -373,13 +376,16 @@ __global__ __launch_bounds__(256) void k_quad_gemm(const cd* __restrict__ rem, c
     for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int b = 0; b < 4; b++) acc[a][b] = mk(0.0);
-    const int ktiles = (nk + QBK - 1) / QBK;
-    load(0);
+    // this block's wavenumber tiles: all of them, or split z of gridDim.z
+    const int ntiles = (nk + QBK - 1) / QBK;
+    const int kt0 = (int)((long long)blockIdx.z * ntiles / gridDim.z);
+    const int kt1 = (int)((long long)(blockIdx.z + 1) * ntiles / gridDim.z);
+    load(kt0);
     store(0);
     __syncthreads();
-    for (int kt = 0; kt < ktiles; kt++) {
-        const int buf = kt & 1;
-        if (kt + 1 < ktiles) load(kt + 1);
+    for (int kt = kt0; kt < kt1; kt++) {
+        const int buf = (kt - kt0) & 1;
+        if (kt + 1 < kt1) load(kt + 1);
 #pragma unroll
         for (int kk = 0; kk < QBK; kk++) {
             cd av[4];
@@ -396,10 +402,24 @@ __global__ __launch_bounds__(256) void k_quad_gemm(const cd* __restrict__ rem, c
                     acc[a][b].im = fma(av[a].im, bv[b], acc[a][b].im);
                 }
         }
-        if (kt + 1 < ktiles) {
+        if (kt + 1 < kt1) {
             store(buf ^ 1);
         }
         __syncthreads();
+    }
+    if (part) {
+        cd* out = part + (size_t)blockIdx.z * nf * nr;
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            const int f = f0 + tf * 4 + a;
+            if (f >= nf) continue;
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                const int j = r0 + tr * 4 + b;
+                if (j < nr) out[(size_t)f * nr + j] = acc[a][b];
+            }
+        }
+        return;
     }
 #pragma unroll
     for (int a = 0; a < 4; a++) {
@@ -416,10 +436,39 @@ __global__ __launch_bounds__(256) void k_quad_gemm(const cd* __restrict__ rem, c
     }
 }
 
+int quad_gemm_splits(int nf, int nk, int nr) {
+    // two blocks per SM of 148; each split keeps at least 8 wavenumber tiles
+    const long long tiles = (long long)((nr + QBN - 1) / QBN) * ((nf + QBM - 1) / QBM);
+    const int ntiles = (nk + QBK - 1) / QBK;
+    if (tiles >= 148 || ntiles < 16) return 1;
+    const int want = (int)((296 + tiles - 1) / tiles);
+    return std::max(1, std::min({want, ntiles / 8, 64}));
+}
+
 void launch_quad_gemm(cudaStream_t s, const cd* rem, const double* W, const cd* C, const double* ranges, int nf,
-                      int nk, int nr, double dk, cd* G) {
-    dim3 grid((nr + QBN - 1) / QBN, (nf + QBM - 1) / QBM);
-    k_quad_gemm<<<grid, 256, 0, s>>>(rem, W, C, ranges, nf, nk, nr, dk, G);
+                      int nk, int nr, double dk, cd* G, int splits, cd* part) {
+    if (splits < 1 || !part) splits = 1;
+    dim3 grid((nr + QBN - 1) / QBN, (nf + QBM - 1) / QBM, splits);
+    k_quad_gemm<<<grid, 256, 0, s>>>(rem, W, C, ranges, nf, nk, nr, dk, G, splits > 1 ? part : nullptr);
+    if (splits > 1) launch_quad_finish(s, part, splits, C, ranges, nf, nr, dk, G);
+}
+
+__global__ void k_quad_finish(const cd* __restrict__ part, int splits, const cd* __restrict__ C,
+                              const double* __restrict__ ranges, int nf, int nr, double dk, cd* __restrict__ G) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)nf * nr) return;
+    const int f = (int)(i / nr), j = (int)(i % nr);
+    cd acc = part[i];
+    for (int z = 1; z < splits; z++) acc = acc + part[(size_t)z * nf * nr + i];
+    const cd c = C[f];
+    G[i] = (c / ranges[j] - (0.5 * dk) * c) + acc;  // fk.go:529-532
+}
+
+void launch_quad_finish(cudaStream_t s, const cd* part, int splits, const cd* C, const double* ranges, int nf,
+                        int nr, double dk, cd* G) {
+    const long long n = (long long)nf * nr;
+    if (n <= 0) return;
+    k_quad_finish<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(part, splits, C, ranges, nf, nr, dk, G);
 }
 
 // ---------------------------------------------- per-frequency-grid sum --

@@ -33,8 +33,12 @@ void launch_j0_slices(cudaStream_t s, const double* ranges, int nr, int nk, int 
                       int8_t* B);
 void launch_slice_rem(cudaStream_t s, const cd* rem, int nk, int Kp, int Mp, int nf, const unsigned long long* rowmax,
                       int* row_exp, int8_t* A);
+// splits > 1 divides the K blocks among blockIdx.z and writes the head-free
+// partial sums to part [splits][M/2][N]; launch_quad_finish then adds them.
 int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int N, int Mp, int Np, int Kp,
-                   const int* row_exp, int col_exp, const cd* C, const double* ranges, double dk, cd* G, int* status);
+                   const int* row_exp, int col_exp, const cd* C, const double* ranges, double dk, cd* G, int* status,
+                   int splits, cd* part);
+int quad_tc_splits(int M, int N, int Kp);  // split count filling the SMs for one chunk shape
 
 // Shared grid, nr <= fused_max_ranges(): propagator and wavenumber sum in one
 // pass (the integrand stays on chip); partial holds nf x ceil(nk/128) x nr.
@@ -47,8 +51,15 @@ void launch_prop_fused(cudaStream_t s, const LayerC* lc, const MediumP* media, c
 void launch_j0_table(cudaStream_t s, const double* ranges, int nr, int nk, double dk, double* W);
 
 // G[f][j] = C_f/r_j - dk C_f/2 + sum_i rem[f][i] W[i][j]; rem is [nf][nk].
+// splits > 1: the wavenumber tiles are divided among blockIdx.z, partial sums
+// go to part [splits][nf][nr] and launch_quad_finish completes G.
 void launch_quad_gemm(cudaStream_t s, const cd* rem, const double* W, const cd* C, const double* ranges,
-                      int nf, int nk, int nr, double dk, cd* G);
+                      int nf, int nk, int nr, double dk, cd* G, int splits, cd* part);
+int quad_gemm_splits(int nf, int nk, int nr);
+
+// G[f][j] = C_f/r_j - dk C_f/2 + sum_z part[z][f][j], z in order (deterministic).
+void launch_quad_finish(cudaStream_t s, const cd* part, int splits, const cd* C, const double* ranges, int nf,
+                        int nr, double dk, cd* G);
 
 // Per-frequency grids: the same sum with J0 evaluated in the loop.
 void launch_quad_ragged(cudaStream_t s, const cd* rem, const cd* C, const double* ranges, int nf, int nr,

@@ -27,6 +27,8 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
+
 #include "gfk_kernels.cuh"
 #include "gfk_tc.cuh"
 
@@ -68,6 +70,7 @@ struct Args {
     double dk;
     cd* G;              // [nf][N]
     int* status;        // [nf] status bits
+    cd* part;           // split partial sums [gridDim.z][M/2][N], or null (one split)
 };
 
 __global__ void __launch_bounds__(THREADS, 1)
@@ -82,7 +85,10 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    const int nkb = a.Kp / BK;
+    // this CTA's K blocks [kb0, kb0 + nkb): all of them, or split z of gridDim.z
+    const int nkb_all = a.Kp / BK;
+    const int kb0 = (int)((long long)blockIdx.z * nkb_all / gridDim.z);
+    const int nkb = (int)((long long)(blockIdx.z + 1) * nkb_all / gridDim.z) - kb0;
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < STAGES; i++) {
@@ -119,10 +125,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                 mbar_expect_tx(&full[st], STAGE_BYTES);
                 uint8_t* base = smem + st * STAGE_BYTES;
 #pragma unroll
-                for (int s = 0; s < S; s++) tma_load_2d(base + s * TILE, &tmA, &full[st], kb * BK, s * a.Mp + m0);
+                for (int s = 0; s < S; s++)
+                    tma_load_2d(base + s * TILE, &tmA, &full[st], (kb0 + kb) * BK, s * a.Mp + m0);
 #pragma unroll
                 for (int t = 0; t < S; t++)
-                    tma_load_2d(base + (S + t) * TILE, &tmB, &full[st], kb * BK, t * a.Np + n0);
+                    tma_load_2d(base + (S + t) * TILE, &tmB, &full[st], (kb0 + kb) * BK, t * a.Np + n0);
                 issued = kb + 1;
             }
             // drain: the last loads of each stage land before the CTA may exit
@@ -175,6 +182,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             c = a.C[f];
         }
         const double cpart = part ? c.im : c.re;
+        cd* const dst = a.part ? a.part + (size_t)blockIdx.z * (a.M >> 1) * a.N : a.G;
 #pragma unroll 1
         for (int j = 0; j < BN / 32; j++) {
             uint32_t v0[32], v1[32], v2[32], v3[32];
@@ -191,9 +199,13 @@ __global__ void __launch_bounds__(THREADS, 1)
                     if (n < a.N) {
                         const double acc = (double)(int)v0[cc] * 0x1p-14 + (double)(int)v1[cc] * 0x1p-21 +
                                            (double)(int)v2[cc] * 0x1p-28 + (double)(int)v3[cc] * 0x1p-35;
-                        const double head = cpart / a.ranges[n] - (0.5 * a.dk) * cpart;  // fk.go:529-532
-                        double* out = reinterpret_cast<double*>(a.G + (size_t)f * a.N + n);
-                        out[part] = head + acc * rscale;
+                        double* out = reinterpret_cast<double*>(dst + (size_t)f * a.N + n);
+                        if (a.part) {
+                            out[part] = acc * rscale;
+                        } else {
+                            const double head = cpart / a.ranges[n] - (0.5 * a.dk) * cpart;  // fk.go:529-532
+                            out[part] = head + acc * rscale;
+                        }
                     }
                 }
             }
@@ -329,9 +341,21 @@ void launch_slice_rem(cudaStream_t s, const cd* rem, int nk, int Kp, int Mp, int
     tc::k_slice_rem<<<grid, 128, 0, s>>>(rem, nk, Kp, Mp, nf, rowmax, row_exp, A);
 }
 
+int quad_tc_splits(int M, int N, int Kp) {
+    // one CTA per SM (its shared memory); each split keeps at least 4 K blocks
+    const long long tiles = (long long)((M + tc::BM - 1) / tc::BM) * ((N + tc::BN - 1) / tc::BN);
+    const int nkb = Kp / tc::BK;
+    if (tiles >= 74 || nkb < 8) return 1;
+    const int want = (int)((148 + tiles - 1) / tiles);
+    return std::max(1, std::min({want, nkb / 4, 32}));
+}
+
 int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int N, int Mp, int Np, int Kp,
-                   const int* row_exp, int col_exp, const cd* C, const double* ranges, double dk, cd* G, int* status) {
+                   const int* row_exp, int col_exp, const cd* C, const double* ranges, double dk, cd* G, int* status,
+                   int splits, cd* part) {
     if (Mp % tc::BM || Np % tc::BN || Kp % tc::BK || M > Mp || N > Np) return 1;
+    if (splits < 1 || !part) splits = 1;
+    if (splits > Kp / tc::BK) return 1;
     CUtensorMap ta, tb;
     if (!make_map(&ta, A, tc::S * Mp, Kp) || !make_map(&tb, B, tc::S * Np, Kp)) return 2;
     static bool attr_set = false;
@@ -341,9 +365,10 @@ int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int 
             return 3;
         attr_set = true;
     }
-    tc::Args a{M, N, Mp, Np, Kp, row_exp, col_exp, C, ranges, dk, G, status};
-    dim3 grid(Np / tc::BN, Mp / tc::BM);
+    tc::Args a{M, N, Mp, Np, Kp, row_exp, col_exp, C, ranges, dk, G, status, splits > 1 ? part : nullptr};
+    dim3 grid(Np / tc::BN, Mp / tc::BM, splits);
     tc::k_quad_tc<<<grid, tc::THREADS, tc::SMEM_BYTES, s>>>(ta, tb, a);
+    if (splits > 1) launch_quad_finish(s, part, splits, C, ranges, M >> 1, N, dk, G);
     return 0;
 }
 

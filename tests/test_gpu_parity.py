@@ -319,6 +319,31 @@ def test_batch_of_uneven_soils_matches_single_plans(gfk, engine, oracle):
         b.close()
 
 
+@pytest.mark.parametrize("quad", ["plain", "split"])
+def test_split_k_sum_matches_one_pass(gfk, engine, quad):
+    """A bank too small to fill the SMs (512 x 64 cells) divides the
+    wavenumber sum among blocks and adds the partial sums in a fixed order;
+    the same soil inside a large batch takes the one-pass sum. Both must agree
+    to rounding, and the split result must be bit-reproducible."""
+    wl = gfk.workloads.single_soil()
+    q = gfk.PLAIN_FP64 if quad == "plain" else gfk.SPLIT_INT8
+    m = wl.medium(gfk.DUNKIN, engine=engine, quadrature=q)
+    a, sa = m.bank_spectra(wl.ranges, wl.freqs, wl.integration())
+    a2, _ = m.bank_spectra(wl.ranges, wl.freqs, wl.integration())
+    assert (sa == 0).all()
+    assert np.array_equal(a, a2)
+    copies = 24
+    b = gfk.Batch([m] * copies, [wl.freqs] * copies, wl.ranges, wl.integration(), engine=engine)
+    b.execute()
+    got, st = b.download()
+    assert (st == 0).all()
+    parts = b.split(got)
+    b.close()
+    per_bin = np.linalg.norm(parts[copies - 1] - a, axis=1) / np.linalg.norm(a, axis=1)
+    assert per_bin.max() < 1e-11, per_bin.max()
+    assert np.array_equal(parts[0], parts[copies - 1])
+
+
 def test_graph_execute_matches_stream_execute(gfk, engine):
     wl = gfk.workloads.single_soil()
     m = wl.medium(gfk.DUNKIN, engine=engine, quadrature=gfk.SPLIT_INT8)
