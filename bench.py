@@ -154,6 +154,39 @@ def fp64_gemm_peak(torch):
     return 2 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def propagated_layers(stack, freqs, omega_imag, k, ref_freq=30.0, default_q=0.0):
+    """Mean number of finite layers the Dunkin solve propagates per
+    (frequency, wavenumber) once it starts at the shallowest layer thick enough
+    to isolate the ones beneath (start_layer in csrc/gfk_solver.cuh: both
+    Re(1 - c^2/v^2) (k h)^2 above 32^2), evaluated on the given sample grid.
+    The propagator's algorithmic count assumes every finite layer."""
+    wc2 = (2 * np.pi * np.asarray(freqs) - 1j * omega_imag) ** 2
+    c2 = wc2[:, None] / (np.asarray(k) ** 2)[None, :]
+    fin = stack[:-1]
+    top = np.full(c2.shape, len(fin), dtype=np.int64)
+    open_ = np.ones(c2.shape, dtype=bool)
+
+    def velocity(v, q, f):  # the Kjartansson velocity at the complex frequency (fk.go:96-110)
+        if q <= 0:
+            return np.full(f.shape, v, dtype=np.complex128)
+        gam = np.arctan(1.0 / q) / np.pi
+        z = (omega_imag + 2j * np.pi * f) / (2 * np.pi * ref_freq)
+        return v * np.cos(np.pi * gam / 2) * np.exp(gam * np.log(z))
+
+    f = np.asarray(freqs, dtype=np.float64)
+    for i, lay in enumerate(fin):
+        q = lay.qs if lay.qs > 0 else (default_q if default_q > 0 else 30.0)
+        qp = lay.qp if lay.qp > 0 else 2.25 * q
+        a, b = velocity(lay.vp, qp, f), velocity(lay.vs, q, f)
+        pa = 1.0 - np.real(c2 / (a * a)[:, None])
+        pb = 1.0 - np.real(c2 / (b * b)[:, None])
+        zeta = np.asarray(k)[None, :] * lay.thickness
+        thick = open_ & (np.minimum(pa, pb) * zeta * zeta > 32.0 ** 2)
+        top[thick] = i
+        open_ &= ~thick
+    return float(top.mean())
+
+
 def cpu_baseline(gfk, wl, threads, target_s=15.0):
     """The oracle's restatement of the reference algorithm (reference-direct:
     Qp = 2.25 Qs, real frequency, guard) on a bounded sample of the workload:
@@ -667,12 +700,21 @@ def main():
         dom, ach = ("k_quad_gemm (FP64 wavenumber sum)" if quad == gfk.PLAIN_FP64 else
                     "k_quad_tc (tensor-core wavenumber sum)"), f_quad / (quad_ms * 1e-3) / 1e12
     roof_time = (f_prop + f_quad) / (fp64_peak * 1e12)
+    kgrid = np.arange(1, wl.samples + 1) * (wl.kmax / wl.samples)
+    l_exec = propagated_layers(wl.stack, wl.freqs[::8], wl.omega_imag, kgrid[::8])
+    f_exec = len(f) * wl.samples * (700 * l_exec + 300)
     roofline = {"bound": "fp64", "kernel": dom, "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": ach / fp64_peak, "traffic": None,
                 "peak_source": "measured here: cuBLAS FP64 GEMM 8192^3 best of 5 (MEASURED_PEAKS.json has no FP64 "
                                "figure)",
                 "algorithmic_flops": {"propagator": f_prop, "quadrature": f_quad},
                 "step_frac_of_fp64_roofline": roof_time / (step_ms * 1e-3),
+                "propagator_executed": {
+                    "note": "the solve starts at the shallowest layer whose own decay isolates the ones beneath "
+                            "(thick-layer start); the algorithmic count above assumes every finite layer",
+                    "mean_layers_propagated": l_exec, "finite_layers": lfin, "flops": f_exec,
+                    "tflops": f_exec / (prop_ms * 1e-3) / 1e12,
+                    "frac": f_exec / (prop_ms * 1e-3) / 1e12 / fp64_peak},
                 "kernel_ms": {"propagator": prop_ms, "quadrature": quad_ms, "other": other_ms},
                 "propagator_launch_shape": {"chosen": variant, "tuning_ms": tune_ms},
                 "quadrature": {"path": "split int8 slices on tcgen05 (10 slice GEMMs)" if quad == gfk.SPLIT_INT8
