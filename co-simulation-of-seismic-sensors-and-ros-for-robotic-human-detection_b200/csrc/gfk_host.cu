@@ -642,7 +642,8 @@ int plan_enqueue(gfk_plan* p, bool timed) {
     size_t seg = 0;
     GFK_CUDA(ctx, cudaMemsetAsync(p->d_status, 0, sizeof(int) * nf, s));
     if (timed && (st = begin_seg(p, 2, &seg))) return st;
-    gfk::launch_layer_consts(s, p->d_lp, p->d_media, p->d_fd, nf, p->solve.omega_imag, form, p->d_lc, p->d_wc2);
+    gfk::launch_layer_consts_fl(s, p->d_lp, p->d_media, p->d_fd, nf, p->max_nl, p->solve.omega_imag, form, p->d_lc,
+                                p->d_wc2);
     gfk::launch_static(s, p->d_lc, p->d_media, p->d_fd, p->d_wc2, nf, form, p->d_C, p->d_status);
     if (p->tc)
         gfk::launch_j0_slices(s, p->d_ranges, p->nr, p->g_n, p->Kp, p->Np, p->g_kmax / p->g_n, p->col_exp, p->d_B);

@@ -18,6 +18,34 @@ namespace gfk {
 
 // ------------------------------------------------------------ constants --
 
+// One layer's constants at one frequency.
+__device__ __forceinline__ LayerC layer_const(const MediumP& med, const LayerP& L, double fr, double wi,
+                                              int formulation) {
+    const double q = q_of(med, L);
+    LayerC out;
+    if (formulation == 0) {
+        // Medium.propsOf (fk.go:119-128): Qp = 2.25 Qs, real frequency
+        const cd a = complex_velocity(med, L.vp, 2.25 * q, fr, 0.0);
+        const cd b = complex_velocity(med, L.vs, q, fr, 0.0);
+        out.c[0] = a;
+        out.c[1] = b;
+        out.c[2] = (L.rho * b) * b;
+        out.c[3] = mk(L.rho);
+    } else {
+        const double qp = L.qp > 0 ? L.qp : 2.25 * q;
+        const cd a = complex_velocity(med, L.vp, qp, fr, wi);
+        const cd b = complex_velocity(med, L.vs, q, fr, wi);
+        const cd a2 = a * a, b2 = b * b;
+        out.c[0] = 1.0 / a2;
+        out.c[1] = 1.0 / b2;
+        out.c[2] = b2 / a2;
+        out.c[3] = (L.rho * b2) / med.mu_ref;
+    }
+    out.h = L.h;
+    out.pad = 0.0;
+    return out;
+}
+
 __global__ void k_layer_consts(const LayerP* __restrict__ lp, const MediumP* __restrict__ media,
                                const FreqDesc* __restrict__ fd, int nf, double wi, int formulation,
                                LayerC* __restrict__ lc, cd* __restrict__ wc2) {
@@ -26,32 +54,7 @@ __global__ void k_layer_consts(const LayerP* __restrict__ lp, const MediumP* __r
     const FreqDesc d = fd[f];
     const MediumP med = media[d.soil];
     const double fr = d.freq;
-    for (int l = 0; l < med.count; l++) {
-        const LayerP L = lp[med.lp_off + l];
-        const double q = q_of(med, L);
-        LayerC out;
-        if (formulation == 0) {
-            // Medium.propsOf (fk.go:119-128): Qp = 2.25 Qs, real frequency
-            const cd a = complex_velocity(med, L.vp, 2.25 * q, fr, 0.0);
-            const cd b = complex_velocity(med, L.vs, q, fr, 0.0);
-            out.c[0] = a;
-            out.c[1] = b;
-            out.c[2] = (L.rho * b) * b;
-            out.c[3] = mk(L.rho);
-        } else {
-            const double qp = L.qp > 0 ? L.qp : 2.25 * q;
-            const cd a = complex_velocity(med, L.vp, qp, fr, wi);
-            const cd b = complex_velocity(med, L.vs, q, fr, wi);
-            const cd a2 = a * a, b2 = b * b;
-            out.c[0] = 1.0 / a2;
-            out.c[1] = 1.0 / b2;
-            out.c[2] = b2 / a2;
-            out.c[3] = (L.rho * b2) / med.mu_ref;
-        }
-        out.h = L.h;
-        out.pad = 0.0;
-        lc[d.lc_off + l] = out;
-    }
+    for (int l = 0; l < med.count; l++) lc[d.lc_off + l] = layer_const(med, lp[med.lp_off + l], fr, wi, formulation);
     const cd wc = mk(kTwoPi * fr, -wi);
     wc2[f] = wc * wc;
 }
@@ -60,6 +63,31 @@ void launch_layer_consts(cudaStream_t s, const LayerP* lp, const MediumP* media,
                          double wi, int formulation, LayerC* lc, cd* wc2) {
     if (nf <= 0) return;
     k_layer_consts<<<(nf + 127) / 128, 128, 0, s>>>(lp, media, fd, nf, wi, formulation, lc, wc2);
+}
+
+// The same constants with one thread per (frequency, layer): a few hundred
+// frequencies of a thin stack otherwise leave most SMs idle while each thread
+// walks its layers' transcendental functions in sequence.
+__global__ void k_layer_consts_fl(const LayerP* __restrict__ lp, const MediumP* __restrict__ media,
+                                  const FreqDesc* __restrict__ fd, int nf, double wi, int formulation,
+                                  LayerC* __restrict__ lc, cd* __restrict__ wc2) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const int l = blockIdx.y;
+    if (f >= nf) return;
+    const FreqDesc d = fd[f];
+    const MediumP med = media[d.soil];
+    if (l < med.count) lc[d.lc_off + l] = layer_const(med, lp[med.lp_off + l], d.freq, wi, formulation);
+    if (l == 0) {
+        const cd wc = mk(kTwoPi * d.freq, -wi);
+        wc2[f] = wc * wc;
+    }
+}
+
+void launch_layer_consts_fl(cudaStream_t s, const LayerP* lp, const MediumP* media, const FreqDesc* fd, int nf,
+                            int max_layers, double wi, int formulation, LayerC* lc, cd* wc2) {
+    if (nf <= 0 || max_layers <= 0) return;
+    dim3 grid((nf + 63) / 64, max_layers);
+    k_layer_consts_fl<<<grid, 64, 0, s>>>(lp, media, fd, nf, wi, formulation, lc, wc2);
 }
 
 __device__ __forceinline__ bool finite_cd(cd a) { return isfinite(a.re) && isfinite(a.im); }

@@ -14,6 +14,9 @@ enum : int { kStSingular = 1, kStNonfinite = 2, kStTimeout = 4 };
 // lc[fd[f].lc_off + l] for every layer of the row's medium, and wc2[f].
 void launch_layer_consts(cudaStream_t s, const LayerP* lp, const MediumP* media, const FreqDesc* fd, int nf,
                          double wi, int formulation, LayerC* lc, cd* wc2);
+// One thread per (frequency, layer); max_layers >= every medium's count.
+void launch_layer_consts_fl(cudaStream_t s, const LayerP* lp, const MediumP* media, const FreqDesc* fd, int nf,
+                            int max_layers, double wi, int formulation, LayerC* lc, cd* wc2);
 
 void launch_static(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2, int nf,
                    int formulation, cd* C, int* status);
