@@ -174,12 +174,20 @@ __global__ void __launch_bounds__(THREADS, 2)
             bias_s[threadIdx.x - 64] = a.bias[n0 + threadIdx.x - 64];
             asm volatile("bar.sync 1, 128;" ::: "memory");
         }
-        const bool ok = mbar_wait(accf, 0);
-        if (!ok) *(volatile int*)abort_flag = 1;  // the tile stays unwritten: no stores below
-        tc_fence_after();
         const int q = warp & 3;
         const int rl = q * 32 + lane;
         const int row = m0 + rl;
+        // backward-data: this row's pre-activations, one 32-column chunk ahead
+        // (the first chunk is in flight while the MMAs run)
+        uint4 zcur[4], znext[4];
+        if (MODE == kBwdData) {
+            const uint4* zs = reinterpret_cast<const uint4*>(a.zin + (size_t)row * a.N + n0);
+#pragma unroll
+            for (int c = 0; c < 4; c++) zcur[c] = zs[c];
+        }
+        const bool ok = mbar_wait(accf, 0);
+        if (!ok) *(volatile int*)abort_flag = 1;  // the tile stays unwritten: no stores below
+        tc_fence_after();
         const bool row_ok = ok && !*(volatile int*)abort_flag;
         bf16* tileO = reinterpret_cast<bf16*>(smem);
         bf16* tileZ = tileO + BM * kTileLd;
@@ -187,6 +195,11 @@ __global__ void __launch_bounds__(THREADS, 2)
         for (int j = 0; j < BN / 32; j++) {
             uint32_t v[32];
             tmem_ld32(tmem + (static_cast<uint32_t>(q * 32) << 16) + j * 32, v);
+            if (MODE == kBwdData && j + 1 < BN / 32) {
+                const uint4* zs = reinterpret_cast<const uint4*>(a.zin + (size_t)row * a.N + n0 + (j + 1) * 32);
+#pragma unroll
+                for (int c = 0; c < 4; c++) znext[c] = zs[c];
+            }
             tmem_wait_ld();
             if (!row_ok) continue;
             const int nb = n0 + j * 32;
@@ -214,15 +227,16 @@ __global__ void __launch_bounds__(THREADS, 2)
                                            pack2(zv[8 * c + 4], zv[8 * c + 5]), pack2(zv[8 * c + 6], zv[8 * c + 7]));
                 }
             } else {  // kBwdData
-                const uint4* zs = reinterpret_cast<const uint4*>(a.zin + (size_t)row * a.N + nb);
                 float zv[32];
 #pragma unroll
-                for (int c = 0; c < 4; c++) unpack8(zs[c], zv + 8 * c);
+                for (int c = 0; c < 4; c++) unpack8(zcur[c], zv + 8 * c);
 #pragma unroll
                 for (int c = 0; c < 32; c++) {
                     const float sg = sigmoid_(zv[c]);
                     y[c] = __uint_as_float(v[c]) * (sg * (1.0f + zv[c] * (1.0f - sg)));
                 }
+#pragma unroll
+                for (int c = 0; c < 4; c++) zcur[c] = znext[c];
             }
             uint4* od = reinterpret_cast<uint4*>(tileO + rl * kTileLd + j * 32);
 #pragma unroll
@@ -340,16 +354,19 @@ __global__ void k_step_begin(TrainScalars* ts) {
     ts->bc2 = static_cast<float>(1.0 - pow(static_cast<double>(ts->beta2), static_cast<double>(t)));
 }
 
-// 32 samples per block: one thread per sample draws the cell and builds its
-// scalars and targets, then one thread per feature fills the 32 rows.
+// kBatchRows samples per block: one thread per sample draws the cell and builds
+// its scalars and targets, then one thread per feature fills the rows. Small
+// blocks keep many of them resident, so the dependent gathers (soil, cell,
+// label) of different blocks overlap.
+constexpr int kBatchRows = 16;
 __global__ void __launch_bounds__(kIn) k_batch(BatchArgs a) {
-    __shared__ bf16 tile[32][kIn + 2];
-    __shared__ PointScalars ps[32];
-    __shared__ int soil_of[32];
+    __shared__ bf16 tile[kBatchRows][kIn + 2];
+    __shared__ PointScalars ps[kBatchRows];
+    __shared__ int soil_of[kBatchRows];
     const long long t = a.ts->step;
-    const int b0 = blockIdx.x * 32;
+    const int b0 = blockIdx.x * kBatchRows;
     const int j = threadIdx.x;
-    if (j < 32) {
+    if (j < kBatchRows) {
         const int b = b0 + j;
         const unsigned long long h = mix64(a.seed ^ mix64(static_cast<unsigned long long>(t) * a.B + b));
         const int soil = a.train[pick(h, a.ntrain)];
@@ -377,14 +394,14 @@ __global__ void __launch_bounds__(kIn) k_batch(BatchArgs a) {
         a.C[2 * b + 1] = c1;
     }
     __syncthreads();
-    for (int i = 0; i < 32; i++)
+    for (int i = 0; i < kBatchRows; i++)
         tile[i][j] = __float2bfloat16_rn(feature(j, a.soilfeat + (size_t)soil_of[i] * kSoilStride, ps[i], a.fourier));
     __syncthreads();
-    for (int i = 0; i < 32; i++) a.X[(size_t)(b0 + i) * kIn + j] = tile[i][j];
-    // X^T: thread j writes its feature's 32 consecutive samples (64 bytes)
-    uint32_t w[16];
+    for (int i = 0; i < kBatchRows; i++) a.X[(size_t)(b0 + i) * kIn + j] = tile[i][j];
+    // X^T: thread j writes its feature's kBatchRows consecutive samples
+    uint32_t w[kBatchRows / 2];
 #pragma unroll
-    for (int i = 0; i < 16; i++) {
+    for (int i = 0; i < kBatchRows / 2; i++) {
         __nv_bfloat162 v;
         v.x = tile[2 * i][j];
         v.y = tile[2 * i + 1][j];
@@ -392,7 +409,7 @@ __global__ void __launch_bounds__(kIn) k_batch(BatchArgs a) {
     }
     uint4* d = reinterpret_cast<uint4*>(a.XT + (size_t)j * a.B + b0);
 #pragma unroll
-    for (int i = 0; i < 4; i++) d[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+    for (int i = 0; i < kBatchRows / 8; i++) d[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
 }
 
 // ------------------------------------------------------------------ head --
@@ -544,9 +561,28 @@ __global__ void __launch_bounds__(256) k_bias_grad(BiasPtrs d, int B, float* gb)
 
 // Grids are (blocks over the largest segment, segments): a block works inside
 // one segment, whose descriptor it reads from device memory.
+// The partials are loaded 32 or 8 at a time before they are added (in the same
+// order as one at a time), so a thread has that many loads in flight instead of
+// one dependent load per partial (the head's segment sums 256 partials).
 __device__ __forceinline__ float seg_grad(const AdamSeg& g, long long j) {
+    const float* __restrict__ src = g.src + j;
     float grad = 0.0f;
-    for (int q = 0; q < g.nsrc; q++) grad += g.src[q * g.stride + j];
+    int q = 0;
+    for (; q + 32 <= g.nsrc; q += 32) {
+        float t[32];
+#pragma unroll
+        for (int u = 0; u < 32; u++) t[u] = __ldg(src + (long long)(q + u) * g.stride);
+#pragma unroll
+        for (int u = 0; u < 32; u++) grad += t[u];
+    }
+    for (; q + 8 <= g.nsrc; q += 8) {
+        float t[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) t[u] = __ldg(src + (long long)(q + u) * g.stride);
+#pragma unroll
+        for (int u = 0; u < 8; u++) grad += t[u];
+    }
+    for (; q < g.nsrc; q++) grad += __ldg(src + (long long)q * g.stride);
     return grad;
 }
 
@@ -557,14 +593,15 @@ __global__ void k_adam(AdamArgs a) {
     const long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (j >= g.n) return;
     const long long i = g.off + j;
+    const float m0 = a.m[i], v0 = a.v[i];
+    float p = a.p[i];
     const float grad = seg_grad(g, j);
     const TrainScalars* ts = a.ts;
     const float b1 = ts->beta1, b2 = ts->beta2;
-    const float m = b1 * a.m[i] + (1.0f - b1) * grad;
-    const float v = b2 * a.v[i] + (1.0f - b2) * grad * grad;
+    const float m = b1 * m0 + (1.0f - b1) * grad;
+    const float v = b2 * v0 + (1.0f - b2) * grad * grad;
     a.m[i] = m;
     a.v[i] = v;
-    float p = a.p[i];
     p -= ts->lr * ((m / ts->bc1) / (sqrtf(v / ts->bc2) + a.eps) + a.weight_decay * p);
     a.p[i] = p;
     if (g.wb) g.wb[j] = __float2bfloat16_rn(p);
@@ -875,7 +912,7 @@ int launch_gemm(cudaStream_t s, int mode, const bf16* A, const bf16* B, int rows
 
 void launch_step_begin(cudaStream_t s, TrainScalars* ts) { k_step_begin<<<1, 1, 0, s>>>(ts); }
 
-void launch_batch(cudaStream_t s, const BatchArgs& a) { k_batch<<<a.B / 32, kIn, 0, s>>>(a); }
+void launch_batch(cudaStream_t s, const BatchArgs& a) { k_batch<<<a.B / kBatchRows, kIn, 0, s>>>(a); }
 
 void launch_head_train(cudaStream_t s, const bf16* H, const bf16* Z, const float* W6, const float* b6, const float* Y,
                        const float* C, int B, bf16* dZ, bf16* dZT, float* gpart, float* lpart) {

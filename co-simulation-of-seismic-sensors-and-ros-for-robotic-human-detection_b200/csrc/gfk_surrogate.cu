@@ -132,6 +132,11 @@ struct gfk_net {
     std::vector<int> graph_train;
     cudaGraphExec_t gexec = nullptr;
     M::AdamArgs adam{};
+    // weight-gradient GEMMs run on a second stream, each as soon as its dZ^T
+    // exists, beside the backward-data chain (forked and joined by events, so
+    // a captured step holds them as parallel branches)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_dz[kLayers] = {}, ev_join = nullptr;
     // inference
     bf16 *iX = nullptr, *iH0 = nullptr, *iH1 = nullptr;
     float* iT = nullptr;
@@ -155,6 +160,12 @@ void net_free(gfk_net* n) {
     gfk_ctx* c = n->ctx;
     if (n->gexec) cudaGraphExecDestroy(n->gexec);
     n->gexec = nullptr;
+    if (n->side) cudaStreamSynchronize(n->side);
+    for (cudaEvent_t& e : n->ev_dz)
+        if (e) cudaEventDestroy(e);
+    if (n->ev_join) cudaEventDestroy(n->ev_join);
+    if (n->side) cudaStreamDestroy(n->side);
+    n->side = nullptr;
     for (auto& l : n->L) {
         sfree(c, l.wb);
         sfree(c, l.wt);
@@ -192,8 +203,8 @@ int check_status(gfk_net* n) {
 }
 
 int gemm(gfk_net* n, int mode, const bf16* A, const bf16* Bm, int rowsA, int rowsB, int K, int splits,
-         const M::GemmArgs& g) {
-    const int r = M::launch_gemm(n->ctx->stream, mode, A, Bm, rowsA, rowsB, K, splits, g);
+         const M::GemmArgs& g, cudaStream_t on = nullptr) {
+    const int r = M::launch_gemm(on ? on : n->ctx->stream, mode, A, Bm, rowsA, rowsB, K, splits, g);
     if (r) return sfail(n->ctx, r == 1 ? GFK_EARG : GFK_ECUDA, "GEMM launch refused (mode %d, %d x %d x %d): %d",
                         mode, rowsA, rowsB, K, r);
     n->ctx->launches++;
@@ -217,6 +228,16 @@ int enqueue_fwd_bwd(gfk_net* n) {
     M::launch_head_train(s, n->H[kLayers - 1], n->Z[kLayers - 1], n->d_p + n->w6off, n->d_p + n->b6off, n->Y,
                          n->Cw, B, n->dZ[kLayers - 1], n->dZT[kLayers - 1], n->gpart, n->lpart);
     n->ctx->launches++;
+    auto wgrad = [&](int l) -> int {  // on the side stream once dZ^T[l] is written
+        SG_CUDA(n->ctx, cudaEventRecord(n->ev_dz[l], s));
+        SG_CUDA(n->ctx, cudaStreamWaitEvent(n->side, n->ev_dz[l], 0));
+        M::GemmArgs g{};
+        g.part = n->L[l].part;
+        g.status = n->d_status;
+        return gemm(n, M::kWgrad, n->dZT[l], l ? n->HT[l - 1] : n->XT, kW, n->L[l].in, B, n->L[l].splits, g,
+                    n->side);
+    };
+    SG_TRY(wgrad(kLayers - 1));
     for (int l = kLayers - 1; l >= 1; l--) {
         M::GemmArgs g{};
         g.zin = n->Z[l - 1];
@@ -224,13 +245,10 @@ int enqueue_fwd_bwd(gfk_net* n) {
         g.outT = n->dZT[l - 1];
         g.status = n->d_status;
         SG_TRY(gemm(n, M::kBwdData, n->dZ[l], n->L[l].wt, B, n->L[l].in, kW, 1, g));
+        SG_TRY(wgrad(l - 1));
     }
-    for (int l = 0; l < kLayers; l++) {
-        M::GemmArgs g{};
-        g.part = n->L[l].part;
-        g.status = n->d_status;
-        SG_TRY(gemm(n, M::kWgrad, n->dZT[l], l ? n->HT[l - 1] : n->XT, kW, n->L[l].in, B, n->L[l].splits, g));
-    }
+    SG_CUDA(n->ctx, cudaEventRecord(n->ev_join, n->side));
+    SG_CUDA(n->ctx, cudaStreamWaitEvent(s, n->ev_join, 0));
     const bf16* dzt[kLayers];
     for (int l = 0; l < kLayers; l++) dzt[l] = n->dZT[l];
     M::launch_bias_grad(s, dzt, kLayers, B, n->gb);
@@ -630,6 +648,13 @@ int gfk_net_create(gfk_ctx* ctx, const gfk_net_config* cfg, gfk_net** out) {
     A(&n->hist, (size_t)kHistCap * 2);
     A(&n->gflat, n->nparam);
     A(&n->d_status, 1);
+    if (st == GFK_OK && cudaStreamCreateWithFlags(&n->side, cudaStreamNonBlocking) != cudaSuccess)
+        st = sfail(ctx, GFK_ECUDA, "side stream creation failed");
+    for (int l = 0; l < kLayers && st == GFK_OK; l++)
+        if (cudaEventCreateWithFlags(&n->ev_dz[l], cudaEventDisableTiming) != cudaSuccess)
+            st = sfail(ctx, GFK_ECUDA, "event creation failed");
+    if (st == GFK_OK && cudaEventCreateWithFlags(&n->ev_join, cudaEventDisableTiming) != cudaSuccess)
+        st = sfail(ctx, GFK_ECUDA, "event creation failed");
     if (st != GFK_OK) {
         net_free(n);
         delete n;
