@@ -710,12 +710,20 @@ def main():
     else:
         dom, ach = ("k_quad_gemm (FP64 wavenumber sum)" if quad == gfk.PLAIN_FP64 else
                     "k_quad_tc (tensor-core wavenumber sum)"), f_quad / (quad_ms * 1e-3) / 1e12
+    # DRAM bytes of one propagator launch: the ncu capture of the graded soil's
+    # every-8th-frequency case (dram__bytes_read + _write = 0.29 + 11.78 MB for
+    # 256 frequencies), scaled by the frequencies one full launch processes
+    traffic, traffic_src = None, None
+    if args.workload != "single" and args.freq_stride == 1 and prop_ms >= quad_ms:
+        traffic = (0.292352e6 + 11.778048e6) * len(f) / 256
+        traffic_src = ("ncu capture of k_prop on 256 of the 2048 frequencies (profiles/k_prop_dunkin_graded_soil.md),"
+                       " scaled by frequencies; the integrand's 16 B per (f, k) mostly stays in L2")
     roof_time = (f_prop + f_quad) / (fp64_peak * 1e12)
     kgrid = np.arange(1, wl.samples + 1) * (wl.kmax / wl.samples)
     l_exec = propagated_layers(wl.stack, wl.freqs[::8], wl.omega_imag, kgrid[::8])
     f_exec = len(f) * wl.samples * (700 * l_exec + 300)
     roofline = {"bound": "fp64", "kernel": dom, "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": ach / fp64_peak, "traffic": None,
+                "frac": ach / fp64_peak, "traffic": traffic, "traffic_source": traffic_src,
                 "peak_source": "measured here: cuBLAS FP64 GEMM 8192^3 best of 5 (MEASURED_PEAKS.json has no FP64 "
                                "figure)",
                 "algorithmic_flops": {"propagator": f_prop, "quadrature": f_quad},
