@@ -242,13 +242,15 @@ void launch_prop(cudaStream_t s, const LayerC* lc, const MediumP* media, const F
 // ------------------------------------------------- fused propagator + sum --
 //
 // For a handful of ranges the wavenumber sum is a dot product per range: each
-// thread multiplies its integrand value k u - C by the Hankel weights
-// W[k][0..nr), the block reduces over its 128 wavenumbers in shared memory in
-// a fixed order, and one partial per (row, k block, range) is written. The
+// thread accumulates its integrand values k u - C times the Hankel weights
+// W[k][0..nr) over kFuseSweeps wavenumbers, the block reduces over its
+// kFuseSweeps x 128 wavenumbers in a fixed order (warp tree, then warps), and
+// one partial per (row, k block, range) is written. The
 // integrand never reaches HBM; k_fused_finish adds the partials in block
 // order (deterministic) and the closed k = 0 panel (fk.go:529-532).
 
 constexpr int kFuseThreads = 128;
+constexpr int kFuseSweeps = 8;  // a block covers kFuseSweeps x 128 wavenumbers of its row
 
 template <int NR>
 __global__ __launch_bounds__(kFuseThreads, 4) void k_prop_fused(const LayerC* __restrict__ lc,
@@ -266,22 +268,28 @@ __global__ __launch_bounds__(kFuseThreads, 4) void k_prop_fused(const LayerC* __
     for (int l = threadIdx.x; l < nl; l += blockDim.x) s_lc[l] = lc[fdesc.lc_off + l];
     __syncthreads();
     const int n = fdesc.kfar > 0 ? fdesc.nk : 0;
-    const int i = blockIdx.x * kFuseThreads + threadIdx.x + 1;
-    cd r = mk(0.0);
-    if (i <= n) {
+    const cd wc2f = wc2[f], cf = C[f];
+    double acc[2 * NR];
+#pragma unroll
+    for (int q = 0; q < 2 * NR; q++) acc[q] = 0.0;
+    // kFuseSweeps wavenumbers per thread, 128 apart, summed in order: one
+    // layer-table load and one block reduction per 512 wavenumbers
+#pragma unroll 1
+    for (int sweep = 0; sweep < kFuseSweeps; sweep++) {
+        const int i = (blockIdx.x * kFuseSweeps + sweep) * kFuseThreads + threadIdx.x + 1;
+        if (i > n) break;
         const double k = (double)i * fdesc.dk;
-        r = k * dunkin_u(s_lc, nl, wc2[f], k, med.mu_ref) - C[f];
+        cd r = k * dunkin_u(s_lc, nl, wc2f, k, med.mu_ref) - cf;
         if (!finite_cd(r)) {
             atomicOr(status + f, kStNonfinite);
             r = mk(0.0);
         }
-    }
-    double acc[2 * NR];
 #pragma unroll
-    for (int j = 0; j < NR; j++) {
-        const double w = (i <= n && j < nr) ? W[(size_t)(i - 1) * nr + j] : 0.0;
-        acc[2 * j] = r.re * w;
-        acc[2 * j + 1] = r.im * w;
+        for (int j = 0; j < NR; j++) {
+            const double w = j < nr ? W[(size_t)(i - 1) * nr + j] : 0.0;
+            acc[2 * j] = fma(r.re, w, acc[2 * j]);
+            acc[2 * j + 1] = fma(r.im, w, acc[2 * j + 1]);
+        }
     }
     // warp tree, then the block's warps in order: a fixed summation order
 #pragma unroll
@@ -324,7 +332,7 @@ void launch_prop_fused(cudaStream_t s, const LayerC* lc, const MediumP* media, c
                        int nf, int nk, const cd* C, const double* W, const double* ranges, int nr, cd* partial,
                        int* status, cd* G) {
     if (nf <= 0 || nk <= 0 || nr <= 0 || nr > 8) return;
-    const int nkb = (nk + kFuseThreads - 1) / kFuseThreads;
+    const int nkb = (nk + kFuseThreads * kFuseSweeps - 1) / (kFuseThreads * kFuseSweeps);
     dim3 grid(nkb, nf);
     if (nr <= 1)
         k_prop_fused<1><<<grid, kFuseThreads, 0, s>>>(lc, media, fd, wc2, C, W, nr, nkb, partial, status);

@@ -236,12 +236,18 @@ __device__ __forceinline__ void digits4(double x128, int8_t d[4]) {
 
 // Integrand rows: rows 2f (re) and 2f+1 (im) of the A slice planes [4][Mp][Kp].
 // 16 consecutive wavenumbers per thread, one 16-byte store per slice and part.
-__global__ void k_slice_rem(const cd* __restrict__ rem, int nk, int Kp, int Mp, int nf,
-                            const unsigned long long* __restrict__ rowmax, int* __restrict__ row_exp,
-                            int8_t* __restrict__ A) {
+// One block of 128 threads per (row, 2048 wavenumbers): the integrand is read
+// coalesced into shared memory (16-byte units XOR-swizzled within each
+// 16-unit run, so both the row-order stores and each thread's 16-unit reads are
+// free of bank conflicts), then each thread slices 16 consecutive values.
+__global__ void __launch_bounds__(128) k_slice_rem(const cd* __restrict__ rem, int nk, int Kp, int Mp, int nf,
+                                                   const unsigned long long* __restrict__ rowmax,
+                                                   int* __restrict__ row_exp, int8_t* __restrict__ A) {
+    __shared__ cd tile[128 * 16];
     const int f = blockIdx.y;
-    const int k0 = (blockIdx.x * blockDim.x + threadIdx.x) * 16;
-    if (f >= nf || k0 >= Kp) return;
+    const int kb = blockIdx.x * (128 * 16);
+    const int t = threadIdx.x;
+    if (f >= nf) return;  // uniform over the block
     int e[2];
     double sc[2];
 #pragma unroll
@@ -250,32 +256,41 @@ __global__ void k_slice_rem(const cd* __restrict__ rem, int nk, int Kp, int Mp, 
         e[p] = mx > 0 ? ilogb(mx * (128.0 / 127.0)) + 1 : 0;  // 2^e >= mx*128/127
         sc[p] = ldexp(128.0, -e[p]);
     }
-    if (k0 == 0 && threadIdx.x == 0) {
+    if (blockIdx.x == 0 && t == 0) {
         row_exp[2 * f] = e[0];
         row_exp[2 * f + 1] = e[1];
     }
     // a row with no device work (its maximum stayed 0) slices to zeros
     // without reading its integrand slot
     const bool live = rowmax[2 * f] != 0 || rowmax[2 * f + 1] != 0;
+    const cd* src = rem + (size_t)f * nk;
+#pragma unroll 4
+    for (int i = 0; i < 16; i++) {
+        const int el = t + 128 * i, k = kb + el;
+        const int r = el >> 4, c = el & 15;
+        tile[(r << 4) | (c ^ (r & 7))] = (live && k < nk) ? src[k] : mk(0.0);
+    }
+    __syncthreads();
+    const int k0 = kb + 16 * t;
+    if (k0 >= Kp) return;
     alignas(16) int8_t out[2][4][16];
 #pragma unroll 4
     for (int i = 0; i < 16; i++) {
-        const int k = k0 + i;
-        const cd v = (live && k < nk) ? rem[(size_t)f * nk + k] : mk(0.0);
+        const cd v = tile[(t << 4) | (i ^ (t & 7))];
         int8_t d[4];
         digits4(v.re * sc[0], d);
 #pragma unroll
-        for (int s = 0; s < 4; s++) out[0][s][i] = d[s];
+        for (int q = 0; q < 4; q++) out[0][q][i] = d[q];
         digits4(v.im * sc[1], d);
 #pragma unroll
-        for (int s = 0; s < 4; s++) out[1][s][i] = d[s];
+        for (int q = 0; q < 4; q++) out[1][q][i] = d[q];
     }
 #pragma unroll
     for (int p = 0; p < 2; p++)
 #pragma unroll
-        for (int s = 0; s < 4; s++)
-            *reinterpret_cast<int4*>(A + ((size_t)s * Mp + 2 * f + p) * Kp + k0) =
-                *reinterpret_cast<const int4*>(out[p][s]);
+        for (int q = 0; q < 4; q++)
+            *reinterpret_cast<int4*>(A + ((size_t)q * Mp + 2 * f + p) * Kp + k0) =
+                *reinterpret_cast<const int4*>(out[p][q]);
 }
 
 // Hankel weights w_i J0(k_i r_j) dk (fk.go:540-546), transposed to [range][k]

@@ -57,6 +57,24 @@ def test_surface_response_matches_oracle_pointwise(gfk, engine, oracle):
     assert np.max(np.abs(got - want) / np.abs(want)) < 1e-11
 
 
+def test_thick_layer_start_matches_full_propagation(gfk, engine, oracle):
+    """The solve starts at the shallowest layer thick enough to isolate the
+    layers beneath it; the oracle propagates every layer. Uneven seeded soils
+    (2-12 layers, 0.2-5 m) put the start at every depth across the k range."""
+    soils, _, _, kmax = gfk.workloads.batched_soils(count=8, seed=3)
+    rng = np.random.default_rng(11)
+    worst = 0.0
+    for st, _ in soils:
+        tup = as_tuples(st)
+        k = rng.uniform(0.01, kmax, 150)
+        f = rng.uniform(1.0, 500.0, 150)
+        m = medium_of(gfk, tup, formulation=1, omega_imag=1.5, engine=engine)
+        got = m.surface_response(k, f)
+        want = np.array([oracle.surface_response(tup, ki, fi, 1, 1.5) for ki, fi in zip(k, f)])
+        worst = max(worst, float(np.max(np.abs(got - want) / np.abs(want))))
+    assert worst < 1e-11, worst
+
+
 def test_reference_mode_per_frequency_grid(gfk, engine, oracle):
     """VerticalDisplacementMulti with the reference's own GridFor grids (the
     ragged path), soft_over_stiff and loam, against the oracle."""
