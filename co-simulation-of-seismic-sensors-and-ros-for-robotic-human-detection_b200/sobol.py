@@ -335,30 +335,44 @@ def metrics_device(engine, d_G, stride, ns, setup):
 def solve_metrics(params, setup, engine, batch_soils=20000, nk=NK, kmax=KMAX, formulation=N.DUNKIN):
     """(peak, centroid) of every parameter row through the GPU f-k solve and
     the GPU trace metrics; the banks never leave the device. Returns
-    (peak, centroid, GPU solver seconds)."""
+    (peak, centroid, GPU solver seconds). The host tables of the next group's
+    plan are built while the previous group executes on the device."""
     freqs = setup.freqs()
     opt = Integration(nk, 0.0, kmax)
     peak = np.zeros(len(params))
     cen = np.zeros(len(params))
     gpu_s = 0.0
-    for b0 in range(0, len(params), batch_soils):
-        chunk = params[b0:b0 + batch_soils]
-        lay, cnt = layer_table(chunk)
-        plan = Batch.from_layers(lay, cnt, freqs, [setup.r], opt, (formulation, N.PLAIN_FP64, setup.omega_imag),
-                                 engine=engine)
-        try:
-            plan.execute()
-            status = plan.statuses()
-            if (status != 0).any():
-                bad = int(np.nonzero(status)[0][0])
-                raise RuntimeError(f"soil {b0 + bad // len(freqs)}: status {N.STATUS_NAMES[int(status[bad])]}")
-            a, b, c = plan.kernel_times()
-            gpu_s += (a + b + c) * 1e-3
-            pk, ce = metrics_device(engine, plan.result_device_ptr(), len(freqs), len(chunk), setup)
-        finally:
+
+    def build(b0):
+        lay, cnt = layer_table(params[b0:b0 + batch_soils])
+        return b0, Batch.from_layers(lay, cnt, freqs, [setup.r], opt, (formulation, N.PLAIN_FP64, setup.omega_imag),
+                                     engine=engine)
+
+    def finish(b0, plan):
+        nonlocal gpu_s
+        ns = len(params[b0:b0 + batch_soils])
+        status = plan.statuses()
+        if (status != 0).any():
+            bad = int(np.nonzero(status)[0][0])
+            raise RuntimeError(f"soil {b0 + bad // len(freqs)}: status {N.STATUS_NAMES[int(status[bad])]}")
+        a, b, c = plan.kernel_times()
+        gpu_s += (a + b + c) * 1e-3
+        peak[b0:b0 + ns], cen[b0:b0 + ns] = metrics_device(engine, plan.result_device_ptr(), len(freqs), ns, setup)
+
+    pending = []
+    try:
+        for b0 in range(0, len(params), batch_soils):
+            pending.append(build(b0))
+            if len(pending) == 2:
+                finish(*pending[0])
+                pending.pop(0)[1].close()
+            pending[-1][1].execute()
+        while pending:
+            finish(*pending[0])
+            pending.pop(0)[1].close()
+    finally:
+        for _, plan in pending:
             plan.close()
-        peak[b0:b0 + len(chunk)] = pk
-        cen[b0:b0 + len(chunk)] = ce
     return peak, cen, gpu_s
 
 
