@@ -439,24 +439,40 @@ def spread(values):
 
 
 def _solve_rows(params, bins_per_soil, setup, engine, batch_soils, nk=NK, kmax=KMAX, formulation=N.DUNKIN):
-    """Yields (plan, soil indices, bin lists) for the listed rows of each
-    soil: one batch plan per group of soils, each soil with its own bins."""
+    """Yields (plan, soil indices) for the listed rows of each soil: one batch
+    plan per group of soils, each soil with its own bins. The next group's
+    plan is built while the previous one executes."""
     freqs = setup.freqs()
     opt = Integration(nk, 0.0, kmax)
     soils = [i for i, b in enumerate(bins_per_soil) if len(b)]
-    for b0 in range(0, len(soils), batch_soils):
-        group = soils[b0:b0 + batch_soils]
+
+    def build(group):
         lay, cnt = layer_table(params[group])
-        plan = Batch.from_layers(lay, cnt, None, [setup.r], opt, (formulation, N.PLAIN_FP64, setup.omega_imag),
+        return Batch.from_layers(lay, cnt, None, [setup.r], opt, (formulation, N.PLAIN_FP64, setup.omega_imag),
                                  engine=engine, freqs_per_medium=[freqs[bins_per_soil[i]] for i in group])
-        try:
-            plan.execute()
-            status = plan.statuses()
-            if (status != 0).any():
-                raise RuntimeError(f"fallback row {int(np.nonzero(status)[0][0])}: status "
-                                   f"{N.STATUS_NAMES[int(status[np.nonzero(status)[0][0]])]}")
-            yield plan, group
-        finally:
+
+    def checked(plan):
+        status = plan.statuses()
+        if (status != 0).any():
+            bad = int(np.nonzero(status)[0][0])
+            raise RuntimeError(f"fallback row {bad}: status {N.STATUS_NAMES[int(status[bad])]}")
+
+    pending = []
+    try:
+        for b0 in range(0, len(soils), batch_soils):
+            group = soils[b0:b0 + batch_soils]
+            pending.append((build(group), group))
+            if len(pending) == 2:
+                checked(pending[0][0])
+                yield pending[0]
+                pending.pop(0)[0].close()
+            pending[-1][0].execute()
+        while pending:
+            checked(pending[0][0])
+            yield pending[0]
+            pending.pop(0)[0].close()
+    finally:
+        for plan, _ in pending:
             plan.close()
 
 
