@@ -21,6 +21,8 @@
 #include <cudaTypedefs.h>
 #include <math_constants.h>
 
+#include <utility>
+
 #include "gfk_kernels.cuh"
 #include "gfk_mlp.cuh"
 #include "gfk_tc.cuh"
@@ -55,6 +57,30 @@ __host__ __device__ inline uint32_t idesc_bf16_128x128() {
     id.n_dim_ = BN >> 3;
     id.m_dim_ = BM >> 4;
     return id.desc_;
+}
+
+// Programmatic dependent launch. The network's kernels are launched so that
+// the next one may be scheduled while the previous one finishes: each calls
+// dep_wait() before its first global-memory access (it returns once the
+// previous kernel in the stream has completed and its writes are visible; a
+// no-op for an ordinary launch) and dep_release() to let its successor start
+// its own set-up early.
+__device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void dep_release() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
+template <typename... P, typename... A>
+void launch_dep(void (*kern)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
 }
 
 // Hardware exponential and approximate reciprocal (no IEEE division): the
@@ -113,6 +139,8 @@ __global__ void __launch_bounds__(THREADS, 2)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
+    dep_wait();  // the set-up above overlaps the previous kernel's tail
+    dep_release();
 
     if (warp == 0) {
         if (lane == 0) {
@@ -340,6 +368,8 @@ __device__ __forceinline__ float feature(int j, const float* sf, const PointScal
 }
 
 __global__ void k_step_begin(TrainScalars* ts) {
+    dep_wait();
+    dep_release();
     const long long t = ++ts->step;
     float lr;
     if (t <= ts->warmup) {
@@ -360,6 +390,8 @@ __global__ void k_step_begin(TrainScalars* ts) {
 // label) of different blocks overlap.
 constexpr int kBatchRows = 16;
 __global__ void __launch_bounds__(kIn) k_batch(BatchArgs a) {
+    dep_wait();
+    dep_release();
     __shared__ bf16 tile[kBatchRows][kIn + 2];
     __shared__ PointScalars ps[kBatchRows];
     __shared__ int soil_of[kBatchRows];
@@ -420,6 +452,8 @@ __global__ void __launch_bounds__(256) k_head_train(const bf16* __restrict__ H, 
                                                     const float* __restrict__ Y, const float* __restrict__ Cw, int B,
                                                     bf16* __restrict__ dZ, bf16* __restrict__ dZT,
                                                     float* __restrict__ gpart, float* __restrict__ lpart) {
+    dep_wait();
+    dep_release();
     __shared__ __align__(16) bf16 tile[kHeadRows][kWidth + 8];
     __shared__ float red[2 * kWidth + 2];
     __shared__ float lred[8][4];
@@ -538,6 +572,8 @@ struct BiasPtrs {
 
 // One block per (output unit, layer): tree sum of that dz^T row.
 __global__ void __launch_bounds__(256) k_bias_grad(BiasPtrs d, int B, float* gb) {
+    dep_wait();
+    dep_release();
     __shared__ float sm[256];
     const int o = blockIdx.x, l = blockIdx.y;
     const bf16* row = d.p[l] + (size_t)o * B;
@@ -589,6 +625,8 @@ __device__ __forceinline__ float seg_grad(const AdamSeg& g, long long j) {
 // AdamW (Loshchilov & Hutter 2019) on the FP32 master copy, gradients summed
 // from their partials in a fixed order; refreshes the BF16 copy W.
 __global__ void k_adam(AdamArgs a) {
+    dep_wait();
+    dep_release();
     const AdamSeg g = a.dseg[blockIdx.y];
     const long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (j >= g.n) return;
@@ -609,6 +647,8 @@ __global__ void k_adam(AdamArgs a) {
 
 // W^T from W for every weight segment, 32 x 32 tiles through shared memory.
 __global__ void k_transpose_w(AdamArgs a) {
+    dep_wait();
+    dep_release();
     __shared__ bf16 t[32][33];
     const AdamSeg g = a.dseg[blockIdx.z];
     if (!g.wb) return;
@@ -636,6 +676,8 @@ __global__ void k_grad_flat(AdamArgs a, float* out) {
 // One warp: fixed-order sums of the head kernel's loss partials; each slot
 // holds the step's two coefficient-weighted mean squared errors.
 __global__ void k_loss_hist(const float* lpart, int nblk, int B, const TrainScalars* ts, float* hist, int cap) {
+    dep_wait();
+    dep_release();
     float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     for (int b = threadIdx.x; b < nblk; b += 32)
         for (int q = 0; q < 4; q++) s[q] += lpart[4 * b + q];
@@ -652,6 +694,8 @@ __global__ void k_loss_hist(const float* lpart, int nblk, int B, const TrainScal
 // ------------------------------------------------------------- inference --
 
 __global__ void __launch_bounds__(kIn) k_features(FeatureArgs a, long long rows_padded) {
+    dep_wait();
+    dep_release();
     const long long q0 = blockIdx.x * 32LL;
     const int j = threadIdx.x;
     for (int i = 0; i < 32; i++) {
@@ -672,6 +716,8 @@ __global__ void __launch_bounds__(kIn) k_features(FeatureArgs a, long long rows_
 }
 
 __global__ void __launch_bounds__(256) k_head_infer(HeadInferArgs a) {
+    dep_wait();
+    dep_release();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long q = blockIdx.x * 8LL + warp;
     if (q >= a.rows) return;
@@ -880,7 +926,12 @@ bool set_attr() {
 
 template <int MODE>
 void launch_mode(cudaStream_t s, const CUtensorMap& ta, const CUtensorMap& tb, dim3 grid, const GemmArgs& a) {
-    k_gemm<MODE><<<grid, THREADS, SMEM_BYTES, s>>>(ta, tb, a);
+    // weight gradients run on a second stream behind an event: an ordinary
+    // launch, so that event stays a full dependency
+    if (MODE == kWgrad)
+        k_gemm<MODE><<<grid, THREADS, SMEM_BYTES, s>>>(ta, tb, a);
+    else
+        launch_dep(k_gemm<MODE>, grid, dim3(THREADS), SMEM_BYTES, s, ta, tb, a);
 }
 }  // namespace
 
@@ -910,19 +961,21 @@ int launch_gemm(cudaStream_t s, int mode, const bf16* A, const bf16* B, int rows
     return 1;
 }
 
-void launch_step_begin(cudaStream_t s, TrainScalars* ts) { k_step_begin<<<1, 1, 0, s>>>(ts); }
+void launch_step_begin(cudaStream_t s, TrainScalars* ts) { launch_dep(k_step_begin, dim3(1), dim3(1), 0, s, ts); }
 
-void launch_batch(cudaStream_t s, const BatchArgs& a) { k_batch<<<a.B / kBatchRows, kIn, 0, s>>>(a); }
+void launch_batch(cudaStream_t s, const BatchArgs& a) {
+    launch_dep(k_batch, dim3(a.B / kBatchRows), dim3(kIn), 0, s, a);
+}
 
 void launch_head_train(cudaStream_t s, const bf16* H, const bf16* Z, const float* W6, const float* b6, const float* Y,
                        const float* C, int B, bf16* dZ, bf16* dZT, float* gpart, float* lpart) {
-    k_head_train<<<B / kHeadRows, 256, 0, s>>>(H, Z, W6, b6, Y, C, B, dZ, dZT, gpart, lpart);
+    launch_dep(k_head_train, dim3(B / kHeadRows), dim3(256), 0, s, H, Z, W6, b6, Y, C, B, dZ, dZT, gpart, lpart);
 }
 
 void launch_bias_grad(cudaStream_t s, const bf16* const* dZT, int layers, int B, float* gb) {
     BiasPtrs d{};
     for (int l = 0; l < layers && l < 8; l++) d.p[l] = dZT[l];
-    k_bias_grad<<<dim3(kWidth, layers), 256, 0, s>>>(d, B, gb);
+    k_bias_grad<<<dim3(kWidth, layers), 256, 0, s>>>(d, B, gb);  // follows the join of the two streams
 }
 
 namespace {
@@ -938,12 +991,12 @@ void launch_transposes(cudaStream_t s, const AdamArgs& a) {
             rows = a.seg[q].rows > rows ? a.seg[q].rows : rows;
             cols = a.seg[q].cols > cols ? a.seg[q].cols : cols;
         }
-    k_transpose_w<<<dim3(cols / 32, rows / 32, a.nseg), dim3(32, 8), 0, s>>>(a);
+    launch_dep(k_transpose_w, dim3(cols / 32, rows / 32, a.nseg), dim3(32, 8), 0, s, a);
 }
 }  // namespace
 
 void launch_adam(cudaStream_t s, const AdamArgs& a, long long) {
-    k_adam<<<dim3((unsigned)((max_seg(a) + 255) / 256), a.nseg), 256, 0, s>>>(a);
+    launch_dep(k_adam, dim3((unsigned)((max_seg(a) + 255) / 256), a.nseg), dim3(256), 0, s, a);
     launch_transposes(s, a);
 }
 
@@ -958,15 +1011,15 @@ void launch_grad_flat(cudaStream_t s, const AdamArgs& a, long long, float* out) 
 
 void launch_loss_hist(cudaStream_t s, const float* lpart, int nblk, int B, const TrainScalars* ts, float* hist,
                       int cap) {
-    k_loss_hist<<<1, 32, 0, s>>>(lpart, nblk, B, ts, hist, cap);
+    launch_dep(k_loss_hist, dim3(1), dim3(32), 0, s, lpart, nblk, B, ts, hist, cap);
 }
 
 void launch_features(cudaStream_t s, const FeatureArgs& a, long long rows_padded) {
-    k_features<<<(unsigned)((rows_padded + 31) / 32), kIn, 0, s>>>(a, rows_padded);
+    launch_dep(k_features, dim3((unsigned)((rows_padded + 31) / 32)), dim3(kIn), 0, s, a, rows_padded);
 }
 
 void launch_head_infer(cudaStream_t s, const HeadInferArgs& a) {
-    k_head_infer<<<(unsigned)((a.rows + 7) / 8), 256, 0, s>>>(a);
+    launch_dep(k_head_infer, dim3((unsigned)((a.rows + 7) / 8)), dim3(256), 0, s, a);
 }
 
 int launch_labels(cudaStream_t s, const LabelArgs& a) {
