@@ -445,6 +445,156 @@ def run_fdtd(args, gfk, torch, rank, world, local):
         print(json.dumps(out))
 
 
+def run_consume(args, gfk, torch, rank, world, local):
+    """Bank consumption (internal/sensing's use of a bank): the graded-soil
+    bank (2049 bins x 1024 ranges, fs 1 kHz, 4096-sample transform) built by
+    the solver and opened on the device once (payload and Bank.prepare
+    tables resident); per step the causal velocity impulse responses of 8192
+    query ranges (1024 samples each): bracket, Bank.Response interpolation,
+    i w, taper and inverse FFT on the device. `value` writes the responses to
+    device memory; `e2e` returns them to pinned host memory."""
+    eng = gfk.Engine(local)
+    wl = gfk.workloads.graded_soil()
+    med = wl.medium(gfk.DUNKIN, engine=eng, quadrature=gfk.SPLIT_INT8)
+    spectra, st = med.bank_spectra(wl.ranges, wl.freqs, wl.integration())
+    h = gfk.Header(gfk.Provenance("gfk-b200 fk"), wl.stack, wl.fs, wl.transform_samples,
+                   gfk.RangeGrid(0.5, 512.0, 1024),
+                   "vertical surface displacement per unit vertical surface point force", "m/N")
+    b = gfk.Bank.new(h)
+    b.data[:, 1:len(wl.freqs) + 1, 0] = spectra.T.real
+    b.data[:, 1:len(wl.freqs) + 1, 1] = spectra.T.imag
+    nq, length = 8192, 1024
+    q = np.random.default_rng(5).uniform(0.5, 512.0, nq)
+    t_open = time.perf_counter()
+    db = b.device(eng)
+    t_open = time.perf_counter() - t_open
+    dev = torch.empty((nq, length), dtype=torch.float64, device=f"cuda:{local}")
+    host = torch.empty((nq, length), dtype=torch.float64, pin_memory=True).numpy()
+    for _ in range(max(args.warmup, 3)):
+        db.impulse_responses(q, length, out_device_ptr=dev.data_ptr())
+        db.impulse_responses(q, length, out=host)
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        db.impulse_responses(q, length, out_device_ptr=dev.data_ptr())  # returns with the responses written
+    t = allmax(time.perf_counter() - t0, world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        db.impulse_responses(q, length, out=host)
+    t_e2e = allmax(time.perf_counter() - t0, world)
+    clk = clocks.stop()
+    t_one = time.perf_counter()
+    one = b.impulse_responses(q[:1024], length, engine=eng)  # the one-shot call: payload up, tables, responses
+    t_one = time.perf_counter() - t_one
+    assert np.isfinite(host).all() and np.array_equal(one, host[:1024])
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import bank_oracle as BO
+        c0 = time.perf_counter()
+        BO.prepare(b.data)
+        c_prep = time.perf_counter() - c0
+        ns = 32
+        c0 = time.perf_counter()
+        want = BO.impulse_responses(b.data, (0.5, 512.0), wl.fs, wl.transform_samples, q[:ns], length)
+        c_all = time.perf_counter() - c0  # includes one more prepare
+        per_q = max(c_all - c_prep, 1e-9) / ns
+        rel = float(np.linalg.norm(host[:ns] - want) / np.linalg.norm(want))
+        cpu = {"value": 1.0 / per_q, "unit": "impulse responses/s", "cores": 1, "kind": "port",
+               "sample": f"{ns} queries ({per_q * 1e3:.1f} ms each) through the numpy restatement "
+                         f"(oracle/bank_oracle.py) after its Bank.prepare ({c_prep:.1f} s, not counted, as the "
+                         f"device bank's one-off open is not)",
+               "relL2_gpu_vs_oracle_on_sample": rel}
+    db.close()
+    eng.close()
+    if rank == 0:
+        ms = 1e3 * t / args.steps
+        out_bytes = nq * length * 8
+        print(json.dumps({
+            "metric": "bank impulse responses/s (internal/sensing from a device-resident bank)",
+            "value": nq * args.steps * world / t, "unit": "impulse responses/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"consume: graded-soil bank 2049 bins x 1024 ranges (0.5-512 m) opened on the "
+                                   f"device once ({1e3 * t_open:.1f} ms), {nq} query ranges per step, velocity "
+                                   f"responses of {length} samples (4096-point transform)"},
+            "e2e": {"value": nq * args.steps * world / t_e2e, "unit": "impulse responses/s",
+                    "h2d_bytes_per_step": nq * 12, "d2h_bytes_per_step": out_bytes,
+                    "ms_per_step": 1e3 * t_e2e / args.steps},
+            "one_shot_call": {"queries": 1024, "ms": 1e3 * t_one,
+                              "note": "gfk_bank_impulse_responses: pageable payload upload, tables, responses"},
+            "gpu_launches": 2 * args.steps, "clocks": clk, "cpu_baseline": cpu}))
+
+
+def run_disp(args, gfk, torch, rank, world, local):
+    """Rayleigh dispersion curves (internal/disp over propmat.Secular): every
+    mode of the 10-layer graded soil at 512 frequencies 2-200 Hz per step, one
+    gfk_dispersion_modes call (a 2000-sample velocity scan per frequency, then
+    one bisection per bracket, one block per frequency)."""
+    D = gfk.disp
+    eng = gfk.Engine(local)
+    wl = gfk.workloads.graded_soil()
+    stack = wl.stack
+    freqs = np.linspace(2.0, 200.0, 512)
+    for _ in range(max(args.warmup, 3)):
+        res = D.modes_many(stack, freqs, engine=eng)
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        res = D.modes_many(stack, freqs, engine=eng)
+    t = allmax(time.perf_counter() - t0, world)
+    clk = clocks.stop()
+    roots = sum(len(r) for r in res)
+    samples, lfin = 2000, len(stack) - 1
+    # secular evaluations per step: the scan (samples + 1 per frequency) plus
+    # ~22 bisection halvings per root (bracket (hi - lo)/2000 down to 1e-10 relative)
+    evals = len(freqs) * (samples + 1) + 22 * roots
+    flops_eval = 3000 * lfin + 200  # per finite layer: 4x4 exponential, 6x6 compound, minor update
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import disp_oracle as DO
+        tup = [(l.thickness, l.vp, l.vs, l.density) for l in stack]
+        c0 = time.perf_counter()
+        ns = 0
+        worst = 0.0
+        while ns < 2 or (time.perf_counter() - c0 < 10.0 and ns < len(freqs)):
+            i = (ns * 97) % len(freqs)
+            want = DO.modes(tup, freqs[i])
+            got = res[i]
+            if len(want) == len(got) and want:
+                worst = max(worst, max(abs(a - b) / b for a, b in zip(got, want)))
+            ns += 1
+        cs = time.perf_counter() - c0
+        cpu = {"value": ns / cs, "unit": "frequencies/s", "cores": 1, "kind": "port",
+               "sample": f"{ns} of the frequencies through the numpy/scipy restatement (oracle/disp_oracle.py)",
+               "max_rel_root_diff_gpu_vs_oracle_on_sample": worst}
+    eng.close()
+    if rank == 0:
+        ms = 1e3 * t / args.steps
+        ach = evals * flops_eval / (ms * 1e-3) / 1e12
+        fp64_peak = fp64_gemm_peak(torch)
+        print(json.dumps({
+            "metric": "dispersion frequencies/s (all Rayleigh modes per frequency)",
+            "value": len(freqs) * args.steps * world / t, "unit": "frequencies/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"disp: graded soil (10 layers over a half-space), {len(freqs)} frequencies "
+                                   f"2-200 Hz, 2000-sample scan, tolerance 1e-10; {roots} roots per step"},
+            "e2e": {"value": len(freqs) * args.steps * world / t, "unit": "frequencies/s",
+                    "h2d_bytes_per_step": len(freqs) * 8 + len(stack) * 48, "d2h_bytes_per_step": len(freqs) * 68 * 8},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": ach / fp64_peak, "traffic": None,
+                         "note": "end-to-end call time; evaluations estimated as the scan plus ~22 bisection "
+                                 "steps per root, each counted at 3000 flops per finite layer + 200"},
+            "clocks": clk, "cpu_baseline": cpu}))
+
+
 def run_train(args, gfk, torch, rank, world, local):
     """Surrogate training throughput: labels for --sur-soils family soils
     from the batched FP64 solver, then W warm-up and K timed AdamW steps of
@@ -576,7 +726,7 @@ def main():
     ap.add_argument("--freq-stride", type=int, default=1,
                     help="profiling only: keep every n-th frequency (a smaller case of the same kernels)")
     ap.add_argument("--workload", default="graded", choices=["graded", "single", "batched", "sobol", "surrogate", "train",
-                                                              "fdtd"],
+                                                              "fdtd", "consume", "disp"],
                     help="graded: the 10-layer graded soil (default); batched: seeded uneven soils; "
                          "sobol: the all-plain Sobol run")
     ap.add_argument("--sobol-n", type=int, default=16384, help="sobol workload: Saltelli base size N")
@@ -611,6 +761,10 @@ def main():
         return run_sobol(args, gfk, torch, rank, world, local)
     if args.workload == "surrogate":
         return run_surrogate(args, gfk, torch, rank, world, local)
+    if args.workload == "consume":
+        return run_consume(args, gfk, torch, rank, world, local)
+    if args.workload == "disp":
+        return run_disp(args, gfk, torch, rank, world, local)
     if args.workload == "train":
         return run_train(args, gfk, torch, rank, world, local)
     if args.workload == "fdtd":

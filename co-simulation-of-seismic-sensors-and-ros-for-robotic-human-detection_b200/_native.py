@@ -36,6 +36,7 @@ EXPORTS = [
     "gfk_bank_pack", "gfk_bank_write", "gfk_vertical_displacement_multi_noalloc",
     "gfk_dispersion_modes", "gfk_secular", "gfk_fdtd_grid", "gfk_fdtd_run",
     "gfk_trace_metrics", "gfk_ensemble_gate", "gfk_scatter_rows", "gfk_bank_tables", "gfk_bank_impulse_responses",
+    "gfk_bank_device_open", "gfk_bank_device_impulse_responses", "gfk_bank_device_close",
     "gfk_dataset_create", "gfk_dataset_fill", "gfk_dataset_stats", "gfk_dataset_labels", "gfk_dataset_destroy",
     "gfk_net_create", "gfk_net_set_scales", "gfk_net_train", "gfk_net_train_ranges", "gfk_net_predict", "gfk_net_evaluate",
     "gfk_net_param_count", "gfk_net_params", "gfk_net_fourier", "gfk_net_probe", "gfk_net_destroy",
@@ -142,6 +143,9 @@ def lib():
         "gfk_bank_tables": (ctypes.c_int, [vp, P(f32), i32, i32, P(d), P(d)]),
         "gfk_bank_impulse_responses": (ctypes.c_int, [vp, P(f32), i32, i32, d, d, d, i32, P(d), i32, P(d), i32, i32,
                                                       P(d)]),
+        "gfk_bank_device_open": (ctypes.c_int, [vp, P(f32), i32, i32, d, d, d, i32, P(vp)]),
+        "gfk_bank_device_impulse_responses": (ctypes.c_int, [vp, P(d), i32, P(d), i32, i32, vp, i32]),
+        "gfk_bank_device_close": (ctypes.c_int, [vp]),
         "gfk_trace_metrics": (ctypes.c_int, [vp, vp, i64, i32, i32, P(d), i32, d, d, i32, i32, P(d), P(d)]),
         "gfk_dataset_create": (ctypes.c_int, [vp, i32, i32, P(d), P(d), P(d), i32, P(d), i32, d, P(vp)]),
         "gfk_dataset_fill": (ctypes.c_int, [vp, vp, i32, i32]),

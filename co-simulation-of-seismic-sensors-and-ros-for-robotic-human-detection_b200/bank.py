@@ -235,6 +235,11 @@ class Bank:
             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return out
 
+    def device(self, engine=None):
+        """The bank uploaded once, with Bank.prepare's tables built on the
+        device, for repeated queries (DeviceBank)."""
+        return DeviceBank(self, engine)
+
     def write(self, path):
         """bank.Write (format.go:215-240), through libgfk's gfk_bank_write."""
         self.header.validate()
@@ -246,6 +251,60 @@ class Bank:
                                     payload.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), payload.size)
         if st:
             raise FkError(st, f"bank: writing {path} failed")
+
+
+class DeviceBank:
+    """A bank resident on the device (gfk_bank_device_open): internal/sensing
+    loads a bank once and queries it contact after contact
+    (sensing.go:196-204), so the payload and its tables stay on the GPU and a
+    query moves only its ranges in and its responses out."""
+
+    def __init__(self, bank, engine=None):
+        from .fk import default_engine
+        self.engine = engine or default_engine()
+        self.header = bank.header
+        h = bank.header
+        pl = bank._payload()
+        p = ctypes.c_void_p()
+        self.engine.check(N.lib().gfk_bank_device_open(
+            self.engine.ctx, pl.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), h.ranges.count, h.bins(),
+            float(h.ranges.min_m), float(h.ranges.max_m), float(h.sample_rate_hz), int(h.samples), ctypes.byref(p)))
+        self.p = p.value
+
+    def impulse_responses(self, ranges, length, sensor=None, velocity=True, out=None, out_device_ptr=None):
+        """Bank.impulse_responses against the resident bank: into out (host,
+        [len(ranges), length] float64, e.g. pinned; allocated when None) or,
+        with out_device_ptr, into device memory (returns None)."""
+        r = np.ascontiguousarray(ranges, dtype=np.float64)
+        sp = None
+        if sensor is not None:
+            sc = np.asarray(sensor, dtype=np.complex128)
+            sa = np.ascontiguousarray(np.stack([sc.real, sc.imag], axis=1).ravel())
+            sp = sa.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        if out_device_ptr is not None:
+            self.engine.check(N.lib().gfk_bank_device_impulse_responses(
+                self.p, r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r), sp, 1 if velocity else 0,
+                int(length), ctypes.c_void_p(out_device_ptr), 1))
+            return None
+        if out is None:
+            out = np.zeros((len(r), int(length)))
+        elif out.shape != (len(r), int(length)) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of shape (len(ranges), length)")
+        self.engine.check(N.lib().gfk_bank_device_impulse_responses(
+            self.p, r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r), sp, 1 if velocity else 0,
+            int(length), out.ctypes.data_as(ctypes.c_void_p), 0))
+        return out
+
+    def close(self):
+        if self.p:
+            N.lib().gfk_bank_device_close(self.p)
+            self.p = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def open_bank(path):

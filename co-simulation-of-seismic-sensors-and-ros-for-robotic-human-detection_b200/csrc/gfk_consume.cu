@@ -17,6 +17,7 @@
 // One thread per bin builds the tables (the unwrap is sequential in range);
 // one block per query range builds its spectrum in shared memory and runs the
 // n-point FFT there (gfk_fft.cuh), n = the bank's Samples <= 4096.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -130,6 +131,36 @@ int cfail(gfk_ctx* ctx, int status, const char* msg) {
         }                                                                                          \
     } while (0)
 
+// format.go:295-309: the lower bracketing range index and the fraction
+// between it and the next, on the host; a range outside the grid is GFK_EARG.
+int bracket(gfk_ctx* ctx, int count, double min_m, double max_m, const double* ranges, int nq, std::vector<int>& lo,
+            std::vector<double>& frac) {
+    const double spacing = count > 1 ? (max_m - min_m) / (count - 1) : 0.0;
+    for (int q = 0; q < nq; q++) {
+        const double r = ranges[q];
+        if (!(r >= min_m && r <= max_m)) {
+            char buf[160];
+            snprintf(buf, sizeof buf, "bank: range %g m is outside the bank's %g to %g m", r, min_m, max_m);
+            return cfail(ctx, GFK_EARG, buf);
+        }
+        if (count == 1) {
+            lo[q] = 0;
+            frac[q] = 0.0;
+            continue;
+        }
+        const double x = (r - min_m) / spacing;
+        int l = (int)std::floor(x);
+        if (l >= count - 1) {
+            lo[q] = count - 2;
+            frac[q] = 1.0;
+        } else {
+            lo[q] = l;
+            frac[q] = x - l;
+        }
+    }
+    return GFK_OK;
+}
+
 // Device copies of a payload and its tables, freed together.
 struct Tables {
     gfk_ctx* ctx = nullptr;
@@ -189,32 +220,9 @@ int gfk_bank_impulse_responses(gfk_ctx* ctx, const float* payload, int32_t count
     if (!(fs_hz > 0)) return cfail(ctx, GFK_EARG, "dsp: sample rate must be positive");
     if (samples < length) return cfail(ctx, GFK_EARG, "dsp: transform size is shorter than the samples to keep");
     if (nq == 0) return GFK_OK;
-    // format.go:295-309 bracket, on the host
     std::vector<int> lo(nq);
     std::vector<double> frac(nq);
-    const double spacing = count > 1 ? (max_m - min_m) / (count - 1) : 0.0;
-    for (int q = 0; q < nq; q++) {
-        const double r = ranges[q];
-        if (!(r >= min_m && r <= max_m)) {
-            char buf[160];
-            snprintf(buf, sizeof buf, "bank: range %g m is outside the bank's %g to %g m", r, min_m, max_m);
-            return cfail(ctx, GFK_EARG, buf);
-        }
-        if (count == 1) {
-            lo[q] = 0;
-            frac[q] = 0.0;
-            continue;
-        }
-        const double x = (r - min_m) / spacing;
-        int l = (int)std::floor(x);
-        if (l >= count - 1) {
-            lo[q] = count - 2;
-            frac[q] = 1.0;
-        } else {
-            lo[q] = l;
-            frac[q] = x - l;
-        }
-    }
+    if (int st = bracket(ctx, count, min_m, max_m, ranges, nq, lo, frac)) return st;
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
     Tables t;
@@ -257,6 +265,162 @@ int gfk_bank_impulse_responses(gfk_ctx* ctx, const float* payload, int32_t count
     CS_CUDA(ctx, cudaGetLastError());
     CS_CUDA(ctx, cudaMemcpyAsync(out, d_out.p, (size_t)nq * length * sizeof(double), cudaMemcpyDeviceToHost, s));
     CS_CUDA(ctx, cudaStreamSynchronize(s));
+    return GFK_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------- device-resident bank --
+
+struct gfk_bank_dev {
+    gfk_ctx* ctx = nullptr;
+    int count = 0, bins = 0, samples = 0;
+    double min_m = 0, max_m = 0, fs = 0;
+    Tables t;                      // payload and Bank.prepare tables
+    double* d_tw = nullptr;        // e^{-2 pi i m / samples}, m < samples/2
+    int* d_lo = nullptr;           // per-query scratch, grown on demand
+    double* d_frac = nullptr;
+    size_t q_cap = 0;
+    double* d_sensor = nullptr;    // bins complex
+    double* d_out = nullptr;       // host-output staging
+    size_t out_cap = 0;
+};
+
+namespace {
+
+void bank_dev_free(gfk_bank_dev* b) {
+    cudaStream_t s = b->ctx->stream;
+    void* ptrs[] = {b->d_tw, b->d_lo, b->d_frac, b->d_sensor, b->d_out};
+    for (void* p : ptrs)
+        if (p) cudaFreeAsync(p, s);
+    // b->t frees the payload and the tables when b is deleted
+}
+
+template <typename T>
+int grow(gfk_ctx* ctx, T** p, size_t* cap, size_t n) {
+    if (n <= *cap) return GFK_OK;
+    if (*p) cudaFreeAsync(*p, ctx->stream);
+    *p = nullptr;
+    *cap = 0;
+    CS_CUDA(ctx, cudaMallocAsync((void**)p, n * sizeof(T), ctx->stream));
+    *cap = n;
+    return GFK_OK;
+}
+
+}  // namespace
+
+void gfk_release_banks(gfk_ctx* ctx) {
+    for (gfk_bank_dev* b : ctx->banks) {
+        bank_dev_free(b);
+        delete b;
+    }
+    ctx->banks.clear();
+}
+
+extern "C" {
+
+int gfk_bank_device_open(gfk_ctx* ctx, const float* payload, int32_t count, int32_t bins, double min_m,
+                         double max_m, double fs_hz, int32_t samples, gfk_bank_dev** out) {
+    if (!ctx || !payload || !out) return GFK_EARG;
+    *out = nullptr;
+    if (count < 1) return cfail(ctx, GFK_EARG, "bank: empty payload");
+    if (samples < 2 || (samples & (samples - 1)) || bins != samples / 2 + 1)
+        return cfail(ctx, GFK_EARG, "bank: samples must be a power of two with bins = samples/2 + 1");
+    if (samples > gfk::consume::kMaxSamples)
+        return cfail(ctx, GFK_ELIMIT, "bank: impulse responses are built for samples <= 4096");
+    if (!(fs_hz > 0)) return cfail(ctx, GFK_EARG, "dsp: sample rate must be positive");
+    if (!(min_m <= max_m)) return cfail(ctx, GFK_EARG, "bank: range grid max is below its min");
+    cudaSetDevice(ctx->device);
+    gfk_bank_dev* b = new gfk_bank_dev();
+    b->ctx = ctx;
+    b->count = count;
+    b->bins = bins;
+    b->samples = samples;
+    b->min_m = min_m;
+    b->max_m = max_m;
+    b->fs = fs_hz;
+    std::vector<double> tw(samples);
+    for (int m = 0; m < samples / 2; m++) {
+        const double a = -2.0 * M_PI * m / samples;
+        tw[2 * m] = std::cos(a);
+        tw[2 * m + 1] = std::sin(a);
+    }
+    int st = build_tables(ctx, payload, count, bins, b->t);
+    size_t cap = 0;
+    if (!st) st = grow(ctx, &b->d_tw, &cap, (size_t)samples);
+    if (!st && cudaMemcpyAsync(b->d_tw, tw.data(), samples * sizeof(double), cudaMemcpyHostToDevice, ctx->stream) !=
+                   cudaSuccess)
+        st = cfail(ctx, GFK_ECUDA, "bank: twiddle upload failed");
+    if (!st && cudaStreamSynchronize(ctx->stream) != cudaSuccess)  // the caller may free its payload now
+        st = cfail(ctx, GFK_ECUDA, "bank: upload or table build failed");
+    if (st) {
+        bank_dev_free(b);
+        delete b;
+        return st;
+    }
+    ctx->banks.push_back(b);
+    *out = b;
+    return GFK_OK;
+}
+
+int gfk_bank_device_impulse_responses(gfk_bank_dev* b, const double* ranges, int32_t nq, const double* sensor,
+                                      int32_t velocity, int32_t length, double* out, int32_t out_on_device) {
+    if (!b || !ranges || !out) return GFK_EARG;
+    gfk_ctx* ctx = b->ctx;
+    if (nq < 0) return cfail(ctx, GFK_EARG, "bank: negative query count");
+    if (length <= 0) return cfail(ctx, GFK_EARG, "dsp: impulse response length must be positive");
+    if (b->samples < length) return cfail(ctx, GFK_EARG, "dsp: transform size is shorter than the samples to keep");
+    if (nq == 0) return GFK_OK;
+    std::vector<int> lo(nq);
+    std::vector<double> frac(nq);
+    if (int st = bracket(ctx, b->count, b->min_m, b->max_m, ranges, nq, lo, frac)) return st;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    size_t qcap = b->q_cap, fcap = b->q_cap;
+    if (int st = grow(ctx, &b->d_lo, &qcap, (size_t)nq)) return st;
+    if (int st = grow(ctx, &b->d_frac, &fcap, (size_t)nq)) return st;
+    b->q_cap = std::min(qcap, fcap);
+    // the host vectors are synchronised below before they go out of scope
+    CS_CUDA(ctx, cudaMemcpyAsync(b->d_lo, lo.data(), nq * sizeof(int), cudaMemcpyHostToDevice, s));
+    CS_CUDA(ctx, cudaMemcpyAsync(b->d_frac, frac.data(), nq * sizeof(double), cudaMemcpyHostToDevice, s));
+    const cd* d_sensor = nullptr;
+    if (sensor) {
+        size_t scap = b->d_sensor ? (size_t)2 * b->bins : 0;
+        if (int st = grow(ctx, &b->d_sensor, &scap, (size_t)2 * b->bins)) return st;
+        CS_CUDA(ctx, cudaMemcpyAsync(b->d_sensor, sensor, (size_t)b->bins * 2 * sizeof(double),
+                                     cudaMemcpyHostToDevice, s));
+        d_sensor = reinterpret_cast<const cd*>(b->d_sensor);
+    }
+    double* dst = out;
+    if (!out_on_device) {
+        if (int st = grow(ctx, &b->d_out, &b->out_cap, (size_t)nq * length)) return st;
+        dst = b->d_out;
+    }
+    const size_t smem = (size_t)2 * b->samples * sizeof(cd);
+    if (smem > 48 * 1024)
+        CS_CUDA(ctx, cudaFuncSetAttribute(gfk::consume::k_impulse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+    gfk::consume::ImpulseArgs a{b->t.logmag, b->t.phase, b->count, b->bins, b->samples, length, b->d_lo, b->d_frac,
+                                d_sensor, velocity, b->fs, reinterpret_cast<const cd*>(b->d_tw), dst};
+    gfk::consume::k_impulse<<<nq, gfk::consume::kThreads, smem, s>>>(a);
+    ctx->launches++;
+    CS_CUDA(ctx, cudaGetLastError());
+    if (!out_on_device)
+        CS_CUDA(ctx, cudaMemcpyAsync(out, b->d_out, (size_t)nq * length * sizeof(double), cudaMemcpyDeviceToHost, s));
+    // the query uploads read host vectors local to this call: wait for them
+    // (and, for host output, for the responses)
+    CS_CUDA(ctx, cudaStreamSynchronize(s));
+    return GFK_OK;
+}
+
+int gfk_bank_device_close(gfk_bank_dev* b) {
+    if (!b) return GFK_OK;
+    gfk_ctx* ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    auto& v = ctx->banks;
+    v.erase(std::remove(v.begin(), v.end(), b), v.end());
+    bank_dev_free(b);
+    delete b;
     return GFK_OK;
 }
 

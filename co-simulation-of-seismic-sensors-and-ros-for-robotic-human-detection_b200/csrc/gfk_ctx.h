@@ -10,6 +10,7 @@
 struct gfk_plan;
 struct gfk_dataset;
 struct gfk_net;
+struct gfk_bank_dev;
 
 struct gfk_ctx {
     int device = 0;
@@ -19,6 +20,7 @@ struct gfk_ctx {
     std::vector<gfk_plan*> plans;        // live plans, destroyed by gfk_close
     std::vector<gfk_dataset*> datasets;  // live surrogate data sets and networks,
     std::vector<gfk_net*> nets;          // destroyed by gfk_close as well
+    std::vector<gfk_bank_dev*> banks;    // device-resident banks (gfk_consume.cu)
     // propagator launch shape chosen by tuning, per (layer count, wavenumber count)
     struct Tuned {
         int nl, nk, variant;
@@ -28,3 +30,5 @@ struct gfk_ctx {
 
 // Frees every surrogate object the context still holds (gfk_surrogate.cu).
 void gfk_release_surrogates(gfk_ctx* ctx);
+// Frees every device-resident bank the context still holds (gfk_consume.cu).
+void gfk_release_banks(gfk_ctx* ctx);

@@ -822,6 +822,7 @@ int gfk_close(gfk_ctx* ctx) {
     }
     ctx->plans.clear();
     gfk_release_surrogates(ctx);
+    gfk_release_banks(ctx);
     if (ctx->stream) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);

@@ -341,6 +341,24 @@ int gfk_bank_impulse_responses(gfk_ctx *ctx, const float *payload, int32_t count
                                const double *ranges_m, int32_t nq, const double *sensor,
                                int32_t velocity, int32_t length, double *out);
 
+/* A bank kept on the device for repeated queries: internal/sensing loads a
+ * bank once and asks it for responses contact after contact
+ * (sensing.go:196-204 over bank.Open, format.go:249-286), so the payload is
+ * uploaded and Bank.prepare's tables built once here (same argument rules as
+ * gfk_bank_impulse_responses), and each query call moves only its ranges in
+ * and its responses out. The handle belongs to ctx (freed by gfk_close if not
+ * closed before). */
+typedef struct gfk_bank_dev gfk_bank_dev;
+int gfk_bank_device_open(gfk_ctx *ctx, const float *payload, int32_t count, int32_t bins, double min_m,
+                         double max_m, double fs_hz, int32_t samples, gfk_bank_dev **out);
+/* gfk_bank_impulse_responses against an open bank. out_on_device nonzero: out
+ * is a device pointer of nq * length doubles on the context's device; zero: out
+ * is host memory (pinned is fastest). Either way the call returns with the
+ * responses written. */
+int gfk_bank_device_impulse_responses(gfk_bank_dev *b, const double *ranges, int32_t nq, const double *sensor,
+                                      int32_t velocity, int32_t length, double *out, int32_t out_on_device);
+int gfk_bank_device_close(gfk_bank_dev *b);
+
 /* ---- sweep metrics of geophone traces ------------------------------------ */
 /* For each of ns soils, the geophone trace synthesised from its displacement
  * spectrum and its two sweep metrics (internal/sweep/sweep.go:128-169 Measure:

@@ -81,3 +81,32 @@ def test_consume_errors(pkg, eng, solved_bank):
     with pytest.raises(pkg.FkError) as e:
         b.impulse_responses([2.0], 2000, engine=eng)
     assert e.value.status == pkg._native.EARG
+
+
+def test_device_bank_matches_one_shot_calls(pkg, eng, solved_bank):
+    """A bank kept on the device answers repeated queries exactly as the
+    one-shot call does (same tables, same kernel), into host memory and into
+    device memory, and reports the one-shot call's errors."""
+    import torch
+    b = solved_bank
+    h = b.header
+    rng = np.random.default_rng(9)
+    f = np.arange(h.bins()) * h.sample_rate_hz / h.samples
+    sensor = 28.8 * (2j * np.pi * f) ** 2 / ((2j * np.pi * f) ** 2 + 2 * 0.7 * 62.83 * 2j * np.pi * f + 62.83 ** 2)
+    with b.device(eng) as db:
+        for n in (5, 37):  # the second call grows the query scratch
+            ranges = rng.uniform(h.ranges.min_m, h.ranges.max_m, n)
+            want = b.impulse_responses(ranges, 300, sensor=sensor, engine=eng)
+            got = db.impulse_responses(ranges, 300, sensor=sensor)
+            assert np.array_equal(got, want)
+            dev = torch.empty((n, 300), dtype=torch.float64, device="cuda:0")
+            assert db.impulse_responses(ranges, 300, sensor=sensor, out_device_ptr=dev.data_ptr()) is None
+            assert np.array_equal(dev.cpu().numpy(), want)
+        plain = db.impulse_responses([2.0, 9.5], 200, velocity=False)
+        assert np.array_equal(plain, b.impulse_responses([2.0, 9.5], 200, velocity=False, engine=eng))
+        with pytest.raises(pkg.FkError) as e:
+            db.impulse_responses([20.0], 100)
+        assert e.value.status == pkg._native.EARG and "outside the bank" in str(e.value)
+        with pytest.raises(pkg.FkError) as e:
+            db.impulse_responses([2.0], 2000)
+        assert e.value.status == pkg._native.EARG
