@@ -76,11 +76,10 @@ struct ImpulseArgs {
 };
 
 __global__ void __launch_bounds__(kThreads) k_impulse(ImpulseArgs a) {
-    extern __shared__ cd buf[];  // [2][n]
-    cd* x = buf;
-    cd* y = buf + a.n;
+    extern __shared__ cd x[];  // [n], the spectrum in bit-reversed order, then the transform
     const int q = blockIdx.x;
     const int n = a.n;
+    const int logn = 31 - __clz(n);
     const int lo = a.lo[q];
     const int hi = a.count == 1 ? lo : lo + 1;
     const double frac = a.frac[q];
@@ -104,12 +103,12 @@ __global__ void __launch_bounds__(kThreads) k_impulse(ImpulseArgs a) {
             if (f > taper_from) h = h * (0.5 * (1.0 + cos(pi * (f - taper_from) / (nyq - taper_from))));
         }
         if (k == 0 || k == n / 2) h.im = 0.0;  // the real transform reads only their real parts
-        x[k] = mk(h.re, -h.im);                // conj of the Hermitian extension
-        if (k > 0 && k < n / 2) x[n - k] = h;
+        x[bitrev(k, logn)] = mk(h.re, -h.im);  // conj of the Hermitian extension
+        if (k > 0 && k < n / 2) x[bitrev(n - k, logn)] = h;
     }
     __syncthreads();
-    const cd* r = fft_pow2(x, y, n, a.tw);
-    for (int t = threadIdx.x; t < a.length; t += blockDim.x) a.out[(size_t)q * a.length + t] = r[t].re / n;
+    fft_pow2_dit_inplace(x, n, a.tw);
+    for (int t = threadIdx.x; t < a.length; t += blockDim.x) a.out[(size_t)q * a.length + t] = x[t].re / n;
 }
 
 }  // namespace consume
@@ -252,7 +251,7 @@ int gfk_bank_impulse_responses(gfk_ctx* ctx, const float* payload, int32_t count
         CS_CUDA(ctx, cudaMallocAsync(&d_sensor.p, (size_t)bins * 2 * sizeof(double), s));
         CS_CUDA(ctx, cudaMemcpyAsync(d_sensor.p, sensor, (size_t)bins * 2 * sizeof(double), cudaMemcpyHostToDevice, s));
     }
-    const size_t smem = (size_t)2 * samples * sizeof(cd);
+    const size_t smem = (size_t)samples * sizeof(cd);
     if (smem > 48 * 1024)
         CS_CUDA(ctx, cudaFuncSetAttribute(gfk::consume::k_impulse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
@@ -396,7 +395,7 @@ int gfk_bank_device_impulse_responses(gfk_bank_dev* b, const double* ranges, int
         if (int st = grow(ctx, &b->d_out, &b->out_cap, (size_t)nq * length)) return st;
         dst = b->d_out;
     }
-    const size_t smem = (size_t)2 * b->samples * sizeof(cd);
+    const size_t smem = (size_t)b->samples * sizeof(cd);
     if (smem > 48 * 1024)
         CS_CUDA(ctx, cudaFuncSetAttribute(gfk::consume::k_impulse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));

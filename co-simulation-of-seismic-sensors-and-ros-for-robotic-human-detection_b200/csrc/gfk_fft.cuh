@@ -35,4 +35,27 @@ __device__ inline cd* fft_pow2(cd* x, cd* y, int n, const cd* __restrict__ tw) {
     return src;
 }
 
+// In-place iterative radix-2 decimation in time (Cooley-Tukey): x holds the
+// input in bit-reversed order (element k at index bitrev(k)); the forward
+// transform (e^{-i}) ends in x in natural order. Half the shared memory of
+// fft_pow2; every thread of the block must call it.
+__device__ inline void fft_pow2_dit_inplace(cd* x, int n, const cd* __restrict__ tw) {
+    for (int len = 2; len <= n; len <<= 1) {
+        const int half = len >> 1, step = n / len;
+        for (int j = threadIdx.x; j < n / 2; j += blockDim.x) {
+            const int pos = j & (half - 1);
+            const int i0 = ((j - pos) << 1) + pos;
+            const cd w = tw[pos * step];
+            const cd a = x[i0];
+            const cd b = x[i0 + half] * w;
+            x[i0] = a + b;
+            x[i0 + half] = a - b;
+        }
+        __syncthreads();
+    }
+}
+
+// Index of element k in the bit-reversed order of a 2^logn record.
+__device__ __forceinline__ int bitrev(int k, int logn) { return (int)(__brev((unsigned)k) >> (32 - logn)); }
+
 }  // namespace gfk
