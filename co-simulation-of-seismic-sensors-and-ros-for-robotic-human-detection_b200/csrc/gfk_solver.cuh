@@ -152,8 +152,11 @@ GFK_HD void decaying_minors(const Terms& t, cd m[6]) {
     m[5] = (mu * mu) * t.r2;
 }
 
-// m <- C(exp(-A zeta)) m up to a scalar: one layer, bottom to top.
-GFK_HD void dunkin_layer_up(const Terms& t, double zeta, cd m[6]) {
+// m <- C(exp(-A zeta)) m up to a scalar: one layer, bottom to top. With
+// renorm the result is rescaled by a power of two (exact) so its largest part
+// is in [1, 2); a layer changes the magnitude by a bounded factor, so callers
+// rescale every few layers (kRenormEvery) and at the surface.
+GFK_HD void dunkin_layer_up(const Terms& t, double zeta, cd m[6], bool renorm = true) {
     const cd ra = t.ra, rb = t.rb, mu = t.mup, u1 = t.u1, x2 = t.x2, r2 = t.r2;
     const cd rarb = ra * rb;
     const cd tt = mu * (1.0 + rb * rb);
@@ -207,6 +210,7 @@ GFK_HD void dunkin_layer_up(const Terms& t, double zeta, cd m[6]) {
     m[4] = mx2 * s05 + (mu * p13) * d23 - (2.0 * ra * tt) * z1 + (2.0 * mrb * u1) * z4;
     m[5] = (mu2 * r2) * s05 + (mu2 * p23) * d23 - (4.0 * mra * tt) * z1 + (2.0 * mu2 * rb * x2) * z4;
     // renormalise by a power of two (exact; the common scale cancels)
+    if (!renorm) return;
     double mx = 0.0;
 #pragma unroll
     for (int i = 0; i < 6; i++) mx = fmax(mx, cnorm1(m[i]));
@@ -229,6 +233,11 @@ GFK_HD void dunkin_layer_up(const Terms& t, double zeta, cd m[6]) {
 // the graded, single and seeded uneven soils the difference stays at rounding
 // level down to kThick = 20 (below that it grows as ~3e2 e^(-2 kThick)).
 constexpr double kThick = 32.0;
+
+// Layers between power-of-two rescalings of the minor vector (the scale is
+// exact and cancels, so the result does not depend on it while nothing
+// overflows; one layer changes the magnitude by far less than 2^64).
+constexpr int kRenormEvery = 4;
 
 GFK_HD bool thick_layer(const LayerC& L, cd c2, double zeta) {
     const double pa = 1.0 - (c2.re * L.c[0].re - c2.im * L.c[0].im);  // Re(1 - ea)
@@ -256,7 +265,7 @@ GFK_HD cd dunkin_u(const LayerC* L, int n, cd wc2, double k, double mu_ref) {
     }
     for (int i = top - 1; i >= 0; i--) {
         Terms t = layer_terms(L[i], c2);
-        dunkin_layer_up(t, k * L[i].h, m);
+        dunkin_layer_up(t, k * L[i].h, m, i % kRenormEvery == 0);
     }
     return m[3] / ((kTwoPi * mu_ref * k) * m[5]);
 }
@@ -277,11 +286,11 @@ GFK_HD void dunkin_u2(const LayerC* L, int n, cd wc2, double k0, double k1, doub
     for (int i = (top0 > top1 ? top0 : top1) - 1; i >= 0; i--) {
         if (i < top0) {
             Terms t0 = layer_terms(L[i], c20);
-            dunkin_layer_up(t0, k0 * L[i].h, m0);
+            dunkin_layer_up(t0, k0 * L[i].h, m0, i % kRenormEvery == 0);
         }
         if (i < top1) {
             Terms t1 = layer_terms(L[i], c21);
-            dunkin_layer_up(t1, k1 * L[i].h, m1);
+            dunkin_layer_up(t1, k1 * L[i].h, m1, i % kRenormEvery == 0);
         }
     }
     u0 = m0[3] / ((kTwoPi * mu_ref * k0) * m0[5]);
