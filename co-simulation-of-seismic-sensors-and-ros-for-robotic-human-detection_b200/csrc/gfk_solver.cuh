@@ -230,9 +230,11 @@ GFK_HD void dunkin_layer_up(const Terms& t, double zeta, cd m[6], bool renorm = 
 // cannot reach the surface in FP64. Propagation therefore starts at the
 // shallowest such layer. Re(sqrt(1 - e)) >= sqrt(Re(1 - e)) gives a cheap
 // sufficient test without the square roots. Against the full propagation on
-// the graded, single and seeded uneven soils the difference stays at rounding
-// level down to kThick = 20 (below that it grows as ~3e2 e^(-2 kThick)).
-constexpr double kThick = 32.0;
+// the graded, single and 40 seeded uneven soils the difference stays at
+// rounding level down to kThick = 20; below that it grows as C e^(-2 kThick)
+// with C = 260-550 at kThick = 8-12 (rising slowly with kThick), so at 26 the
+// neglected part is ~1e-19 relative, three orders below FP64 rounding.
+constexpr double kThick = 26.0;
 
 // Layers between power-of-two rescalings of the minor vector (the scale is
 // exact and cancels, so the result does not depend on it while nothing
