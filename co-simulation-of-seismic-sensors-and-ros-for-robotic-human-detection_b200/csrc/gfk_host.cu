@@ -223,7 +223,8 @@ struct gfk_plan {
     // split-K wavenumber sums for chunks too small to fill the SMs
     int ksplit = 1;
     cd* d_ksum = nullptr;  // [ksplit][rows of a chunk][nr] partial sums
-    int32_t launches_per_exec = 0;
+    int32_t launches_per_exec = 0;  // after the first execute (which also builds the Hankel weights)
+    bool weights_ready = false;
     int prop_variant = -1;       // Dunkin launch shape; -1 until the first execute tunes it
     std::vector<float> tune_ms;  // per variant, from the tuning run
     // CUDA graph of one whole execute
@@ -568,7 +569,7 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
     int nchunks = 0;
     for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
         if (p->chunk_begin[c + 1] > p->chunk_begin[c]) nchunks++;
-    p->launches_per_exec = p->nf > 0 ? (p->tc ? 3 + 3 * nchunks : 2 + 2 * nchunks + (p->shared ? 1 : 0)) : 0;
+    p->launches_per_exec = p->nf > 0 ? (p->tc ? 2 + 3 * nchunks : 2 + 2 * nchunks) : 0;
     if (p->nf > 0 && p->ksplit > 1) p->launches_per_exec += nchunks;
     if (p->fused) p->prop_variant = 0;  // one launch shape; nothing to tune
     *out = p;
@@ -645,12 +646,19 @@ int plan_enqueue(gfk_plan* p, bool timed) {
     gfk::launch_layer_consts_fl(s, p->d_lp, p->d_media, p->d_fd, nf, p->max_nl, p->solve.omega_imag, form, p->d_lc,
                                 p->d_wc2);
     gfk::launch_static(s, p->d_lc, p->d_media, p->d_fd, p->d_wc2, nf, form, p->d_C, p->d_status);
-    if (p->tc)
-        gfk::launch_j0_slices(s, p->d_ranges, p->nr, p->g_n, p->Kp, p->Np, p->g_kmax / p->g_n, p->col_exp, p->d_B);
-    else if (p->shared)
-        gfk::launch_j0_table(s, p->d_ranges, p->nr, p->g_n, p->g_kmax / p->g_n, p->d_W);
+    // the Hankel weights depend only on the plan's grid and ranges: built by
+    // the first execute, kept for the later ones (and out of a captured graph)
+    if (p->shared && !p->weights_ready) {
+        if (p->tc)
+            gfk::launch_j0_slices(s, p->d_ranges, p->nr, p->g_n, p->Kp, p->Np, p->g_kmax / p->g_n, p->col_exp,
+                                  p->d_B);
+        else
+            gfk::launch_j0_table(s, p->d_ranges, p->nr, p->g_n, p->g_kmax / p->g_n, p->d_W);
+        ctx->launches++;
+        p->weights_ready = true;
+    }
     if (timed && (st = end_seg(p, seg))) return st;
-    ctx->launches += 2 + (p->shared ? 1 : 0);
+    ctx->launches += 2;
     if (timed && p->prop_variant < 0 && (st = tune_prop(p))) return st;
     const double dk = p->shared ? p->g_kmax / p->g_n : 0.0;
     for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++) {
