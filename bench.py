@@ -4,7 +4,9 @@ One step = one full Green's-function bank of the graded-soil workload
 (10 finite layers over a half-space, 2048 frequencies x 16384 wavenumbers x
 1024 ranges, complex Dunkin propagators in FP64, shared-grid quadrature),
 recomputed from the medium: layer constants, static coefficients, the
-propagator over every (f, k), the J0 table and the wavenumber sum.
+propagator over every (f, k) and the wavenumber sum. The Hankel (J0) weights
+depend only on the plan's grid and ranges and are built by its first execute;
+the e2e leg builds a new plan, weights included, every step.
 
   value  cells/s with the medium already on the device (gfk_plan_execute),
          timed with CUDA events on the plan's stream, L2 flushed between steps
