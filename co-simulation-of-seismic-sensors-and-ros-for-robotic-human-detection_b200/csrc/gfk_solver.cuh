@@ -258,7 +258,7 @@ GFK_HD int start_layer(const LayerC* L, int n, cd c2, double k) {
 // Surface vertical displacement per newton (fk.go:276-327) by minor
 // propagation: u_z = i b4 M_12/M_23 with b4 = -i/(2 pi mu_ref k).
 GFK_HD cd dunkin_u(const LayerC* L, int n, cd wc2, double k, double mu_ref) {
-    const cd c2 = wc2 * (1.0 / (k * k));
+    const cd c2 = wc2 * rcp_(k * k);  // rcp_ is the correctly rounded 1/x
     const int top = start_layer(L, n, c2, k);
     cd m[6];
     {
@@ -269,14 +269,16 @@ GFK_HD cd dunkin_u(const LayerC* L, int n, cd wc2, double k, double mu_ref) {
         Terms t = layer_terms(L[i], c2);
         dunkin_layer_up(t, k * L[i].h, m, i % kRenormEvery == 0);
     }
-    return m[3] / ((kTwoPi * mu_ref * k) * m[5]);
+    // the minors end rescaled into [1, 2), so |denominator|^2 stays in range
+    // for one real reciprocal
+    return cdiv_fast(m[3], (kTwoPi * mu_ref * k) * m[5]);
 }
 
 // Two wavenumbers of one frequency in lockstep through the layers: two
 // independent dependency chains per thread, for latency hiding at low occupancy.
 GFK_HD void dunkin_u2(const LayerC* L, int n, cd wc2, double k0, double k1, double mu_ref, cd& u0, cd& u1) {
-    const cd c20 = wc2 * (1.0 / (k0 * k0));
-    const cd c21 = wc2 * (1.0 / (k1 * k1));
+    const cd c20 = wc2 * rcp_(k0 * k0);
+    const cd c21 = wc2 * rcp_(k1 * k1);
     const int top0 = start_layer(L, n, c20, k0), top1 = start_layer(L, n, c21, k1);
     cd m0[6], m1[6];
     {
@@ -295,8 +297,8 @@ GFK_HD void dunkin_u2(const LayerC* L, int n, cd wc2, double k0, double k1, doub
             dunkin_layer_up(t1, k1 * L[i].h, m1, i % kRenormEvery == 0);
         }
     }
-    u0 = m0[3] / ((kTwoPi * mu_ref * k0) * m0[5]);
-    u1 = m1[3] / ((kTwoPi * mu_ref * k1) * m1[5]);
+    u0 = cdiv_fast(m0[3], (kTwoPi * mu_ref * k0) * m0[5]);
+    u1 = cdiv_fast(m1[3], (kTwoPi * mu_ref * k1) * m1[5]);
 }
 
 // ------------------------------------------------------ reference direct --
