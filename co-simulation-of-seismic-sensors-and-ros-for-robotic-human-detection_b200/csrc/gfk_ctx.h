@@ -15,6 +15,7 @@ struct gfk_bank_dev;
 struct gfk_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // device-to-host copies beside the compute (created on first use)
     std::string last_error;
     int64_t launches = 0;
     std::vector<gfk_plan*> plans;        // live plans, destroyed by gfk_close

@@ -227,6 +227,10 @@ struct gfk_plan {
     bool weights_ready = false;
     int prop_variant = -1;       // Dunkin launch shape; -1 until the first execute tunes it
     std::vector<float> tune_ms;  // per variant, from the tuning run
+    // end-to-end call into pinned host memory: each chunk's rows are copied
+    // out on the context's copy stream while the next chunk computes
+    double* async_out = nullptr;
+    cudaEvent_t ev_chunk = nullptr;
     // CUDA graph of one whole execute
     bool use_graph = false;
     cudaGraphExec_t gexec = nullptr;
@@ -247,6 +251,7 @@ void plan_free(gfk_plan* p) {
     if (!p) return;
     cudaStream_t s = p->ctx ? p->ctx->stream : nullptr;
     if (p->gexec) cudaGraphExecDestroy(p->gexec);
+    if (p->ev_chunk) cudaEventDestroy(p->ev_chunk);
     void* ptrs[] = {p->d_lp,  p->d_media, p->d_fd, p->d_ranges, p->d_W, p->d_lc,     p->d_wc2,
                     p->d_C,   p->d_rem,   p->d_G,  p->d_status, p->d_A, p->d_B,      p->d_rowexp,
                     p->d_rowmax, p->d_partial, p->d_ksum};
@@ -327,7 +332,8 @@ struct SoilIn {
 };
 
 int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s, const double* ranges, int32_t nr,
-               gfk_integration opt, GridMode mode, gfk_plan** out) {
+               gfk_integration opt, GridMode mode, gfk_plan** out, int chunk_rows = 0) {
+    const int max_rows = chunk_rows > 0 ? std::min(chunk_rows, kMaxChunkRows) : kMaxChunkRows;
     *out = nullptr;
     if (!ctx) return GFK_EARG;
     if (!s) return fail(ctx, GFK_EARG, "solve options missing");
@@ -490,7 +496,7 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
     p->chunk_begin.push_back(0);
     for (int f = 0; f < p->nf; f++) {
         const int nk = p->shared ? p->g_n : (p->fd[f].kfar > 0 ? p->fd[f].nk : 0);
-        if (rows_in > 0 && (acc + nk > budget || rows_in >= kMaxChunkRows)) {
+        if (rows_in > 0 && (acc + nk > budget || rows_in >= max_rows)) {
             p->chunk_begin.push_back(f);
             p->chunk_max_nk.push_back(cmax);
             cap = std::max(cap, acc);
@@ -632,6 +638,18 @@ int tune_prop(gfk_plan* p) {
     return GFK_OK;
 }
 
+// With async_out set, queues the download of rows [fb, fb + n) on the copy
+// stream once the compute stream has finished them.
+int copy_chunk_out(gfk_plan* p, int fb, int n) {
+    if (!p->async_out || n <= 0) return GFK_OK;
+    gfk_ctx* ctx = p->ctx;
+    GFK_CUDA(ctx, cudaEventRecord(p->ev_chunk, ctx->stream));
+    GFK_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, p->ev_chunk, 0));
+    GFK_CUDA(ctx, cudaMemcpyAsync(p->async_out + (size_t)2 * fb * p->nr, p->d_G + (size_t)fb * p->nr,
+                                  sizeof(cd) * (size_t)n * p->nr, cudaMemcpyDeviceToHost, ctx->copy_stream));
+    return GFK_OK;
+}
+
 // Enqueues one whole execute on the context's stream. `timed` records the
 // per-kernel-class event segments (not inside a graph capture).
 int plan_enqueue(gfk_plan* p, bool timed) {
@@ -673,6 +691,7 @@ int plan_enqueue(gfk_plan* p, bool timed) {
                                    p->d_G + (size_t)fb * p->nr);
             if (timed && (st = end_seg(p, seg))) return st;
             ctx->launches += 2;
+            if ((st = copy_chunk_out(p, fb, cnf))) return st;
             continue;
         }
         if (p->tc) GFK_CUDA(ctx, cudaMemsetAsync(p->d_rowmax, 0, sizeof(unsigned long long) * 2 * cnf, s));
@@ -698,6 +717,7 @@ int plan_enqueue(gfk_plan* p, bool timed) {
         }
         if (timed && (st = end_seg(p, seg))) return st;
         ctx->launches += 2;
+        if ((st = copy_chunk_out(p, fb, cnf))) return st;
     }
     GFK_CUDA(ctx, cudaGetLastError());
     return GFK_OK;
@@ -770,9 +790,10 @@ int plan_download(gfk_plan* p, double* out, int32_t* status) {
 }
 
 int plan_one(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const double* ranges, int32_t nr,
-             const double* freqs, int32_t nf, gfk_integration opt, GridMode mode, gfk_plan** out) {
+             const double* freqs, int32_t nf, gfk_integration opt, GridMode mode, gfk_plan** out,
+             int chunk_rows = 0) {
     SoilIn si{m, freqs, nf};
-    return plan_build(ctx, &si, 1, s, ranges, nr, opt, mode, out);
+    return plan_build(ctx, &si, 1, s, ranges, nr, opt, mode, out, chunk_rows);
 }
 
 }  // namespace
@@ -831,6 +852,10 @@ int gfk_close(gfk_ctx* ctx) {
     ctx->plans.clear();
     gfk_release_surrogates(ctx);
     gfk_release_banks(ctx);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
     if (ctx->stream) {
         cudaStreamSynchronize(ctx->stream);
         cudaStreamDestroy(ctx->stream);
@@ -943,11 +968,41 @@ int gfk_bank_spectra(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, cons
                      const double* freqs, int32_t nf, gfk_integration opt, double* out, int32_t* status_per_f) {
     if (!ctx) return GFK_EARG;
     cudaSetDevice(ctx->device);
+    // Into page-locked host memory a large bank (>= 8 MB) is computed in two
+    // row chunks, the first downloaded on a second stream while the second
+    // computes (smaller banks lose more to the extra launches than they hide).
+    bool overlap = false;
+    if (out && nf >= 256 && nr >= 1 && (int64_t)nf * nr * 16 >= (int64_t(8) << 20)) {
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost) overlap = true;
+        cudaGetLastError();  // a pageable pointer is not an error
+    }
+    if (overlap && !ctx->copy_stream &&
+        cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        ctx->copy_stream = nullptr;
+        overlap = false;
+    }
     gfk_plan* p = nullptr;
-    int st = plan_one(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, &p);
+    int st = plan_one(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, &p, overlap ? (nf + 1) / 2 : 0);
     if (st) return st;
+    if (overlap && p->chunk_begin.size() > 2 &&
+        cudaEventCreateWithFlags(&p->ev_chunk, cudaEventDisableTiming) == cudaSuccess)
+        p->async_out = out;
     st = plan_exec(p);
-    if (!st) st = plan_download(p, out, status_per_f);
+    if (p->async_out) {
+        if (cudaStreamSynchronize(ctx->copy_stream) != cudaSuccess && !st)
+            st = fail(ctx, GFK_ECUDA, "bank download failed");
+        if (!st) {  // statuses, and failed rows zeroed, as plan_download gives them
+            std::vector<int32_t> stv(std::max(p->nf, 1));
+            st = plan_download(p, nullptr, stv.data());
+            for (int f = 0; f < p->nf; f++) {
+                if (stv[f]) std::memset(out + (size_t)2 * nr * f, 0, sizeof(double) * 2 * nr);
+                if (status_per_f) status_per_f[f] = stv[f];
+            }
+        }
+    } else if (!st) {
+        st = plan_download(p, out, status_per_f);
+    }
     std::string msg = ctx->last_error;
     plan_free(p);
     delete p;

@@ -200,15 +200,20 @@ class Medium:
         eng.check(st)
         return out[0::2] + 1j * out[1::2]
 
-    def bank_spectra(self, ranges, freqs, opt=None, raise_on_error=True):
+    def bank_spectra(self, ranges, freqs, opt=None, raise_on_error=True, out=None):
         """VerticalDisplacementMulti at many frequencies in one GPU call, as
         cmd/geobank/main.go:133-167 builds a bank. Returns ([nf, nr] complex128,
         per-frequency status); raises on the first failing frequency unless
-        raise_on_error is False."""
+        raise_on_error is False. `out` may supply the [nf, 2 nr] float64
+        (re, im) buffer; in page-locked memory a larger bank is downloaded in
+        chunks while the rest computes."""
         opt = opt or Integration()
         r = np.ascontiguousarray(ranges, dtype=np.float64)
         f = np.ascontiguousarray(freqs, dtype=np.float64)
-        out = np.zeros((len(f), 2 * len(r)))
+        if out is None:
+            out = np.zeros((len(f), 2 * len(r)))
+        elif out.shape != (len(f), 2 * len(r)) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of shape (len(freqs), 2 len(ranges))")
         status = np.zeros(len(f), dtype=np.int32)
         eng = self._engine()
         with _c_medium(self) as cm:

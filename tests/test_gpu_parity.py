@@ -413,3 +413,31 @@ def test_sobol_banks_and_metrics_against_oracle(gfk, engine, oracle):
         y = S.traces(np.vstack([G[i], want[:, 0]]), setup)
         pk, cen = S.measure(y, setup.fs)
         assert abs(pk[0] - pk[1]) / pk[1] < 1e-8 and abs(cen[0] - cen[1]) < 1e-6
+
+
+def test_pinned_bank_download_overlaps_and_matches(gfk, engine):
+    """Into page-locked memory gfk_bank_spectra computes a larger bank in row
+    chunks and downloads each while the next computes; the bank equals the
+    one-piece call to rounding (the split sums differ only in their split
+    count), and failing rows come back zeroed with their statuses."""
+    import torch
+    wl = gfk.workloads.single_soil()
+    wl.ranges = np.linspace(1.0, 64.0, 2048)  # 512 x 2048 cells = 16 MB: the chunked path
+    for q in (gfk.PLAIN_FP64, gfk.SPLIT_INT8):
+        m = wl.medium(gfk.DUNKIN, engine=engine, quadrature=q)
+        want, sw = m.bank_spectra(wl.ranges, wl.freqs, wl.integration())
+        pinned = torch.zeros((len(wl.freqs), 2 * len(wl.ranges)), dtype=torch.float64, pin_memory=True).numpy()
+        got, sg = m.bank_spectra(wl.ranges, wl.freqs, wl.integration(), out=pinned)
+        assert (sw == 0).all() and (sg == 0).all()
+        per_bin = np.linalg.norm(got - want, axis=1) / np.linalg.norm(want, axis=1)
+        assert per_bin.max() < 1e-11, per_bin.max()
+        got2, _ = m.bank_spectra(wl.ranges, wl.freqs, wl.integration(), out=pinned)
+        assert np.array_equal(got, got2)
+    freqs = wl.freqs.copy()
+    freqs[300] = -5.0
+    m = wl.medium(gfk.DUNKIN, engine=engine)
+    pinned = torch.full((len(freqs), 2 * len(wl.ranges)), 7.0, dtype=torch.float64, pin_memory=True).numpy()
+    got, st = m.bank_spectra(wl.ranges, freqs, wl.integration(), raise_on_error=False, out=pinned)
+    want, stw = m.bank_spectra(wl.ranges, freqs, wl.integration(), raise_on_error=False)
+    assert st[300] == gfk._native.EARG and (st == stw).all()
+    assert (got[300] == 0).all() and np.abs(got[:300] - want[:300]).max() <= 1e-11 * np.abs(want).max()
