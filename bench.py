@@ -589,7 +589,8 @@ def run_disp(args, gfk, torch, rank, world, local):
             "config": {"workload": f"disp: graded soil (10 layers over a half-space), {len(freqs)} frequencies "
                                    f"2-200 Hz, 2000-sample scan, tolerance 1e-10; {roots} roots per step"},
             "e2e": {"value": len(freqs) * args.steps * world / t, "unit": "frequencies/s",
-                    "h2d_bytes_per_step": len(freqs) * 8 + len(stack) * 48, "d2h_bytes_per_step": len(freqs) * 68 * 8},
+                    "h2d_bytes_per_step": len(freqs) * 8 + len(stack) * 48,
+                    "d2h_bytes_per_step": len(freqs) * (64 * 8 + 4)},  # modes_many's [nf][64] roots + counts
             "gpu_launches": args.steps,
             "roofline": {"bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
                          "frac": ach / fp64_peak, "traffic": None,
