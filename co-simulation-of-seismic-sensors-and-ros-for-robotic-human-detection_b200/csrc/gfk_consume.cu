@@ -15,8 +15,9 @@
 //              inverse-transformed (1/n), the first `length` samples kept.
 //
 // One thread per bin builds the tables (the unwrap is sequential in range);
-// one block per query range builds its spectrum in shared memory and runs the
-// n-point FFT there (gfk_fft.cuh), n = the bank's Samples <= 4096.
+// one block per query range builds its half spectrum in shared memory and runs
+// the inverse real transform there as an n/2-point complex FFT (gfk_fft.cuh),
+// n = the bank's Samples <= 4096.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -75,17 +76,23 @@ struct ImpulseArgs {
     double* out;            // [nq][length]
 };
 
+// The inverse real transform of the half spectrum H_0..H_m (m = n/2) as one
+// complex transform of size m (the even/odd split of the output): with
+// w = e^{2 pi i / n},
+//   Z_k = (H_k + conj(H_{m-k})) + i w^k (H_k - conj(H_{m-k})),  k < m,
+//   z = IDFT_m(Z) / n  gives  y_2j = Re z_j,  y_2j+1 = Im z_j,
+// and IDFT_m(Z) = conj(DFT_m(conj Z)). Shared memory: m + 1 values.
 __global__ void __launch_bounds__(kThreads) k_impulse(ImpulseArgs a) {
-    extern __shared__ cd x[];  // [n], the spectrum in bit-reversed order, then the transform
+    extern __shared__ cd x[];  // [m + 1]: H, then conj(Z) (bit-reversed), then its transform
     const int q = blockIdx.x;
-    const int n = a.n;
-    const int logn = 31 - __clz(n);
+    const int n = a.n, m = n / 2;
+    const int logm = 31 - __clz(m);
     const int lo = a.lo[q];
     const int hi = a.count == 1 ? lo : lo + 1;
     const double frac = a.frac[q];
     const double nyq = a.fs / 2, taper_from = 0.8 * nyq;
     const double pi = 3.14159265358979323846;
-    for (int k = threadIdx.x; k <= n / 2; k += blockDim.x) {
+    for (int k = threadIdx.x; k <= m; k += blockDim.x) {
         cd h = mk(0.0);
         const double f = k * a.fs / n;
         if (k > 0 && k < a.bins) {
@@ -95,20 +102,46 @@ __global__ void __launch_bounds__(kThreads) k_impulse(ImpulseArgs a) {
                 const double ph = a.phase[i0] + frac * (a.phase[i1] - a.phase[i0]);
                 double sn, cs;
                 sincos(ph, &sn, &cs);
-                const double m = exp(lm);
-                h = mk(m * cs, m * sn);
+                const double mg = exp(lm);
+                h = mk(mg * cs, mg * sn);
                 if (a.velocity) h = mk(0.0, 2.0 * pi * f) * h;
                 if (a.sensor) h = h * a.sensor[k];
             }
             if (f > taper_from) h = h * (0.5 * (1.0 + cos(pi * (f - taper_from) / (nyq - taper_from))));
         }
-        if (k == 0 || k == n / 2) h.im = 0.0;  // the real transform reads only their real parts
-        x[bitrev(k, logn)] = mk(h.re, -h.im);  // conj of the Hermitian extension
-        if (k > 0 && k < n / 2) x[bitrev(n - k, logn)] = h;
+        if (k == 0 || k == m) h.im = 0.0;  // the real transform reads only their real parts
+        x[k] = h;
     }
     __syncthreads();
-    fft_pow2_dit_inplace(x, n, a.tw);
-    for (int t = threadIdx.x; t < a.length; t += blockDim.x) a.out[(size_t)q * a.length + t] = x[t].re / n;
+    // conj(Z_k) and conj(Z_{m-k}) by the thread that owns the pair (k, m - k)
+    for (int k = threadIdx.x; k <= m / 2; k += blockDim.x) {
+        const int k2 = m - k;
+        const cd hk = x[k], hk2 = x[k2];
+        const cd wk = mk(a.tw[k].re, -a.tw[k].im);  // e^{2 pi i k / n}
+        const cd zk = (hk + mk(hk2.re, -hk2.im)) + cmul_i(wk * (hk - mk(hk2.re, -hk2.im)));
+        x[k] = mk(zk.re, -zk.im);
+        if (k > 0 && k < m / 2) {
+            const cd wk2 = mk(a.tw[k2].re, -a.tw[k2].im);
+            const cd zk2 = (hk2 + mk(hk.re, -hk.im)) + cmul_i(wk2 * (hk2 - mk(hk.re, -hk.im)));
+            x[k2] = mk(zk2.re, -zk2.im);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; logm > 0 && i < m; i += blockDim.x) {  // into bit-reversed order
+        const int r = bitrev(i, logm);
+        if (i < r) {
+            const cd t = x[i];
+            x[i] = x[r];
+            x[r] = t;
+        }
+    }
+    __syncthreads();
+    fft_pow2_dit_inplace(x, m, a.tw, n);
+    const double inv = 1.0 / n;
+    for (int t = threadIdx.x; t < a.length; t += blockDim.x) {
+        const cd w = x[t >> 1];
+        a.out[(size_t)q * a.length + t] = ((t & 1) ? -w.im : w.re) * inv;
+    }
 }
 
 }  // namespace consume
@@ -251,7 +284,7 @@ int gfk_bank_impulse_responses(gfk_ctx* ctx, const float* payload, int32_t count
         CS_CUDA(ctx, cudaMallocAsync(&d_sensor.p, (size_t)bins * 2 * sizeof(double), s));
         CS_CUDA(ctx, cudaMemcpyAsync(d_sensor.p, sensor, (size_t)bins * 2 * sizeof(double), cudaMemcpyHostToDevice, s));
     }
-    const size_t smem = (size_t)samples * sizeof(cd);
+    const size_t smem = (size_t)(samples / 2 + 1) * sizeof(cd);
     if (smem > 48 * 1024)
         CS_CUDA(ctx, cudaFuncSetAttribute(gfk::consume::k_impulse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
@@ -395,7 +428,7 @@ int gfk_bank_device_impulse_responses(gfk_bank_dev* b, const double* ranges, int
         if (int st = grow(ctx, &b->d_out, &b->out_cap, (size_t)nq * length)) return st;
         dst = b->d_out;
     }
-    const size_t smem = (size_t)b->samples * sizeof(cd);
+    const size_t smem = (size_t)(b->samples / 2 + 1) * sizeof(cd);
     if (smem > 48 * 1024)
         CS_CUDA(ctx, cudaFuncSetAttribute(gfk::consume::k_impulse, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));

@@ -39,9 +39,12 @@ __device__ inline cd* fft_pow2(cd* x, cd* y, int n, const cd* __restrict__ tw) {
 // input in bit-reversed order (element k at index bitrev(k)); the forward
 // transform (e^{-i}) ends in x in natural order. Half the shared memory of
 // fft_pow2; every thread of the block must call it.
-__device__ inline void fft_pow2_dit_inplace(cd* x, int n, const cd* __restrict__ tw) {
+__device__ inline void fft_pow2_dit_inplace(cd* x, int n, const cd* __restrict__ tw, int tw_n = 0) {
+    // tw holds e^{-2 pi i m / tw_n}, m < tw_n / 2 (tw_n = n by default; a
+    // multiple of n reuses a larger transform's table)
+    const int tn = tw_n > 0 ? tw_n : n;
     for (int len = 2; len <= n; len <<= 1) {
-        const int half = len >> 1, step = n / len;
+        const int half = len >> 1, step = tn / len;
         for (int j = threadIdx.x; j < n / 2; j += blockDim.x) {
             const int pos = j & (half - 1);
             const int i0 = ((j - pos) << 1) + pos;
