@@ -17,9 +17,10 @@
 // Modes (disp.go:62-103, bisect disp.go:194-217): the secular function on
 // samples + 1 evenly spaced velocities in [0.85 Vs_min, Vs_halfspace (1 - 1e-9)]
 // (all threads), the sign changes between defined neighbours in order (one
-// thread), and one bisection per bracket (one thread each) with the
-// reference's stopping rules; a bracket whose bisection meets an undefined
-// value yields no root, as in the reference.
+// thread), and one bisection per bracket (a group of lanes each, evaluating
+// several steps' midpoints at once, below) with the reference's stopping
+// rules; a bracket whose bisection meets an undefined value yields no root, as
+// in the reference.
 #include <cmath>
 #include <vector>
 
@@ -31,7 +32,11 @@ namespace gfk {
 namespace disp {
 
 constexpr int kMaxLayers = 64;
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;
+constexpr int kSpecDepth = 3;                        // bisection steps per round
+constexpr int kSpecNodes = (1 << kSpecDepth) - 1;    // midpoints evaluated per round
+constexpr int kSpecLanes = 8;                        // lanes per bracket (a power of two > kSpecNodes)
+static_assert(kSpecLanes > kSpecNodes && 32 % kSpecLanes == 0, "bracket groups tile a warp");
 constexpr int kMaxModes = 64;
 constexpr int kMaxSamples = 16384;
 
@@ -209,36 +214,74 @@ __global__ void __launch_bounds__(kThreads) k_modes(const __grid_constant__ Stac
     }
     __syncthreads();
     const int nb = nbr < kMaxModes ? nbr : kMaxModes;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-        const int i = br[b];
-        double lo = i - 1 == 0 ? a.lo : a.lo + (double)(i - 1) * step;
-        double hi = a.lo + (double)i * step;
-        double flo;
-        double r = -1.0;  // no root
-        if (secular_c(st, freq, lo, &flo)) {
-            bool done = false;
-            for (int it = 0; it < 200 && !done; it++) {
+    // Bisection, kSpecDepth steps per round: the kSpecNodes lanes of a group
+    // evaluate every midpoint the next kSpecDepth steps could visit (a complete
+    // binary tree of brackets, each computed by the same halvings the
+    // sequential search would make), then each lane walks the path the
+    // sequential search takes through them. The midpoints, the decisions and
+    // the stopping rules are those of the one-thread search, so the roots are
+    // the same doubles; the dependent chain is kSpecDepth times shorter.
+    const int lane = threadIdx.x & 31, grp = lane / kSpecLanes, node = lane % kSpecLanes;
+    const int groups = (blockDim.x / 32) * (32 / kSpecLanes);
+    const int gid = (threadIdx.x / 32) * (32 / kSpecLanes) + grp;
+    for (int b0 = 0; b0 < nb; b0 += groups) {
+        const int b = b0 + gid;
+        const bool active = b < nb;
+        double lo = 0.0, hi = 0.0, flo = 0.0, r = -1.0;
+        bool done = !active;
+        if (active) {
+            const int i = br[b];
+            lo = i - 1 == 0 ? a.lo : a.lo + (double)(i - 1) * step;
+            hi = a.lo + (double)i * step;
+            flo = vals[i - 1];  // the scan's value at this very velocity (defined: a bracket end)
+        }
+        int it = 0;
+        while (__any_sync(0xffffffffu, !done)) {
+            // this lane's tree node: heap index h = node + 1 at depth floor(log2 h)
+            double v = 0.0;
+            int vok = 0;
+            if (!done && node < kSpecNodes) {
+                const int h = node + 1, d = 31 - __clz(h);
+                double nlo = lo, nhi = hi;
+                for (int sh = d - 1; sh >= 0; sh--) {
+                    const double mid = 0.5 * (nlo + nhi);
+                    if ((h >> sh) & 1) nlo = mid; else nhi = mid;
+                }
+                vok = secular_c(st, freq, 0.5 * (nlo + nhi), &v) ? 1 : 0;
+            }
+            int h = 1;
+            for (int step_ = 0; step_ < kSpecDepth; step_++) {
+                const int src = (lane & ~(kSpecLanes - 1)) + (h - 1);
+                const double hv = __shfl_sync(0xffffffffu, v, src);
+                const int hok = __shfl_sync(0xffffffffu, vok, src);
+                if (done) continue;
+                if (it >= 200) {
+                    r = 0.5 * (lo + hi);
+                    done = true;
+                    continue;
+                }
                 const double mid = 0.5 * (lo + hi);
                 if (mid == lo || mid == hi || (hi - lo) < a.tol * mid) {
                     r = mid;
                     done = true;
-                    break;
+                    continue;
                 }
-                double v;
-                if (!secular_c(st, freq, mid, &v)) {
+                it++;
+                if (!hok) {
                     done = true;  // undefined inside the bracket: no root
-                    break;
+                    continue;
                 }
-                if (sign_change(flo, v)) {
+                if (sign_change(flo, hv)) {
                     hi = mid;
+                    h = 2 * h;
                 } else {
                     lo = mid;
-                    flo = v;
+                    flo = hv;
+                    h = 2 * h + 1;
                 }
             }
-            if (!done) r = 0.5 * (lo + hi);
         }
-        root[b] = r;
+        if (active && node == 0) root[b] = r;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
