@@ -433,6 +433,13 @@ def test_pinned_bank_download_overlaps_and_matches(gfk, engine):
         assert per_bin.max() < 1e-11, per_bin.max()
         got2, _ = m.bank_spectra(wl.ranges, wl.freqs, wl.integration(), out=pinned)
         assert np.array_equal(got, got2)
+    # per-frequency grids (GridFor): the sequential per-row sum, so chunking changes nothing
+    m = gfk.Medium(wl.stack, formulation=gfk.DUNKIN, omega_imag=wl.omega_imag, engine=engine)
+    f2 = wl.freqs[:256]
+    want, _ = m.bank_spectra(wl.ranges, f2)
+    pinned2 = torch.zeros((len(f2), 2 * len(wl.ranges)), dtype=torch.float64, pin_memory=True).numpy()
+    got, st = m.bank_spectra(wl.ranges, f2, out=pinned2)
+    assert (st == 0).all() and np.array_equal(got, want)
     freqs = wl.freqs.copy()
     freqs[300] = -5.0
     m = wl.medium(gfk.DUNKIN, engine=engine)
