@@ -202,12 +202,13 @@ def propagated_layers(stack, freqs, omega_imag, k, ref_freq=30.0, default_q=0.0)
 
 def cpu_baseline(gfk, wl, threads, target_s=15.0):
     """The oracle's restatement of the reference algorithm (reference-direct:
-    Qp = 2.25 Qs, real frequency, guard) on a bounded sample of the workload:
-    all ranges, the full wavenumber grid, frequencies from the band the
-    reference answers, on `threads` host threads."""
+    Qp = 2.25 Qs, real frequency, guard), compiled -O3 -march=native for this
+    host, on a bounded sample of the workload: all ranges, the full wavenumber
+    grid, frequencies from the band the reference answers, on `threads` host
+    threads (one frequency per thread at a time, as geobank's goroutines)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
-    O.build()
+    timed, flags = O.timed_lib()
     st = [(l.thickness, l.vp, l.vs, l.density, l.qs, 0.0) for l in wl.stack]
     m = O.OracleMedium(st)
     answered = np.array([O.check_layer_phase(m, f) == 0 for f in wl.freqs])
@@ -215,19 +216,62 @@ def cpu_baseline(gfk, wl, threads, target_s=15.0):
     # one probe frequency per thread to size the sample
     probe = band[np.linspace(0, len(band) - 1, threads).astype(int)]
     t0 = time.perf_counter()
-    O.bank_spectra(m, wl.ranges, probe, samples=wl.samples, kmax=wl.kmax, threads=threads)
+    O.bank_spectra(m, wl.ranges, probe, samples=wl.samples, kmax=wl.kmax, threads=threads, library=timed)
     per_round = time.perf_counter() - t0
     rounds = max(1, int(target_s / max(per_round, 1e-3)))
     sample = band[np.linspace(0, len(band) - 1, min(len(band), rounds * threads)).astype(int)]
     t0 = time.perf_counter()
-    _, status = O.bank_spectra(m, wl.ranges, sample, samples=wl.samples, kmax=wl.kmax, threads=threads)
+    _, status = O.bank_spectra(m, wl.ranges, sample, samples=wl.samples, kmax=wl.kmax, threads=threads,
+                               library=timed)
     dt = time.perf_counter() - t0
     cells = len(sample) * len(wl.ranges)
-    return {"value": cells / dt, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": cells / dt, "unit": UNIT, "cores": threads, "threads": threads, "kind": "port",
+            "flags": flags, "bins_sampled": int(len(sample)), "bins_answered": int(len(band)),
+            "band": "reference parity band: the bins the reference's MaxLayerPhase guard answers "
+                    f"({band.min():.2f}-{band.max():.2f} Hz of {wl.freqs.min():.2f}-{wl.freqs.max():.2f} Hz)",
             "sample": f"{len(sample)} of the {len(band)} bins the reference answers (<= guard), all "
                       f"{len(wl.ranges)} ranges, {wl.samples} wavenumbers, reference-direct restatement "
-                      f"(oracle/gfk_oracle.c), {dt:.1f} s",
+                      f"(oracle/gfk_oracle.c built {flags}), {dt:.1f} s on {threads} threads",
             "status_ok": bool((status == 0).all())}
+
+
+def cpu_baseline_batched(soils, ranges, nk, kmax, threads, target_s=12.0, nsample=8):
+    """The same restatement on the uneven soils: `nsample` soils spread over
+    the seeded list, for each the bins the reference's guard answers, sampled
+    so the whole leg takes about target_s on `threads` host threads."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    timed, flags = O.timed_lib()
+    picks = [soils[i] for i in np.linspace(0, len(soils) - 1, nsample).astype(int)]
+    cases = []
+    for st, fr in picks:
+        m = O.OracleMedium([(l.thickness, l.vp, l.vs, l.density, l.qs, 0.0) for l in st])
+        band = fr[np.array([O.check_layer_phase(m, f) == 0 for f in fr])]
+        if len(band):
+            cases.append((m, band))
+    # size the sample with one round of `threads` bins of the first soil
+    m0, b0 = cases[0]
+    probe = b0[np.linspace(0, len(b0) - 1, threads).astype(int)]
+    t0 = time.perf_counter()
+    O.bank_spectra(m0, ranges, probe, samples=nk, kmax=kmax, threads=threads, library=timed)
+    per_bin = (time.perf_counter() - t0) / len(probe) * threads
+    per_soil = max(threads, int(target_s / max(per_bin, 1e-6) * threads / len(cases)))
+    cells, bins, dt, ok = 0, 0, 0.0, True
+    for m, band in cases:
+        sample = band[np.linspace(0, len(band) - 1, min(len(band), per_soil)).astype(int)]
+        t0 = time.perf_counter()
+        _, status = O.bank_spectra(m, ranges, sample, samples=nk, kmax=kmax, threads=threads, library=timed)
+        dt += time.perf_counter() - t0
+        cells += len(sample) * len(ranges)
+        bins += len(sample)
+        ok &= bool((status == 0).all())
+    return {"value": cells / dt, "unit": UNIT, "cores": threads, "threads": threads, "kind": "port",
+            "flags": flags, "bins_sampled": bins, "soils_sampled": len(cases),
+            "band": "reference parity band per soil: the bins the reference's MaxLayerPhase guard answers",
+            "sample": f"{bins} bins of {len(cases)} of the soils (evenly spread over the seeded list), all "
+                      f"{len(ranges)} ranges, {nk} wavenumbers, reference-direct restatement "
+                      f"(oracle/gfk_oracle.c built {flags}), {dt:.1f} s on {threads} threads",
+            "status_ok": ok}
 
 
 def run_reference(args):
@@ -276,6 +320,148 @@ def config_of(wl, note):
                         f"{wl.ranges[0]:g}-{wl.ranges[-1]:g} m, w_I = pi/T",
             "soils": 1, "frequencies": len(wl.freqs), "wavenumbers": wl.samples, "ranges": len(wl.ranges),
             "cells_per_step": wl.cells(), "l2": l2, "note": note}
+
+
+# DRAM traffic of one graded-soil propagator launch per frequency it
+# processes (dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture,
+# divided by the captured launch's frequencies).
+PROP_TRAFFIC_BYTES_PER_FREQ = (1305600 + 231434496 + 1118208 + 228752896) / 2 / 1024
+PROP_TRAFFIC_SOURCE = ("ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, 2 launches) of k_prop on every "
+                       "other frequency of the graded soil (1024 x 16384, a 268 MB integrand > L2), scaled by "
+                       "frequencies")
+
+
+def dev_view(torch, ptr, count, local):
+    """A float64 torch tensor over `count` doubles of libgfk device memory
+    (no copy)."""
+    class _Buf:
+        __cuda_array_interface__ = {"shape": (count,), "typestr": "<f8", "data": (ptr, False), "version": 3}
+    return torch.as_tensor(_Buf(), device=f"cuda:{local}")
+
+
+def batched_leg(gfk, torch, eng, local, rank, world, fp64_peak, steps=3, cpu=True):
+    """The 4096 seeded uneven soils (256-2048 bins each, 8192 wavenumbers, 128
+    ranges; this rank's share) as one batch plan with the split sum, for the
+    default bench line: device-resident throughput (one CUDA graph per
+    execute, stream span), end to end from host media into pinned host
+    memory, the split sum's rel-L2 against the FP64 sum of the same bank per
+    soil, the propagator's roofline and a CPU baseline on a sample."""
+    soils, ranges, nk, kmax = gfk.workloads.batched_soils()
+    mine = gfk.workloads.shard(soils, rank, world)
+    opt = gfk.Integration(nk, 0.0, kmax)
+    freqs = [fr for _, fr in mine]
+    rows = [len(fr) for fr in freqs]
+    nrows = sum(rows)
+    nr = len(ranges)
+    cells = nrows * nr
+
+    def media(quad):
+        return [gfk.Medium(st, formulation=gfk.DUNKIN, quadrature=quad, engine=eng) for st, _ in mine]
+
+    gstream = torch.cuda.ExternalStream(eng.stream(), device=f"cuda:{local}")
+    t0 = time.perf_counter()
+    plan = gfk.Batch(media(gfk.SPLIT_INT8), freqs, ranges, opt, engine=eng)
+    build_s = time.perf_counter() - t0
+    plan.execute()  # first execute: launch-shape tuning and the Hankel weights
+    plan.kernel_times(reset=True)
+    plan.execute()  # one execute timed kernel by kernel
+    prop_ms, quad_ms, other_ms = plan.kernel_times(reset=True)
+    plan.use_graph(True)
+    plan.execute()  # captures the graph
+    torch.cuda.synchronize()
+    launches0 = eng.kernel_launches()
+    spans = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    barrier(world)
+    with torch.cuda.stream(gstream):
+        for a, b in spans:
+            a.record(gstream)
+            plan.execute()
+            b.record(gstream)
+    torch.cuda.synchronize()
+    launches = eng.kernel_launches() - launches0
+    step_ms = allmax(sum(a.elapsed_time(b) for a, b in spans) / steps, world)
+    cells_all = cells * world
+    value = cells_all / (step_ms * 1e-3)
+
+    # the split sum against the FP64 sum of the same integrand, per soil, on the device
+    pp = gfk.Batch(media(gfk.PLAIN_FP64), freqs, ranges, opt, engine=eng)
+    pp.execute()
+    st_split, st_plain = plan.statuses(), pp.statuses()
+    torch.cuda.synchronize()
+    gs = dev_view(torch, plan.result_device_ptr(), nrows * nr * 2, local).view(nrows, nr * 2)
+    gp = dev_view(torch, pp.result_device_ptr(), nrows * nr * 2, local).view(nrows, nr * 2)
+    num = torch.empty(nrows, dtype=torch.float64, device=gs.device)
+    den = torch.empty_like(num)
+    for r0 in range(0, nrows, 1 << 18):
+        r1 = min(nrows, r0 + (1 << 18))
+        num[r0:r1] = (gs[r0:r1] - gp[r0:r1]).square().sum(1)
+        den[r0:r1] = gp[r0:r1].square().sum(1)
+    soil_of = torch.as_tensor(np.repeat(np.arange(len(rows)), rows), device=gs.device)
+    snum = torch.zeros(len(rows), dtype=torch.float64, device=gs.device).index_add_(0, soil_of, num)
+    sden = torch.zeros_like(snum).index_add_(0, soil_of, den)
+    per_soil = (snum / sden).sqrt().cpu().numpy()
+    per_row = (num / den).sqrt()
+    accuracy = {"relL2_split_vs_fp64_per_soil": {"max": float(per_soil.max()),
+                                                  "median": float(np.median(per_soil)),
+                                                  "worst_soil": int(np.argmax(per_soil))},
+                "relL2_whole_bank": float((num.sum() / den.sum()).sqrt()),
+                "max_row_relL2": float(per_row.max()),
+                "soils_over_1e-6": int((per_soil > 1e-6).sum()),
+                "statuses_ok": bool((st_split == 0).all() and (st_plain == 0).all())}
+    del gs, gp, num, den, per_row
+    pp.close()
+
+    # end to end: host media and grids in, the FP64 rows back into pinned host memory
+    host_rows = torch.empty(nrows * nr * 2, dtype=torch.float64, pin_memory=True).numpy()
+    host_rows = host_rows.view(np.complex128).reshape(nrows, nr)
+    barrier(world)
+    t0 = time.perf_counter()
+    e2e_plan = gfk.Batch(media(gfk.SPLIT_INT8), freqs, ranges, opt, engine=eng)
+    e2e_plan.execute()
+    e2e_plan.download(out=host_rows)
+    e2e_s = allmax(time.perf_counter() - t0, world)
+    e2e_plan.close()
+    layers = sum(len(st) for st, _ in mine)
+    plan.close()
+
+    # the propagator's roofline: fixed count (every finite layer) and the
+    # layers actually propagated, sampled on every 16th soil's grid
+    flops = sum(len(fr) * nk * (700 * (len(st) - 1) + 300) for st, fr in mine)
+    kgrid = np.arange(1, nk + 1) * (kmax / nk)
+    en = ed = 0.0
+    for st, fr in mine[::16]:
+        lx = propagated_layers(st, fr[::8], 0.0, kgrid[::32])
+        en += len(fr) * (700 * lx + 300)
+        ed += len(fr) * (700 * (len(st) - 1) + 300)
+    exec_ratio = en / ed if ed else 1.0
+    ach = flops * exec_ratio / (prop_ms * 1e-3) / 1e12
+    out = {"workload": f"batched_soils: {len(soils)} seeded soils (2-12 entries, Vs log-U 80-600, Vp/Vs U 1.7-3.0, "
+                       f"rho U 1500-2200, Qs U 10-60, Qp 2Qs, h log-U 0.2-5 m), 256-2048 bins each over 0-500 Hz, "
+                       f"{nk} wavenumbers to {kmax:.1f} rad/m, {nr} ranges 1-128 m, real frequencies; split sum; "
+                       "one CUDA graph per execute",
+           "value": value, "unit": UNIT, "ms_per_step": step_ms, "steps": steps, "warmup": 3,
+           "timing": "stream span of each graph launch (CUDA events on libgfk's stream), mean over the steps, max "
+                     "over ranks; the 9.7 GB result and the 4 GB integrand chunks exceed L2, so no flush",
+           "soils_per_rank": len(mine), "rows_per_rank": nrows, "cells_per_step": cells_all,
+           "plan_build_s": build_s, "gpu_launches": launches,
+           "kernel_ms": {"propagator": prop_ms, "quadrature": quad_ms, "other": other_ms},
+           "e2e": {"value": cells_all / e2e_s, "unit": UNIT, "s_per_step": e2e_s, "steps": 1,
+                   "h2d_bytes_per_step": layers * 48 + nrows * 8,
+                   "d2h_bytes_per_step": nrows * nr * 16 + nrows * 4,
+                   "note": "plan build from host media, execute, download into pinned host memory"},
+           "accuracy": accuracy,
+           "roofline": {"bound": "fp64", "kernel": "k_prop (Dunkin propagator)", "achieved": ach,
+                        "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach / fp64_peak, "traffic": None,
+                        "work": "executed: 700 flops per finite layer actually propagated + 300 per (f, k), the "
+                                "propagated share sampled on every 16th soil",
+                        "executed_share_of_fixed_count": exec_ratio,
+                        "fixed_count": {"tflops": flops / (prop_ms * 1e-3) / 1e12,
+                                        "frac": flops / (prop_ms * 1e-3) / 1e12 / fp64_peak}}}
+    if cpu:
+        cb = cpu_baseline_batched(soils, ranges, nk, kmax, os.cpu_count() or 1)
+        cb.pop("status_ok", None)
+        out["cpu_baseline"] = cb
+    return out
 
 
 def run_batched(args, gfk, torch, rank, world, local):
@@ -748,6 +934,8 @@ def main():
     ap.add_argument("--save-nets", default="", help="directory to save the trained members")
     ap.add_argument("--quadrature", default="split", choices=["split", "fp64"],
                     help="split: exact int8-slice tensor-core sum (default); fp64: the plain FP64 sum")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="default workload: skip the batched uneven-soils object in the line")
     ap.add_argument("--profile", action="store_true",
                     help="profiling only: skip the e2e leg, the FP64 peak probe and the CPU baseline")
     args = ap.parse_args()
@@ -780,6 +968,9 @@ def main():
     quad = gfk.PLAIN_FP64 if args.quadrature == "fp64" else gfk.SPLIT_INT8
     med = wl.medium(gfk.DUNKIN, engine=eng, quadrature=quad)
     plan = gfk.Plan(med, wl.ranges, wl.freqs, wl.integration(), engine=eng)
+    # libgfk queues its work on its own (non-blocking) stream: the L2 flush
+    # and the span events go on that stream, in order with the kernels
+    gstream = torch.cuda.ExternalStream(eng.stream(), device=f"cuda:{local}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     for _ in range(max(args.warmup, 0)):
@@ -789,25 +980,29 @@ def main():
     plan.kernel_times(reset=True)
     variant, tune_ms = plan.tuning()
 
-    # --- device-resident timing -----------------------------------------
+    # --- device-resident timing: the stream span of each execute ----------
     clocks = ClockSampler(local)
     clocks.start()
     launches0 = eng.kernel_launches()
+    spans = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier(world)
     torch.cuda.synchronize()
     t_wall = time.perf_counter()
-    step_ms = 0.0
-    for _ in range(args.steps):
-        flush.fill_(1)
-        plan.execute()
+    with torch.cuda.stream(gstream):
+        for a, b in spans:
+            flush.fill_(1)
+            a.record(gstream)
+            plan.execute()
+            b.record(gstream)
     torch.cuda.synchronize()
     barrier(world)
     wall = time.perf_counter() - t_wall
     launches = eng.kernel_launches() - launches0
     prop_ms, quad_ms, other_ms = plan.kernel_times(reset=True)
-    step_ms = prop_ms + quad_ms + other_ms
+    kernel_sum_ms = prop_ms + quad_ms + other_ms
+    span_ms = sum(a.elapsed_time(b) for a, b in spans) / max(args.steps, 1)
     clk = clocks.stop()
-    step_ms = allmax(step_ms, world)
+    step_ms = allmax(span_ms, world)
     cells_all = wl.cells() * world
     value = cells_all / (step_ms * 1e-3)
 
@@ -857,15 +1052,20 @@ def main():
         rel = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
         per_bin = float(np.max(np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)))
         pp.kernel_times(reset=True)
-        for _ in range(args.steps):
-            flush.fill_(1)
-            pp.execute()
+        pspans = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(args.steps)]
+        with torch.cuda.stream(gstream):
+            for a, b in pspans:
+                flush.fill_(1)
+                a.record(gstream)
+                pp.execute()
+                b.record(gstream)
         torch.cuda.synchronize()
         pprop, pquad, pother = pp.kernel_times(reset=True)
-        pms = allmax(pprop + pquad + pother, world)
+        pms = allmax(sum(a.elapsed_time(b) for a, b in pspans) / max(args.steps, 1), world)
         plain_leg = {"value": cells_all / (pms * 1e-3), "unit": UNIT, "ms_per_step": pms,
                      "kernel_ms": {"propagator": pprop, "quadrature": pquad, "other": pother},
-                     "split_over_plain": (cells_all / (step_ms * 1e-3)) / (cells_all / (pms * 1e-3)),
+                     "split_over_plain": pms / step_ms,
                      "relL2_split_vs_fp64": rel, "max_bin_relL2_split_vs_fp64": per_bin}
         pp.close()
 
@@ -875,35 +1075,35 @@ def main():
     lfin = nl - 1
     f_prop = len(f) * wl.samples * (700 * lfin + 300)   # algorithmic FP64 flops per propagator launch
     f_quad = 4 * len(f) * wl.samples * len(r)           # complex x real MAC, per quadrature launch
-    if prop_ms >= quad_ms:
-        dom, ach = "k_prop (Dunkin propagator)", f_prop / (prop_ms * 1e-3) / 1e12
-    else:
-        dom, ach = ("k_quad_gemm (FP64 wavenumber sum)" if quad == gfk.PLAIN_FP64 else
-                    "k_quad_tc (tensor-core wavenumber sum)"), f_quad / (quad_ms * 1e-3) / 1e12
-    # DRAM bytes of one propagator launch: the ncu capture of the graded soil's
-    # every-8th-frequency case (dram__bytes_read + _write = 0.29 + 11.78 MB for
-    # 256 frequencies), scaled by the frequencies one full launch processes
-    traffic, traffic_src = None, None
-    if args.workload != "single" and args.freq_stride == 1 and prop_ms >= quad_ms:
-        traffic = (0.292352e6 + 11.778048e6) * len(f) / 256
-        traffic_src = ("ncu capture of k_prop on 256 of the 2048 frequencies (profiles/k_prop_dunkin_graded_soil.md),"
-                       " scaled by frequencies; the integrand's 16 B per (f, k) mostly stays in L2")
-    roof_time = (f_prop + f_quad) / (fp64_peak * 1e12)
     kgrid = np.arange(1, wl.samples + 1) * (wl.kmax / wl.samples)
     l_exec = propagated_layers(wl.stack, wl.freqs[::8], wl.omega_imag, kgrid[::8])
     f_exec = len(f) * wl.samples * (700 * l_exec + 300)
+    if prop_ms >= quad_ms:
+        dom, ach = "k_prop (Dunkin propagator)", f_exec / (prop_ms * 1e-3) / 1e12
+    else:
+        dom, ach = ("k_quad_gemm (FP64 wavenumber sum)" if quad == gfk.PLAIN_FP64 else
+                    "k_quad_tc (tensor-core wavenumber sum)"), f_quad / (quad_ms * 1e-3) / 1e12
+    # DRAM bytes of one propagator launch, from an ncu capture of the graded
+    # soil's every-other-frequency case (its 268 MB integrand exceeds L2),
+    # scaled by the frequencies one full launch processes
+    traffic, traffic_src = None, None
+    if args.workload != "single" and args.freq_stride == 1 and prop_ms >= quad_ms:
+        traffic = PROP_TRAFFIC_BYTES_PER_FREQ * len(f)
+        traffic_src = PROP_TRAFFIC_SOURCE
+    roof_time = (f_prop + f_quad) / (fp64_peak * 1e12)
     roofline = {"bound": "fp64", "kernel": dom, "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": ach / fp64_peak, "traffic": traffic, "traffic_source": traffic_src,
+                "work": "executed: 700 flops per finite layer actually propagated (the thick-layer start skips "
+                        "layers beneath the shallowest isolating one) + 300 per (f, k)",
                 "peak_source": "measured here: cuBLAS FP64 GEMM 8192^3 best of 5 (MEASURED_PEAKS.json has no FP64 "
                                "figure)",
-                "algorithmic_flops": {"propagator": f_prop, "quadrature": f_quad},
+                "algorithmic_flops": {"propagator_fixed": f_prop, "propagator_executed": f_exec,
+                                      "quadrature": f_quad},
+                "mean_layers_propagated": l_exec, "finite_layers": lfin,
+                "fixed_count": {"note": "the same launch credited with every finite layer (the survey's count)",
+                                "tflops": f_prop / (prop_ms * 1e-3) / 1e12,
+                                "frac": f_prop / (prop_ms * 1e-3) / 1e12 / fp64_peak},
                 "step_frac_of_fp64_roofline": roof_time / (step_ms * 1e-3),
-                "propagator_executed": {
-                    "note": "the solve starts at the shallowest layer whose own decay isolates the ones beneath "
-                            "(thick-layer start); the algorithmic count above assumes every finite layer",
-                    "mean_layers_propagated": l_exec, "finite_layers": lfin, "flops": f_exec,
-                    "tflops": f_exec / (prop_ms * 1e-3) / 1e12,
-                    "frac": f_exec / (prop_ms * 1e-3) / 1e12 / fp64_peak},
                 "kernel_ms": {"propagator": prop_ms, "quadrature": quad_ms, "other": other_ms},
                 "propagator_launch_shape": {"chosen": variant, "tuning_ms": tune_ms},
                 "quadrature": {"path": "split int8 slices on tcgen05 (10 slice GEMMs)" if quad == gfk.SPLIT_INT8
@@ -916,6 +1116,12 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(gfk, wl, os.cpu_count() or 1)
         cb.pop("status_ok", None)
+    plan.close()
+    del flush
+    batched = None
+    if not args.no_batched and args.workload == "graded" and args.freq_stride == 1:
+        batched = batched_leg(gfk, torch, eng, local, rank, world, fp64_peak,
+                              steps=min(args.steps, 3), cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
@@ -924,6 +1130,9 @@ def main():
                                         ("wavenumber sum as exact int8 slices on the tcgen05 tensor cores, FP64 "
                                          "recombination" if quad == gfk.SPLIT_INT8 else "FP64 wavenumber sum")),
                               parallelism=f"replicas{world}" if world > 1 else "single"),
+               "timing": {"value_is": "stream span of each execute (CUDA events on libgfk's stream around it, the "
+                                      "L2 flush outside), mean over the timed steps, max over ranks",
+                          "kernel_sum_ms_per_step": kernel_sum_ms},
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                        "ms_per_step": e2e_s * 1e3},
                "gpu_launches": launches, "clocks": clk, "roofline": roofline,
@@ -932,8 +1141,9 @@ def main():
             out["cpu_baseline"] = cb
         if plain_leg:
             out["plain_fp64"] = plain_leg
+        if batched:
+            out["batched"] = batched
         print(json.dumps(out))
-    plan.close()
     eng.close()
     if world > 1:
         import torch.distributed as dist

@@ -195,9 +195,11 @@ __global__ void __launch_bounds__(kThreads) k_modes(const __grid_constant__ Stac
     __shared__ int nbr;
     const int fi = blockIdx.x;
     const double freq = a.freqs[fi];
-    const double step = (a.hi * (1.0 - 1e-9) - a.lo) / a.samples;
+    // the scan's velocities with one rounding per operation (no contraction
+    // into FMAs), so the host can form the very same doubles: lo + i step
+    const double step = __dsub_rn(__dmul_rn(a.hi, 1.0 - 1e-9), a.lo) / a.samples;
     for (int i = threadIdx.x; i <= a.samples; i += blockDim.x) {
-        const double c = i == 0 ? a.lo : a.lo + (double)i * step;
+        const double c = i == 0 ? a.lo : __dadd_rn(a.lo, __dmul_rn((double)i, step));
         double v = 0.0;
         ok[i] = secular_c(st, freq, c, &v) ? 1 : 0;
         vals[i] = v;
@@ -231,8 +233,8 @@ __global__ void __launch_bounds__(kThreads) k_modes(const __grid_constant__ Stac
         bool done = !active;
         if (active) {
             const int i = br[b];
-            lo = i - 1 == 0 ? a.lo : a.lo + (double)(i - 1) * step;
-            hi = a.lo + (double)i * step;
+            lo = i - 1 == 0 ? a.lo : __dadd_rn(a.lo, __dmul_rn((double)(i - 1), step));
+            hi = __dadd_rn(a.lo, __dmul_rn((double)i, step));
             flo = vals[i - 1];  // the scan's value at this very velocity (defined: a bracket end)
         }
         int it = 0;

@@ -868,6 +868,8 @@ const char* gfk_last_error(const gfk_ctx* ctx) { return ctx ? ctx->last_error.c_
 
 int64_t gfk_kernel_launches(const gfk_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+void* gfk_stream(const gfk_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
 int gfk_stack_validate(const gfk_medium* m) { return validate(nullptr, m); }
 
 int gfk_check_layer_phase(const gfk_medium* m, double freq_hz) { return check_layer_phase(nullptr, m, freq_hz); }

@@ -17,8 +17,14 @@
 // Host code may not use the array's name as a device address; the address is
 // looked up once per device with cudaGetSymbolAddress, with that device
 // current, by the first call made on it. Make that first call before any
-// stream capture begins.
+// stream capture begins. The address belongs to the device's current CUDA
+// context: if the caller resets the device (cudaDeviceReset) or otherwise
+// replaces its primary context, the next call sees a new context ID and looks
+// the address up again, so that call is a first call too.
+#include <cuda.h>
+
 #include <cstddef>
+#include <cstring>
 #include <mutex>
 
 #include "../../include/gfk.h"
@@ -52,16 +58,49 @@ static_assert(sizeof(Scalars) <= 256, "scalar block too small");
 static_assert(offsetof(Scalars, row) % 8 == 0 && offsetof(Scalars, wc2) % 8 == 0, "alignment");
 
 std::mutex g_setup_mu;
-void* g_scratch_addr[256] = {nullptr};  // device address of the array, per device ordinal
+void* g_scratch_addr[256] = {nullptr};            // device address of the array, per device ordinal
+unsigned long long g_scratch_ctx[256] = {0};      // ID of the context that address belongs to
 
+// The current context's unique ID (cuCtxGetId, through the runtime's driver
+// entry points, so libgfk needs no -lcuda); 0 when there is none or the
+// driver cannot say.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(p);
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(p);
+        looked_up = true;
+    }
+    if (!get_current || !get_id) return 0;
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// The array's device address on `device` (current): looked up with
+// cudaGetSymbolAddress on the first call in a context, then reused while
+// that context stays current.
 int scratch_address(int device, unsigned char** out) {
     if (device < 0 || device >= 256) return GFK_ECUDA;
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_addr[device]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_scratch_addr[device] || ctx == 0 || ctx != g_scratch_ctx[device]) {
         void* ptr = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
         if (e != cudaSuccess || !ptr) return GFK_ECUDA;
         g_scratch_addr[device] = ptr;
+        g_scratch_ctx[device] = current_context_id();  // the lookup makes the primary context current
     }
     *out = static_cast<unsigned char*>(g_scratch_addr[device]);
     return GFK_OK;
@@ -158,8 +197,12 @@ extern "C" int gfk_vertical_displacement_multi_noalloc(const gfk_medium* m, cons
     ok(cudaMemcpyAsync(out, d_G, sizeof(cd) * nr, cudaMemcpyDeviceToHost, strm));
     ok(cudaMemcpyAsync(&flags, d_status, sizeof(int), cudaMemcpyDeviceToHost, strm));
     ok(cudaStreamSynchronize(strm));
-    if (e != cudaSuccess) return GFK_ECUDA;
-    if (flags & gfk::kStSingular) return GFK_ESINGULAR;
-    if (flags & gfk::kStNonfinite) return GFK_ENONFINITE;
-    return GFK_OK;
+    // a failed call leaves zeros in out, as gfk_vertical_displacement_multi
+    // does for a failed frequency, never partial or non-finite values
+    int result = GFK_OK;
+    if (e != cudaSuccess) result = GFK_ECUDA;
+    else if (flags & gfk::kStSingular) result = GFK_ESINGULAR;
+    else if (flags & gfk::kStNonfinite) result = GFK_ENONFINITE;
+    if (result != GFK_OK) std::memset(out, 0, sizeof(double) * 2 * (size_t)nr);
+    return result;
 }

@@ -256,6 +256,10 @@ class Engine:
     def kernel_launches(self):
         return int(N.lib().gfk_kernel_launches(self.ctx))
 
+    def stream(self):
+        """The context's CUDA stream handle (an integer cudaStream_t)."""
+        return int(N.lib().gfk_stream(self.ctx) or 0)
+
     def close(self):
         if self.ctx:
             for p in list(self._plans):

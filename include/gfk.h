@@ -135,6 +135,10 @@ const char *gfk_status_string(int status);
 const char *gfk_last_error(const gfk_ctx *ctx);
 /* Number of libgfk kernels launched by this context since it was opened. */
 int64_t gfk_kernel_launches(const gfk_ctx *ctx);
+/* No counterpart in the reference (Go calls are synchronous): the CUDA stream
+ * (a cudaStream_t, non-blocking) every call of this context is queued on, so
+ * a caller can order its own device work and timing events with libgfk's. */
+void *gfk_stream(const gfk_ctx *ctx);
 
 /* ---- host-only helpers (no device work) ---------------------------------- */
 /* layer.Stack.Validate (internal/layer/layer.go:53-73). */
@@ -238,9 +242,14 @@ int gfk_batch_create(gfk_ctx *ctx, const gfk_medium *media, int32_t nsoil,
  * work runs on `stream` (a cudaStream_t, NULL for the default stream) of the
  * current device and the call returns after it completes. The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) with that
- * device current; make it before any stream capture begins. All calls share
- * the array, so calls whose GPU work overlaps race and must be serialised by
- * the caller. Statuses as gfk_vertical_displacement_multi; no message is kept. */
+ * device current; make it before any stream capture begins. The address is
+ * kept per device together with the ID of the CUDA context it belongs to, so
+ * after a cudaDeviceReset (a new primary context) the next call looks it up
+ * again and is a first call in that respect too. All calls share the array,
+ * so calls whose GPU work overlaps race and must be serialised by the caller.
+ * Statuses as gfk_vertical_displacement_multi; on any failure after the
+ * device work, out holds zeros, as a failed frequency does there. No message
+ * is kept. */
 #define GFK_NOALLOC_MAX_RANGES 16384
 #define GFK_NOALLOC_MAX_SAMPLES 196608
 int gfk_vertical_displacement_multi_noalloc(const gfk_medium *m, const gfk_solve *s,

@@ -66,6 +66,29 @@ def build():
 
 
 _lib = None
+_timed = None
+
+# The timed CPU baseline's build: the same source optimised for the host it
+# runs on. The parity build (Makefile) keeps -O2 -ffp-contract=off.
+TIMED_CFLAGS = ["-O3", "-march=native", "-fPIC", "-std=gnu11", "-shared"]
+
+
+def _bind(l):
+    P = ctypes.POINTER
+    d = ctypes.c_double
+    l.or_surface_response.argtypes = [P(Medium), P(Solve), d, d, P(d)]
+    l.or_static_coefficient.argtypes = [P(Medium), P(Solve), d, d, P(d)]
+    l.or_grid_for.argtypes = [P(Medium), P(d), ctypes.c_int, d, Integration, P(Grid)]
+    l.or_vertical_displacement_multi.argtypes = [P(Medium), P(Solve), P(d), ctypes.c_int, d,
+                                                 Integration, P(d)]
+    l.or_vertical_displacement.argtypes = [P(Medium), P(Solve), d, d, Integration, P(d)]
+    l.or_bank_spectra.argtypes = [P(Medium), P(Solve), P(d), ctypes.c_int, P(d), ctypes.c_int,
+                                  Integration, P(d), P(ctypes.c_int32), ctypes.c_int]
+    l.or_check_layer_phase.argtypes = [P(Medium), d]
+    l.or_validate.argtypes = [P(Medium)]
+    l.or_j0.argtypes = [d]
+    l.or_j0.restype = d
+    return l
 
 
 def lib():
@@ -73,22 +96,24 @@ def lib():
     if _lib is None:
         if not LIB_PATH.exists():
             build()
-        _lib = ctypes.CDLL(str(LIB_PATH))
-        P = ctypes.POINTER
-        d = ctypes.c_double
-        _lib.or_surface_response.argtypes = [P(Medium), P(Solve), d, d, P(d)]
-        _lib.or_static_coefficient.argtypes = [P(Medium), P(Solve), d, d, P(d)]
-        _lib.or_grid_for.argtypes = [P(Medium), P(d), ctypes.c_int, d, Integration, P(Grid)]
-        _lib.or_vertical_displacement_multi.argtypes = [P(Medium), P(Solve), P(d), ctypes.c_int, d,
-                                                        Integration, P(d)]
-        _lib.or_vertical_displacement.argtypes = [P(Medium), P(Solve), d, d, Integration, P(d)]
-        _lib.or_bank_spectra.argtypes = [P(Medium), P(Solve), P(d), ctypes.c_int, P(d), ctypes.c_int,
-                                         Integration, P(d), P(ctypes.c_int32), ctypes.c_int]
-        _lib.or_check_layer_phase.argtypes = [P(Medium), d]
-        _lib.or_validate.argtypes = [P(Medium)]
-        _lib.or_j0.argtypes = [d]
-        _lib.or_j0.restype = d
+        _lib = _bind(ctypes.CDLL(str(LIB_PATH)))
     return _lib
+
+
+def timed_lib():
+    """The oracle compiled with TIMED_CFLAGS for THIS host's CPU, into a
+    private temporary directory (a -march=native library must not travel to
+    another machine). Returns (library, flags string)."""
+    global _timed
+    if _timed is None:
+        import shutil
+        import tempfile
+        out = pathlib.Path(tempfile.mkdtemp(prefix="gfk_oracle_timed_")) / "libgfk_oracle_timed.so"
+        cc = os.environ.get("CC") or shutil.which("gcc") or "cc"
+        subprocess.run([cc, *TIMED_CFLAGS, "-o", str(out), str(HERE / "gfk_oracle.c"), "-lm", "-lpthread"],
+                       check=True)
+        _timed = (_bind(ctypes.CDLL(str(out))), " ".join(TIMED_CFLAGS))
+    return _timed
 
 
 class OracleMedium:
@@ -170,8 +195,9 @@ def vertical_displacement(medium, r, f, samples=0, kmax_factor=0.0, kmax=0.0,
 
 
 def bank_spectra(medium, ranges, freqs, samples=0, kmax_factor=0.0, kmax=0.0, formulation=REFERENCE_DIRECT,
-                 omega_imag=0.0, guard=0, threads=None):
-    """[nf, nr] complex128 and per-frequency status, threaded over frequency."""
+                 omega_imag=0.0, guard=0, threads=None, library=None):
+    """[nf, nr] complex128 and per-frequency status, threaded over frequency.
+    library: a library from timed_lib() in place of the parity build."""
     m = _medium(medium)
     r = np.ascontiguousarray(ranges, dtype=np.float64)
     f = np.ascontiguousarray(freqs, dtype=np.float64)
@@ -179,7 +205,7 @@ def bank_spectra(medium, ranges, freqs, samples=0, kmax_factor=0.0, kmax=0.0, fo
     status = np.zeros(len(f), dtype=np.int32)
     threads = threads or os.cpu_count() or 1
     P = ctypes.POINTER
-    lib().or_bank_spectra(ctypes.byref(m.c), ctypes.byref(_solve(formulation, omega_imag, guard)),
+    (library or lib()).or_bank_spectra(ctypes.byref(m.c), ctypes.byref(_solve(formulation, omega_imag, guard)),
                           r.ctypes.data_as(P(ctypes.c_double)), len(r),
                           f.ctypes.data_as(P(ctypes.c_double)), len(f), _integ(samples, kmax_factor, kmax),
                           out.ctypes.data_as(P(ctypes.c_double)), status.ctypes.data_as(P(ctypes.c_int32)),

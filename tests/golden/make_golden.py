@@ -1,9 +1,9 @@
 """Generates the committed golden fixtures under tests/golden/.
 
-Run in a container that has the reference checkout (read-only) at
-$GFK_REFERENCE (default /root/reference):
+Run where a checkout of the reference project is available (it is only
+read), with GFK_REFERENCE naming its root directory:
 
-    python tests/golden/make_golden.py
+    GFK_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 Writes:
   python_written.bank   the reference's own Python writer (py/bankfmt/bankfmt.py
@@ -34,7 +34,9 @@ import sys
 
 HERE = pathlib.Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REF = pathlib.Path(os.environ.get("GFK_REFERENCE", "/root/reference"))
+if not os.environ.get("GFK_REFERENCE"):
+    sys.exit("make_golden.py: set GFK_REFERENCE to the reference checkout's root directory")
+REF = pathlib.Path(os.environ["GFK_REFERENCE"])
 
 
 def bank_fixtures():

@@ -126,3 +126,55 @@ def test_rejects_bad_arguments(pkg, eng):
     with pytest.raises(pkg.FkError) as e:
         pkg.disp.modes(bad, 20.0, engine=eng)
     assert e.value.status == pkg._native.ESTACK
+
+
+def _sequential_roots(secular, lo, hi, samples, tol):
+    """disp.Modes' one-thread search (internal/disp/disp.go:68-196, restated in
+    oracle/disp_oracle.py): the scan's sign changes, then one bisection per
+    bracket with the reference's stopping rules, over the given secular
+    function (a callable on a list of velocities returning values and
+    defined-flags)."""
+    step = (hi * (1 - 1e-9) - lo) / samples
+    cs = [lo] + [lo + i * step for i in range(1, samples + 1)]
+    vals, ok = secular(cs)
+    roots = []
+    for i in range(1, samples + 1):
+        if not (ok[i] and ok[i - 1] and D._sign_change(vals[i - 1], vals[i])):
+            continue
+        blo, bhi, flo = cs[i - 1], cs[i], vals[i - 1]
+        root = None
+        for it in range(201):
+            mid = 0.5 * (blo + bhi)
+            if it == 200 or mid == blo or mid == bhi or (bhi - blo) < tol * mid:
+                root = mid
+                break
+            v, vok = secular([mid])
+            if not vok[0]:
+                break  # undefined inside the bracket: no root
+            if D._sign_change(flo, v[0]):
+                bhi = mid
+            else:
+                blo, flo = mid, v[0]
+        if root is not None:
+            roots.append(root)
+    return roots
+
+
+@pytest.mark.parametrize("tol", [0.0, 1e-300], ids=["default_tol", "to_the_last_bit"])
+def test_roots_equal_sequential_search_exactly(pkg, eng, tol):
+    """k_modes evaluates three bisection steps' midpoints at once and walks the
+    path the one-thread search takes; its roots must be the sequential
+    search's doubles exactly, when both use the GPU's own secular function
+    (gfk_secular). With tolerance 1e-300 every bracket runs until its midpoint
+    equals an end (~40 halvings)."""
+    for path in GOLDEN:
+        g = json.loads(path.read_text())
+        st = stack_of(pkg, g)
+        lo, hi = pkg.disp.bounds(st)
+        for f in (4.0, 37.0, 110.0):
+            def secular(cs, f=f):
+                v, ok = pkg.disp.secular_at_velocity(st, [f] * len(cs), cs, engine=eng)
+                return list(v), [bool(o) and math.isfinite(x) for o, x in zip(ok, v)]
+            want = _sequential_roots(secular, lo, hi, 2000, tol if tol > 0 else 1e-10)
+            got = pkg.disp.modes_many(st, [f], opt=pkg.disp.Search(0, tol), engine=eng)[0]
+            assert got == want, (path.stem, f, got, want)

@@ -448,3 +448,89 @@ def test_pinned_bank_download_overlaps_and_matches(gfk, engine):
     want, stw = m.bank_spectra(wl.ranges, freqs, wl.integration(), raise_on_error=False)
     assert st[300] == gfk._native.EARG and (st == stw).all()
     assert (got[300] == 0).all() and np.abs(got[:300] - want[:300]).max() <= 1e-11 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("form", [0, 1], ids=["reference_direct", "dunkin"])
+def test_layered_causality_known_answers(gfk, engine, form):
+    """TestLayeredResponseHasNoPrecursor (internal/fk/causality_test.go:45-141)
+    through libgfk: 1228 bins to 120 Hz of the 2 m layer over a half-space,
+    each on GridFor's own wavenumber grid, shaped and transformed as the
+    reference's test does. The peak times, the precursor and the negative-time
+    residue equal what the reference's run logged, to its printed digits
+    (docs/validation-report.md:278-280), in both formulations (Dunkin with the
+    reference's Qp = 2.25 Qs at real frequencies)."""
+    import causality_case as CC
+    KA = json.loads((GOLDEN / "known_answers.json").read_text())
+    st = CC.STACK if form == 0 else [tuple(l[:5]) + (2.25 * l[4],) for l in CC.STACK]
+    m = medium_of(gfk, st, default_q=CC.DEFAULT_Q, formulation=form, engine=engine)
+    _, freqs = CC.bins()
+    spectra, status = m.bank_spectra(CC.RANGES, freqs)
+    assert (status == 0).all()
+    CC.check_against_logged(CC.metrics(spectra), KA["causality_precursor"])
+
+
+@pytest.mark.parametrize("form", [0, 1], ids=["reference_direct", "dunkin"])
+def test_sls_medium_matches_oracle(gfk, engine, oracle, form):
+    """Medium.Relax: one standard linear solid replaces constant Q for P and S
+    alike (internal/fk/fk.go:44-52, 84-88, 96-102; internal/visco/visco.go:55-108),
+    on a two-layer stack. GPU against the oracle's restatement: pointwise
+    surface responses and a bank, Dunkin at a complex frequency offset."""
+    st = [(1.5, 400.0, 170.0, 1650.0, 0.0, 0.0), (3.0, 650.0, 260.0, 1850.0, 0.0, 0.0),
+          (0.0, 900.0, 420.0, 2000.0, 0.0, 0.0)]
+    sls = gfk.SLS.fit(25.0, 30.0)
+    wi = 0.0 if form == 0 else 1.5
+    m = medium_of(gfk, st, relax=sls, ref_freq=30.0, formulation=form, omega_imag=wi, engine=engine)
+    om = oracle.OracleMedium(st, ref_freq=30.0, sls=(sls.tau_sigma, sls.tau_eps))
+    rng = np.random.default_rng(3)
+    f = rng.uniform(1.0, 80.0, 200)
+    k = rng.uniform(0.01, 4.0, 200) * 2 * np.pi * f / 170.0
+    got = m.surface_response(k, f)
+    want = np.array([oracle.surface_response(om, ki, fi, form, wi) for ki, fi in zip(k, f)])
+    assert np.max(np.abs(got - want) / np.abs(want)) < (1e-6 if form == 0 else 1e-11)
+    ranges = np.arange(1.0, 33.0)
+    freqs = np.linspace(2.0, 80.0, 40)
+    kmax = 2.5 * 2 * np.pi * 80.0 / 170.0
+    opt = gfk.Integration(4096, 0.0, kmax)
+    g, gs = m.bank_spectra(ranges, freqs, opt)
+    w, ws = oracle.bank_spectra(om, ranges, freqs, samples=4096, kmax=kmax, formulation=form, omega_imag=wi)
+    assert (gs == 0).all() and (ws == 0).all()
+    assert rel_l2(g, w) < (1e-6 if form == 0 else 1e-9)
+    # the relaxation is not constant Q: the same stack at Q = 25 differs
+    mq = medium_of(gfk, [l[:4] + (25.0, 0.0) for l in st], ref_freq=30.0, formulation=form, omega_imag=wi,
+                   engine=engine)
+    gq, _ = mq.bank_spectra(ranges, freqs, opt)
+    assert rel_l2(gq, g) > 1e-3
+
+
+def _hardest_batched_soils(soils, count):
+    """The seeded uneven soils whose split sums cancel most: the lowest
+    min(Vs Qs) (slow, lossy layers) and the highest min(Qs) (sharp poles)."""
+    by_vsq = sorted(range(len(soils)), key=lambda i: min(l.vs * l.qs for l in soils[i][0]))
+    by_q = sorted(range(len(soils)), key=lambda i: -min(l.qs for l in soils[i][0]))
+    return list(dict.fromkeys(by_vsq[:count // 2] + by_q[:count // 2]))
+
+
+def test_split_sum_on_hardest_batched_soils(gfk, engine):
+    """The exact int8-slice wavenumber sum against the FP64 sum on the same
+    integrand, on the 64 hardest of the 4096 seeded uneven soils at their full
+    size (256-2048 bins each, 8192 wavenumbers, 128 ranges): rel-L2 <= 1e-6 per
+    soil, and <= 1e-5 in every bin."""
+    soils, ranges, nk, kmax = gfk.workloads.batched_soils()
+    pick = _hardest_batched_soils(soils, 64)
+    assert len(pick) >= 60
+    opt = gfk.Integration(nk, 0.0, kmax)
+    out = {}
+    for quad in (gfk.PLAIN_FP64, gfk.SPLIT_INT8):
+        media = [gfk.Medium(soils[i][0], formulation=gfk.DUNKIN, quadrature=quad, engine=engine) for i in pick]
+        b = gfk.Batch(media, [soils[i][1] for i in pick], ranges, opt, engine=engine)
+        b.execute()
+        got, status = b.download()
+        assert (status == 0).all() and np.isfinite(got).all()
+        out[quad] = b.split(got)
+        b.close()
+    worst_soil = worst_bin = 0.0
+    for a, s in zip(out[gfk.PLAIN_FP64], out[gfk.SPLIT_INT8]):
+        worst_soil = max(worst_soil, rel_l2(s, a))
+        worst_bin = max(worst_bin, float(np.max(np.linalg.norm(s - a, axis=1) / np.linalg.norm(a, axis=1))))
+    assert worst_soil < 1e-6, worst_soil
+    assert worst_bin < 1e-5, worst_bin

@@ -226,3 +226,17 @@ def test_dunkin_matches_direct_in_guarded_band(oracle, gfk):
     b, sb = oracle.bank_spectra(st, wl.ranges[::8], freqs, samples=1024, kmax=wl.kmax, formulation=1)
     assert (sa == 0).all() and (sb == 0).all()
     assert np.linalg.norm(a - b) / np.linalg.norm(a) < 1e-6
+
+
+def test_layered_causality_known_answers(oracle):
+    """TestLayeredResponseHasNoPrecursor (internal/fk/causality_test.go:45-141):
+    the oracle's reference-direct spectra of the 2 m layer over a half-space,
+    shaped and transformed as the reference's test does, reproduce the logged
+    peak times, precursor and negative-time values to their printed digits
+    (docs/validation-report.md:278-280) — a pin on layered output."""
+    import causality_case as CC
+    m = oracle.OracleMedium(CC.STACK, default_q=CC.DEFAULT_Q)
+    _, freqs = CC.bins()
+    spectra, status = oracle.bank_spectra(m, CC.RANGES, freqs)
+    assert (status == 0).all()
+    CC.check_against_logged(CC.metrics(spectra), KA["causality_precursor"])

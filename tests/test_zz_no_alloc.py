@@ -61,5 +61,21 @@ def test_noalloc_matches_allocating_entry_point_twice():
         # and the guard still refuses what the reference refuses
         st, _ = _call_noalloc(gfk, cases[1][0], cases[1][1], 300.0, gfk.Integration())
         assert st == N.EGUARD
+        # a call that fails on the device (a 1e-200 m range puts the grid at
+        # k ~ 1e201, where k^2 overflows and the solve turns non-finite) returns
+        # the allocating call's status and leaves zeros in out, not NaNs
+        dunkin = cases[0][0]
+        tiny = np.array([1e-200, 1.0])
+        opt = gfk.Integration(64, 0.0, 1.0)
+        with pytest.raises(gfk.FkError) as e:
+            dunkin.vertical_displacement_multi(tiny, 40.0, opt)
+        st, got = _call_noalloc(gfk, dunkin, tiny, 40.0, opt)
+        assert st == e.value.status == N.ENONFINITE
+        assert np.array_equal(got, np.zeros(2, dtype=complex))
+        # and the next call in the same array is unaffected
+        st, got = _call_noalloc(gfk, *cases[0])
+        assert st == 0
+        want = cases[0][0].vertical_displacement_multi(*cases[0][1:])
+        assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-9
     finally:
         eng.close()
