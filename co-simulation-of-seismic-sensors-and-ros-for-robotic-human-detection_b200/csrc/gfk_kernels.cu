@@ -169,7 +169,8 @@ __global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict
             mre = fabs(r.re); mim = fabs(r.im);
         } else if (ILP == 1) {
             const double k = (double)i0 * d;
-            cd r = k * dunkin_u(s_lc, nl, wc2[f], k, mu_ref) - c;
+            const cd u = dunkin_u(s_lc, nl, wc2[f], k, mu_ref);
+            cd r = k * u - c;
             if (!finite_cd(r)) { bad |= kStNonfinite; r = mk(0.0); }
             row[i0 - 1] = r;
             mre = fabs(r.re); mim = fabs(r.im);

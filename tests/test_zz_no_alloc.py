@@ -61,15 +61,17 @@ def test_noalloc_matches_allocating_entry_point_twice():
         # and the guard still refuses what the reference refuses
         st, _ = _call_noalloc(gfk, cases[1][0], cases[1][1], 300.0, gfk.Integration())
         assert st == N.EGUARD
-        # a call that fails on the device (a 1e-200 m range puts the grid at
-        # k ~ 1e201, where k^2 overflows and the solve turns non-finite) returns
-        # the allocating call's status and leaves zeros in out, not NaNs
-        dunkin = cases[0][0]
-        tiny = np.array([1e-200, 1.0])
-        opt = gfk.Integration(64, 0.0, 1.0)
+        # a call that fails on the device (a density of 1e305 kg/m^3 passes
+        # the stack's validation, but rho Vs^2 overflows, so every layer
+        # constant and the response are non-finite) returns the allocating
+        # call's status and leaves zeros in out, not NaNs
+        heavy = gfk.Medium(gfk.Stack([gfk.Layer(3.0, 400, 160, 1e305), gfk.Layer(0, 900, 400, 1e305)]),
+                           formulation=gfk.DUNKIN, engine=eng)
+        ranges = np.array([2.0, 5.0])
+        opt = gfk.Integration(256, 0.0, 20.0)
         with pytest.raises(gfk.FkError) as e:
-            dunkin.vertical_displacement_multi(tiny, 40.0, opt)
-        st, got = _call_noalloc(gfk, dunkin, tiny, 40.0, opt)
+            heavy.vertical_displacement_multi(ranges, 40.0, opt)
+        st, got = _call_noalloc(gfk, heavy, ranges, 40.0, opt)
         assert st == e.value.status == N.ENONFINITE
         assert np.array_equal(got, np.zeros(2, dtype=complex))
         # and the next call in the same array is unaffected
