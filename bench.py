@@ -170,7 +170,7 @@ def propagated_layers(stack, freqs, omega_imag, k, ref_freq=30.0, default_q=0.0)
     """Mean number of finite layers the Dunkin solve propagates per
     (frequency, wavenumber) once it starts at the shallowest layer thick enough
     to isolate the ones beneath (start_layer in csrc/gfk_solver.cuh: both
-    Re(1 - c^2/v^2) (k h)^2 above kThick^2 = 26^2), evaluated on the given
+    Re(1 - c^2/v^2) (k h)^2 above kThick^2 = 23^2), evaluated on the given
     sample grid.
     The propagator's algorithmic count assumes every finite layer."""
     wc2 = (2 * np.pi * np.asarray(freqs) - 1j * omega_imag) ** 2
@@ -194,7 +194,7 @@ def propagated_layers(stack, freqs, omega_imag, k, ref_freq=30.0, default_q=0.0)
         pa = 1.0 - np.real(c2 / (a * a)[:, None])
         pb = 1.0 - np.real(c2 / (b * b)[:, None])
         zeta = np.asarray(k)[None, :] * lay.thickness
-        thick = open_ & (np.minimum(pa, pb) * zeta * zeta > 26.0 ** 2)
+        thick = open_ & (np.minimum(pa, pb) * zeta * zeta > 23.0 ** 2)
         top[thick] = i
         open_ &= ~thick
     return float(top.mean())

@@ -582,8 +582,9 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
     return GFK_OK;
 }
 
-// Times every Dunkin launch shape on a window of up to 64 rows of the first
-// chunk (its middle) and keeps the fastest. The window's integrand rows are
+// Times every Dunkin launch shape on a window of up to 256 rows of the first
+// chunk (its middle) and keeps the fastest (64-row windows could not tell
+// shapes 4% apart at full size). The window's integrand rows are
 // recomputed by the real launch afterwards.
 int tune_prop(gfk_plan* p) {
     gfk_ctx* ctx = p->ctx;
@@ -601,7 +602,7 @@ int tune_prop(gfk_plan* p) {
             return GFK_OK;
         }
     const int c0 = p->chunk_begin[0], c1 = p->chunk_begin[1];
-    const int win = std::min(64, c1 - c0);
+    const int win = std::min(256, c1 - c0);
     if (win <= 0) return GFK_OK;
     const int fb = c0 + (c1 - c0 - win) / 2;
     int cmax = 0;
