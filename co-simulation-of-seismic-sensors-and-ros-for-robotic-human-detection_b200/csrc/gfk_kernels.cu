@@ -367,126 +367,192 @@ void launch_j0_table(cudaStream_t s, const double* ranges, int nr, int nk, doubl
 // ----------------------------------------------------- FP64 quadrature --
 //
 // G[f][j] = C_f/r_j - (dk/2) C_f + sum_i rem[f][i] W[i][j]:
-// a complex (nf x nk) by real (nk x nr) product on the FP64 pipe.
-// Block tile 64 f x 64 r x 16 k, 256 threads, 4 x 4 complex accumulators each,
-// register-staged double buffering of the shared-memory tiles.
+// a complex (nf x nk) by real (nk x nr) product, computed as the real GEMM of
+// the 2 nf rows (re, im) of the integrand on the FP64 tensor cores:
+// mma.sync m8n8k4 f64 (A 8x4 row-major, B 4x8 column-major, FP64 accumulate;
+// lane t holds A[t/4][t%4], B[t%4][t/4] and C[t/4][2(t%4) + {0,1}]). Block
+// tile 128 real rows (64 frequencies) x 16 TNW ranges x 16 wavenumbers, 8
+// warps as 4 (rows) x 2 (ranges), a warp owning 32 x 8 TNW of the output
+// (4 x TNW 8x8 accumulator tiles). The tiles move global -> shared with
+// cp.async in a 3-stage ring; a stage holds the integrand as [k][2f + part]
+// and the weights as [k][r], both with a row stride of 8 mod 16 doubles, so
+// each fragment load (4 wavenumber rows x 8 consecutive doubles) takes the
+// minimum two shared-memory wavefronts.
 
-constexpr int QBM = 64, QBN = 64, QBK = 16;
+namespace qd {
+constexpr int BM = 128, BK = 16, STAGES = 3, THREADS = 256;  // real rows, wavenumbers per stage
+constexpr int ASTR = BM + 8;
+template <int TNW>
+__host__ __device__ constexpr int bstr() { return 16 * TNW + 8; }
+template <int TNW>
+constexpr int smem_bytes() { return STAGES * (BK * ASTR + BK * bstr<TNW>()) * (int)sizeof(double); }
 
-__global__ __launch_bounds__(256) void k_quad_gemm(const cd* __restrict__ rem, const double* __restrict__ W,
-                                                   const cd* __restrict__ C, const double* __restrict__ ranges,
-                                                   int nf, int nk, int nr, double dk, cd* __restrict__ G,
-                                                   cd* __restrict__ part) {
-    __shared__ __align__(16) cd sA[2][QBK][QBM];
-    __shared__ __align__(16) double sB[2][QBK][QBN];
-    const int tid = threadIdx.x;
-    const int tr = tid & 15, tf = tid >> 4;
-    const int f0 = blockIdx.y * QBM, r0 = blockIdx.x * QBN;
-    // global -> register staging: A 4 complex along k, B 4 doubles along r
-    const int af = tid >> 2, ak = (tid & 3) * 4;
-    const int bk = tid >> 4, br = (tid & 15) * 4;
-    cd ra[4];
-    double rb[4];
-    auto load = [&](int kt) {
-        const int kb = kt * QBK;
-        const int gf = f0 + af;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int gk = kb + ak + q;
-            ra[q] = (gf < nf && gk < nk) ? rem[(size_t)gf * nk + gk] : mk(0.0);
-        }
-        const int gk = kb + bk;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int gr = r0 + br + q;
-            rb[q] = (gk < nk && gr < nr) ? W[(size_t)gk * nr + gr] : 0.0;
-        }
-    };
-    auto store = [&](int buf) {
-#pragma unroll
-        for (int q = 0; q < 4; q++) sA[buf][ak + q][af] = ra[q];
-#pragma unroll
-        for (int q = 0; q < 4; q++) sB[buf][bk][br + q] = rb[q];
-    };
-    cd acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = mk(0.0);
-    // this block's wavenumber tiles: all of them, or split z of gridDim.z
-    const int ntiles = (nk + QBK - 1) / QBK;
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+}  // namespace qd
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <int TNW>
+__global__ __launch_bounds__(qd::THREADS, TNW == 8 ? 1 : 2) void k_quad_gemm(const cd* __restrict__ rem,
+                                                              const double* __restrict__ W,
+                                                              const cd* __restrict__ C,
+                                                              const double* __restrict__ ranges, int nf, int nk,
+                                                              int nr, double dk, cd* __restrict__ G,
+                                                              cd* __restrict__ part) {
+    using namespace qd;
+    constexpr int BN = 16 * TNW, BSTR = bstr<TNW>();
+    extern __shared__ __align__(16) double d_smem[];
+    double* const sA = d_smem;                       // [STAGES][BK][ASTR]
+    double* const sB = d_smem + STAGES * BK * ASTR;  // [STAGES][BK][BSTR]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 3, wn = warp >> 2;
+    const int f0 = blockIdx.y * (BM / 2);
+    const int n0 = blockIdx.x * BN;
+    const int ntiles = (nk + BK - 1) / BK;
     const int kt0 = (int)((long long)blockIdx.z * ntiles / gridDim.z);
-    const int kt1 = (int)((long long)(blockIdx.z + 1) * ntiles / gridDim.z);
-    load(kt0);
-    store(0);
-    __syncthreads();
-    for (int kt = kt0; kt < kt1; kt++) {
-        const int buf = (kt - kt0) & 1;
-        if (kt + 1 < kt1) load(kt + 1);
+    const int nt = (int)((long long)(blockIdx.z + 1) * ntiles / gridDim.z) - kt0;
+
+    auto load = [&](int stage, int kt) {
+        const int kb = kt * BK;
+        double* a = sA + stage * BK * ASTR;
+        double* b = sB + stage * BK * BSTR;
+        const int fr = tid >> 2, kq = (tid & 3) * 4;
+        const int gf = f0 + fr;
 #pragma unroll
-        for (int kk = 0; kk < QBK; kk++) {
-            cd av[4];
-            double bv[4];
-#pragma unroll
-            for (int a = 0; a < 4; a++) av[a] = sA[buf][kk][tf * 4 + a];
-#pragma unroll
-            for (int b = 0; b < 4; b++) bv[b] = sB[buf][kk][tr * 4 + b];
-#pragma unroll
-            for (int a = 0; a < 4; a++)
-#pragma unroll
-                for (int b = 0; b < 4; b++) {
-                    acc[a][b].re = fma(av[a].re, bv[b], acc[a][b].re);
-                    acc[a][b].im = fma(av[a].im, bv[b], acc[a][b].im);
-                }
+        for (int q = 0; q < 4; q++) {
+            const int k = kb + kq + q;
+            const bool ok = gf < nf && k < nk;
+            qd::cp_async16(a + (kq + q) * ASTR + 2 * fr,
+                           ok ? (const void*)(rem + (size_t)gf * nk + k) : (const void*)rem, ok);
         }
-        if (kt + 1 < kt1) {
-            store(buf ^ 1);
-        }
-        __syncthreads();
-    }
-    if (part) {
-        cd* out = part + (size_t)blockIdx.z * nf * nr;
+        const int kr = tid >> 4, c0 = (tid & 15) * 2;
+        const int k = kb + kr;
 #pragma unroll
-        for (int a = 0; a < 4; a++) {
-            const int f = f0 + tf * 4 + a;
-            if (f >= nf) continue;
+        for (int q = 0; q < BN / 32; q++)
 #pragma unroll
-            for (int b = 0; b < 4; b++) {
-                const int j = r0 + tr * 4 + b;
-                if (j < nr) out[(size_t)f * nr + j] = acc[a][b];
+            for (int e = 0; e < 2; e++) {
+                const int col = c0 + 32 * q + e, gc = n0 + col;
+                const bool ok = k < nk && gc < nr;
+                qd::cp_async8(b + kr * BSTR + col, ok ? (const void*)(W + (size_t)k * nr + gc) : (const void*)W, ok);
             }
-        }
-        return;
+    };
+
+    double acc[4][TNW][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < TNW; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; s++) {
+        if (s < nt) load(s, kt0 + s);
+        qd::cp_commit();
     }
+    const int fa = (lane & 3) * ASTR + wm * 32 + (lane >> 2);       // this lane's A fragment element
+    const int fb = (lane & 3) * BSTR + wn * 8 * TNW + (lane >> 2);  // and B fragment element
+    for (int t = 0; t < nt; t++) {
+        qd::cp_wait<STAGES - 2>();
+        __syncthreads();
+        if (t + STAGES - 1 < nt) load((t + STAGES - 1) % STAGES, kt0 + t + STAGES - 1);
+        qd::cp_commit();
+        const double* a = sA + (t % STAGES) * BK * ASTR + fa;
+        const double* b = sB + (t % STAGES) * BK * BSTR + fb;
 #pragma unroll
-    for (int a = 0; a < 4; a++) {
-        const int f = f0 + tf * 4 + a;
-        if (f >= nf) continue;
-        const cd c = C[f];
+        for (int k4 = 0; k4 < BK / 4; k4++) {
+            double av[4], bv[TNW];
 #pragma unroll
-        for (int b = 0; b < 4; b++) {
-            const int j = r0 + tr * 4 + b;
-            if (j >= nr) continue;
-            const cd head = c / ranges[j] - (0.5 * dk) * c;  // fk.go:529-532
-            G[(size_t)f * nr + j] = head + acc[a][b];
+            for (int i = 0; i < 4; i++) av[i] = a[4 * k4 * ASTR + 8 * i];
+#pragma unroll
+            for (int j = 0; j < TNW; j++) bv[j] = b[4 * k4 * BSTR + 8 * j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < TNW; j++) dmma(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
         }
+    }
+    qd::cp_wait<0>();
+
+    // lane holds real row wm*32 + 8i + lane/4 (frequency f0 + row/2, part row&1)
+    // and ranges wn*8 TNW + 8j + 2(lane%4) + {0,1}
+    double* const dst = reinterpret_cast<double*>(part ? part + (size_t)blockIdx.z * nf * nr : G);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int row = wm * 32 + 8 * i + (lane >> 2);
+        const int f = f0 + (row >> 1), pr = row & 1;
+        if (f >= nf) continue;
+        const double cp = pr ? C[f].im : C[f].re;
+#pragma unroll
+        for (int j = 0; j < TNW; j++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int jj = n0 + wn * 8 * TNW + 8 * j + 2 * (lane & 3) + e;
+                if (jj >= nr) continue;
+                double v = acc[i][j][e];
+                if (!part) v = (cp / ranges[jj] - (0.5 * dk) * cp) + v;  // fk.go:529-532
+                dst[2 * ((size_t)f * nr + jj) + pr] = v;
+            }
     }
 }
 
 int quad_gemm_splits(int nf, int nk, int nr) {
-    // two blocks per SM of 148; each split keeps at least 8 wavenumber tiles
-    const long long tiles = (long long)((nr + QBN - 1) / QBN) * ((nf + QBM - 1) / QBM);
-    const int ntiles = (nk + QBK - 1) / QBK;
-    if (tiles >= 148 || ntiles < 16) return 1;
-    const int want = (int)((296 + tiles - 1) / tiles);
-    return std::max(1, std::min({want, ntiles / 8, 64}));
+    // one block per SM of 148: the split count (<= 64, each split >= 8
+    // wavenumber tiles) whose blocks fill the last wave best, the smallest of
+    // equals; banks of many waves keep one split
+    const int bn = nr > 64 ? 128 : 64;
+    const long long tiles = (long long)((nr + bn - 1) / bn) * ((2 * nf + qd::BM - 1) / qd::BM);
+    const int ntiles = (nk + qd::BK - 1) / qd::BK;
+    if (tiles >= 8 * 148) return 1;
+    int best = 1;
+    double best_eff = 0.0;
+    for (int s = 1; s <= std::min(64, std::max(1, ntiles / 8)); s++) {
+        const long long blocks = tiles * s;
+        const double eff = (double)blocks / ((double)((blocks + 147) / 148) * 148.0);
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = s;
+        }
+    }
+    return best;
 }
+
+namespace {
+template <class K>
+void set_smem_once(K kernel, int bytes, bool* done) {
+    if (!*done) *done = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+}
+}  // namespace
 
 void launch_quad_gemm(cudaStream_t s, const cd* rem, const double* W, const cd* C, const double* ranges, int nf,
                       int nk, int nr, double dk, cd* G, int splits, cd* part) {
+    if (nf <= 0 || nr <= 0) return;
     if (splits < 1 || !part) splits = 1;
-    dim3 grid((nr + QBN - 1) / QBN, (nf + QBM - 1) / QBM, splits);
-    k_quad_gemm<<<grid, 256, 0, s>>>(rem, W, C, ranges, nf, nk, nr, dk, G, splits > 1 ? part : nullptr);
+    cd* const p = splits > 1 ? part : nullptr;
+    // a failed attribute call leaves the launch to fail, and the caller's
+    // cudaGetLastError to report it
+    static bool a8 = false, a4 = false;
+    if (nr > 64) {
+        set_smem_once(k_quad_gemm<8>, qd::smem_bytes<8>(), &a8);
+        dim3 grid((nr + 127) / 128, (2 * nf + qd::BM - 1) / qd::BM, splits);
+        k_quad_gemm<8><<<grid, qd::THREADS, qd::smem_bytes<8>(), s>>>(rem, W, C, ranges, nf, nk, nr, dk, G, p);
+    } else {
+        set_smem_once(k_quad_gemm<4>, qd::smem_bytes<4>(), &a4);
+        dim3 grid((nr + 63) / 64, (2 * nf + qd::BM - 1) / qd::BM, splits);
+        k_quad_gemm<4><<<grid, qd::THREADS, qd::smem_bytes<4>(), s>>>(rem, W, C, ranges, nf, nk, nr, dk, G, p);
+    }
     if (splits > 1) launch_quad_finish(s, part, splits, C, ranges, nf, nr, dk, G);
 }
 
