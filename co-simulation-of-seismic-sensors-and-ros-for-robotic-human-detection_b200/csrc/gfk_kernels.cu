@@ -509,24 +509,23 @@ __global__ __launch_bounds__(qd::THREADS, TNW == 8 ? 1 : 2) void k_quad_gemm(con
 }
 
 int quad_gemm_splits(int nf, int nk, int nr) {
-    // one block per SM of 148: the split count (<= 64, each split >= 8
-    // wavenumber tiles) whose blocks fill the last wave best, the smallest of
-    // equals; banks of many waves keep one split
+    // one block per SM of 148: the smallest split count (<= 64, each split
+    // >= 8 wavenumber tiles) whose blocks fill the waves within 2% of the best
+    // count's (more splits only add partial sums); banks of many waves keep one
     const int bn = nr > 64 ? 128 : 64;
     const long long tiles = (long long)((nr + bn - 1) / bn) * ((2 * nf + qd::BM - 1) / qd::BM);
     const int ntiles = (nk + qd::BK - 1) / qd::BK;
     if (tiles >= 8 * 148) return 1;
-    int best = 1;
-    double best_eff = 0.0;
-    for (int s = 1; s <= std::min(64, std::max(1, ntiles / 8)); s++) {
+    const int smax = std::min(64, std::max(1, ntiles / 8));
+    auto eff = [&](int s) {
         const long long blocks = tiles * s;
-        const double eff = (double)blocks / ((double)((blocks + 147) / 148) * 148.0);
-        if (eff > best_eff + 1e-9) {
-            best_eff = eff;
-            best = s;
-        }
-    }
-    return best;
+        return (double)blocks / ((double)((blocks + 147) / 148) * 148.0);
+    };
+    double best = 0.0;
+    for (int s = 1; s <= smax; s++) best = std::max(best, eff(s));
+    for (int s = 1; s <= smax; s++)
+        if (eff(s) >= best - 0.02) return s;
+    return 1;
 }
 
 namespace {
