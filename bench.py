@@ -339,6 +339,95 @@ def dev_view(torch, ptr, count, local):
     return torch.as_tensor(_Buf(), device=f"cuda:{local}")
 
 
+def abi_bank_spectra(gfk, eng, med, wl, out_host, status_host):
+    """The call geobank would make: gfk_bank_spectra through the C ABI, host
+    medium and grids in, the [nf][nr] complex128 bank into the pinned
+    `out_host` (a torch tensor of nf x 2 nr float64)."""
+    from gfk_b200.fk import _c_medium
+    N = gfk._native
+    r = np.ascontiguousarray(wl.ranges)
+    f = np.ascontiguousarray(wl.freqs)
+    with _c_medium(med) as cm:
+        st = N.lib().gfk_bank_spectra(eng.ctx, ctypes.byref(cm), ctypes.byref(med._solve()),
+                                      r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r),
+                                      f.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(f),
+                                      wl.integration().c(),
+                                      ctypes.cast(out_host.data_ptr(), ctypes.POINTER(ctypes.c_double)),
+                                      ctypes.cast(status_host.data_ptr(), ctypes.POINTER(ctypes.c_int32)))
+    eng.check(st)
+
+
+def single_leg(gfk, torch, eng, local, world, fp64_peak, steps=20, warmup=5, cpu=True):
+    """The single-soil workload (2 layers over a half-space, 512 bins x 64
+    ranges, 4096 wavenumbers) for the default bench line, in the plain FP64
+    form (the reference's complex128 bank, computed by the FP64 propagator
+    and the FP64 tensor-core sum) with the split sum beside it: device-resident
+    stream span (L2 flushed between steps), end to end through gfk_bank_spectra
+    into pinned host memory, the propagator's roofline, and the CPU baseline
+    on the bins the reference answers."""
+    wl = gfk.workloads.single_soil()
+    gstream = torch.cuda.ExternalStream(eng.stream(), device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    out = {"workload": "single_soil: 0.5 m (Vs 150, Vp 300, rho 1700, Qs 15, Qp 30) and 2 m (250, 500, 1800, 25, 50) "
+                       "layers over a half-space (400, 800, 2000, 40, 80); 512 bins 0-500 Hz (fs 1 kHz), 4096 "
+                       f"wavenumbers to {wl.kmax:.1f} rad/m, 64 ranges 1-64 m, w_I = pi/T",
+           "cells_per_step": wl.cells() * world}
+    got = {}
+    for name, quad in (("plain_fp64", gfk.PLAIN_FP64), ("split", gfk.SPLIT_INT8)):
+        med = wl.medium(gfk.DUNKIN, engine=eng, quadrature=quad)
+        plan = gfk.Plan(med, wl.ranges, wl.freqs, wl.integration(), engine=eng)
+        for _ in range(warmup):
+            plan.execute()
+        got[name], st = plan.download()
+        assert (st == 0).all()
+        plan.kernel_times(reset=True)
+        spans = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        launches0 = eng.kernel_launches()
+        with torch.cuda.stream(gstream):
+            for a, b in spans:
+                flush.fill_(1)
+                a.record(gstream)
+                plan.execute()
+                b.record(gstream)
+        torch.cuda.synchronize()
+        launches = eng.kernel_launches() - launches0
+        prop_ms, quad_ms, other_ms = plan.kernel_times(reset=True)
+        ms = allmax(sum(a.elapsed_time(b) for a, b in spans) / steps, world)
+        plan.close()
+        host = torch.empty((len(wl.freqs), 2 * len(wl.ranges)), dtype=torch.float64, pin_memory=True)
+        hstat = torch.zeros(len(wl.freqs), dtype=torch.int32, pin_memory=True)
+        abi_bank_spectra(gfk, eng, med, wl, host, hstat)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            abi_bank_spectra(gfk, eng, med, wl, host, hstat)
+        e2e_s = allmax((time.perf_counter() - t0) / steps, world)
+        kgrid = np.arange(1, wl.samples + 1) * (wl.kmax / wl.samples)
+        lx = propagated_layers(wl.stack, wl.freqs[::4], wl.omega_imag, kgrid[::4])
+        f_exec = len(wl.freqs) * wl.samples * (700 * lx + 300)
+        f_fixed = len(wl.freqs) * wl.samples * (700 * (len(wl.stack) - 1) + 300)
+        out[name] = {"value": wl.cells() * world / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+                     "warmup": warmup, "gpu_launches": launches,
+                     "kernel_ms": {"propagator": prop_ms, "quadrature": quad_ms, "other": other_ms},
+                     "e2e": {"value": wl.cells() * world / e2e_s, "unit": UNIT, "ms_per_step": e2e_s * 1e3,
+                             "h2d_bytes_per_step": len(wl.stack) * 48 + len(wl.ranges) * 8 + len(wl.freqs) * 36,
+                             "d2h_bytes_per_step": wl.cells() * 16 + len(wl.freqs) * 4},
+                     "roofline": {"bound": "fp64", "kernel": "k_prop (Dunkin propagator)",
+                                  "achieved": f_exec / (prop_ms * 1e-3) / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
+                                  "frac": f_exec / (prop_ms * 1e-3) / 1e12 / fp64_peak,
+                                  "mean_layers_propagated": lx,
+                                  "fixed_count_frac": f_fixed / (prop_ms * 1e-3) / 1e12 / fp64_peak}}
+    a, b = got["plain_fp64"], got["split"]
+    out["split"]["relL2_split_vs_fp64"] = float(np.linalg.norm(b - a) / np.linalg.norm(a))
+    out["value"], out["unit"], out["ms_per_step"] = out["plain_fp64"]["value"], UNIT, out["plain_fp64"]["ms_per_step"]
+    out["timing"] = "stream span of each execute on libgfk's stream, L2 flushed (256 MiB write) between steps"
+    if cpu:
+        cb = cpu_baseline(gfk, wl, os.cpu_count() or 1, target_s=8.0)
+        cb.pop("status_ok", None)
+        out["cpu_baseline"] = cb
+    del flush
+    return out
+
+
 def batched_leg(gfk, torch, eng, local, rank, world, fp64_peak, steps=3, cpu=True):
     """The 4096 seeded uneven soils (256-2048 bins each, 8192 wavenumbers, 128
     ranges; this rank's share) as one batch plan with the split sum, for the
@@ -866,7 +955,8 @@ def run_surrogate(args, gfk, torch, rank, world, local):
     ds.close()
     res_p = S.run_plain(eng, n=args.sobol_n, seed=0)
     log(f"plain sobol: {res_p.seconds}")
-    res_s = S.run_surrogate(eng, nets, n=args.sobol_n, seed=0, threshold=args.threshold, gate="rows")
+    res_s = S.run_surrogate(eng, nets, n=args.sobol_n, seed=0, threshold=args.threshold, gate="rows",
+                            amp_threshold=args.amp_threshold)
     log(f"surrogate sobol (row gate): {res_s.seconds}")
     res_g = S.run_surrogate(eng, nets, n=args.sobol_n, seed=0, threshold=args.threshold, gate="soil")
     log(f"surrogate sobol (soil gate): {res_g.seconds}")
@@ -895,7 +985,8 @@ def run_surrogate(args, gfk, torch, rank, world, local):
                                       f"x 512 bins labels (training ranges {args.sur_ranges or 'all'}), "
                                       f"{args.members} x MLP 6x512 SiLU BF16 {args.sur_steps} steps batch 8192; "
                                       f"Sobol N={args.sobol_n} d=8 at 10 m; f-k fallback on the rows where the "
-                                      f"ensemble spread exceeds {args.threshold:.0%} of the trace-spectrum peak"},
+                                      f"ensemble spread exceeds {args.threshold:.0%} of the trace-spectrum peak "
+                                      f"or the predicted |G S| exceeds {args.amp_threshold:.1%} of it"},
                "index_abs_error": err, "metric_rel_error_p50_p90_p99": rel,
                "soil_gate": {"speedup": res_p.seconds["total"] / res_g.seconds["total"],
                              "index_abs_error": index_errors(res_g), "metric_rel_error_p50_p90_p99":
@@ -931,11 +1022,13 @@ def main():
                          "soils' 8-parameter box inside it")
     ap.add_argument("--sur-ranges", default="", help="surrogate training range indices r0,r1 (default: all)")
     ap.add_argument("--threshold", type=float, default=0.01, help="ensemble spread above which soils fall back")
+    ap.add_argument("--amp-threshold", type=float, default=0.001,
+                    help="row gate: also re-solve rows whose predicted |G S| exceeds this share of the soil's peak")
     ap.add_argument("--save-nets", default="", help="directory to save the trained members")
     ap.add_argument("--quadrature", default="split", choices=["split", "fp64"],
                     help="split: exact int8-slice tensor-core sum (default); fp64: the plain FP64 sum")
     ap.add_argument("--no-batched", action="store_true",
-                    help="default workload: skip the batched uneven-soils object in the line")
+                    help="default workload: skip the single-soil and batched uneven-soils objects in the line")
     ap.add_argument("--profile", action="store_true",
                     help="profiling only: skip the e2e leg, the FP64 peak probe and the CPU baseline")
     args = ap.parse_args()
@@ -1014,15 +1107,7 @@ def main():
     f = np.ascontiguousarray(wl.freqs)
 
     def e2e_call():
-        from gfk_b200.fk import _c_medium
-        with _c_medium(med) as cm:
-            st = N.lib().gfk_bank_spectra(eng.ctx, ctypes.byref(cm), ctypes.byref(med._solve()),
-                                          r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r),
-                                          f.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(f),
-                                          wl.integration().c(),
-                                          ctypes.cast(out_host.data_ptr(), ctypes.POINTER(ctypes.c_double)),
-                                          ctypes.cast(status_host.data_ptr(), ctypes.POINTER(ctypes.c_int32)))
-        eng.check(st)
+        abi_bank_spectra(gfk, eng, med, wl, out_host, status_host)
 
     if args.profile:
         plan.close()
@@ -1118,8 +1203,10 @@ def main():
         cb.pop("status_ok", None)
     plan.close()
     del flush
-    batched = None
+    single = batched = None
     if not args.no_batched and args.workload == "graded" and args.freq_stride == 1:
+        single = single_leg(gfk, torch, eng, local, world, fp64_peak,
+                            cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
         batched = batched_leg(gfk, torch, eng, local, rank, world, fp64_peak,
                               steps=min(args.steps, 3), cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
     if rank == 0:
@@ -1141,6 +1228,8 @@ def main():
             out["cpu_baseline"] = cb
         if plain_leg:
             out["plain_fp64"] = plain_leg
+        if single:
+            out["single"] = single
         if batched:
             out["batched"] = batched
         print(json.dumps(out))

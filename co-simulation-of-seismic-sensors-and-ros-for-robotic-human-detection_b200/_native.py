@@ -139,7 +139,8 @@ def lib():
         "gfk_fdtd_run": (ctypes.c_int, [vp, P(GfkFdtdModel), P(d), i32, P(d), i32, i32, P(d), P(d), P(d)]),
         "gfk_dispersion_modes": (ctypes.c_int, [vp, P(GfkMedium), P(d), i32, GfkSearch, i32, P(d), P(i32)]),
         "gfk_secular": (ctypes.c_int, [vp, P(GfkMedium), P(d), P(d), i64, P(d), P(i32)]),
-        "gfk_ensemble_gate": (ctypes.c_int, [vp, P(vp), i32, i64, i32, i32, P(d), d, vp, P(ctypes.c_uint8), P(d)]),
+        "gfk_ensemble_gate": (ctypes.c_int, [vp, P(vp), i32, i64, i32, i32, P(d), d, d, vp, P(ctypes.c_uint8),
+                                             P(d)]),
         "gfk_scatter_rows": (ctypes.c_int, [vp, vp, i64, P(i64), i64, vp]),
         "gfk_bank_tables": (ctypes.c_int, [vp, P(f32), i32, i32, P(d), P(d)]),
         "gfk_bank_impulse_responses": (ctypes.c_int, [vp, P(f32), i32, i32, d, d, d, i32, P(d), i32, P(d), i32, i32,

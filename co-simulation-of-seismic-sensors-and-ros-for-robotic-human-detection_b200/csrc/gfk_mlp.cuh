@@ -217,6 +217,7 @@ struct GateArgs {
     int ns, nbins;
     const cd* S;
     double threshold;
+    double amp_threshold;  // > 0: also flag rows whose |mean S| exceeds it times the peak
     cd* mean;
     unsigned char* flag;
     double* spread;

@@ -407,8 +407,8 @@ int gfk_trace_metrics(gfk_ctx* ctx, const double* d_G, int64_t stride, int32_t n
 }
 
 int gfk_ensemble_gate(gfk_ctx* ctx, const double* const* d_members, int32_t E, int64_t stride, int32_t ns,
-                      int32_t nbins, const double* shaping, double threshold, double* d_mean, uint8_t* flags,
-                      double* spread) {
+                      int32_t nbins, const double* shaping, double threshold, double amp_threshold, double* d_mean,
+                      uint8_t* flags, double* spread) {
     if (!ctx || !d_members || !shaping || !d_mean || !flags || !spread) return GFK_EARG;
     if (E < 1 || E > gfk::trace::kMaxMembers || ns < 0 || nbins < 1 || stride < nbins)
         return sfail(ctx, GFK_EARG, "ensemble gate: bad sizes");
@@ -422,6 +422,7 @@ int gfk_ensemble_gate(gfk_ctx* ctx, const double* const* d_members, int32_t E, i
     a.ns = ns;
     a.nbins = nbins;
     a.threshold = threshold;
+    a.amp_threshold = amp_threshold;
     a.mean = reinterpret_cast<cd*>(d_mean);
     cd* d_S = nullptr;
     unsigned char* d_flag = nullptr;

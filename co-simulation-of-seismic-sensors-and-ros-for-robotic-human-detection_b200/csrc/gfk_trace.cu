@@ -98,8 +98,12 @@ __global__ void __launch_bounds__(kThreads) k_gate(GateArgs a) {
         const cd m = a.mean[(size_t)s * a.nbins + k];
         double d = 0.0;
         for (int e = 0; e < a.E; e++) d = fmax(d, cabs_(a.members[e][(size_t)s * a.stride + k] - m));
-        const double ratio = peak > 0.0 ? d * cabs_(a.S[k + 1]) / peak : 0.0;
-        a.flag[(size_t)s * a.nbins + k] = ratio > a.threshold ? 1 : 0;
+        const double sk = cabs_(a.S[k + 1]);
+        const double ratio = peak > 0.0 ? d * sk / peak : 0.0;
+        // an energetic row goes to the f-k solve whatever the members say:
+        // members that agree can all be wrong, and these rows carry the trace
+        const bool loud = a.amp_threshold > 0.0 && cabs_(m) * sk > a.amp_threshold * peak;
+        a.flag[(size_t)s * a.nbins + k] = (ratio > a.threshold || loud) ? 1 : 0;
         worst = fmax(worst, ratio);
     }
     red[tid] = worst;

@@ -477,7 +477,7 @@ def _solve_rows(params, bins_per_soil, setup, engine, batch_soils, nk=NK, kmax=K
 
 
 def run_surrogate(engine, nets, n=16384, seed=0, setup=None, threshold=0.01, batch_soils=20000, gate="rows",
-                  chunk_soils=32768):
+                  chunk_soils=32768, amp_threshold=0.001):
     """The Sobol run with the surrogate answering and the plain GPU f-k solve
     as fallback and judge.
 
@@ -486,6 +486,10 @@ def run_surrogate(engine, nets, n=16384, seed=0, setup=None, threshold=0.01, bat
     members disagree by more than `threshold` of the soil's trace-spectrum
     peak (gfk_ensemble_gate), which the f-k solve recomputes in place
     (gfk_scatter_rows); metrics then run on the merged device spectra.
+    With amp_threshold > 0 the rows whose predicted |G S_k| exceeds
+    amp_threshold of that peak are re-solved too: members trained on the same
+    data can agree on an energetic row and all be wrong, and those rows carry
+    the trace.
     gate="soil": each network's metrics are computed; where the ensemble's
     relative spread of either metric exceeds `threshold` the whole soil is
     re-solved and its plain metrics replace the ensemble mean."""
@@ -541,7 +545,7 @@ def run_surrogate(engine, nets, n=16384, seed=0, setup=None, threshold=0.01, bat
         sp = np.zeros(m)
         engine.check(N.lib().gfk_ensemble_gate(
             engine.ctx, ptrs, len(nets), nb, m, nb, S.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), threshold,
-            ctypes.c_void_p(mean.data_ptr()), flags.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+            amp_threshold, ctypes.c_void_p(mean.data_ptr()), flags.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
             sp.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         tb = time.perf_counter()
         t_pred += tb - ta

@@ -391,10 +391,12 @@ int gfk_trace_metrics(gfk_ctx *ctx, const double *d_G, int64_t stride, int32_t n
  * receives their mean; flags (host, [ns][nbins] bytes) marks the rows whose
  * ensemble disagreement, weighted by the trace shaping |S_k| (the factors of
  * gfk_trace_metrics, n/2 + 1 = nbins + 1 pairs, host), exceeds threshold times
- * the peak of |mean S| over the soil's bins; spread (host, ns) receives each
- * soil's largest such ratio. E <= 16. */
+ * the peak of |mean S| over the soil's bins, and, when amp_threshold > 0, the
+ * rows whose |mean S_k| itself exceeds amp_threshold times that peak (the
+ * energetic rows, re-solved even where the members agree); spread (host, ns)
+ * receives each soil's largest disagreement ratio. E <= 16. */
 int gfk_ensemble_gate(gfk_ctx *ctx, const double *const *d_members, int32_t E, int64_t stride,
-                      int32_t ns, int32_t nbins, const double *shaping, double threshold,
+                      int32_t ns, int32_t nbins, const double *shaping, double threshold, double amp_threshold,
                       double *d_mean, uint8_t *flags, double *spread);
 /* d_dst[2 index[i]] <- d_src[2 i src_stride] (re, im pairs), i < n; index host,
  * the pointers device memory. Puts solved rows back into a spectrum buffer. */
