@@ -26,7 +26,7 @@ NET_FOURIER = 47
 
 # every symbol include/gfk.h declares
 EXPORTS = [
-    "gfk_open", "gfk_close", "gfk_status_string", "gfk_last_error", "gfk_kernel_launches", "gfk_stream",
+    "gfk_open", "gfk_close", "gfk_status_string", "gfk_last_error", "gfk_kernel_launches", "gfk_stream", "gfk_selftest_wait_timeout",
     "gfk_stack_validate", "gfk_check_layer_phase", "gfk_grid_for",
     "gfk_surface_response", "gfk_static_coefficient", "gfk_vertical_displacement",
     "gfk_vertical_displacement_multi", "gfk_bank_spectra",
@@ -109,6 +109,7 @@ def lib():
         "gfk_last_error": (ctypes.c_char_p, [vp]),
         "gfk_kernel_launches": (i64, [vp]),
         "gfk_stream": (vp, [vp]),
+        "gfk_selftest_wait_timeout": (ctypes.c_int, [vp, i64, P(i32)]),
         "gfk_stack_validate": (ctypes.c_int, [P(GfkMedium)]),
         "gfk_check_layer_phase": (ctypes.c_int, [P(GfkMedium), d]),
         "gfk_grid_for": (ctypes.c_int, [P(GfkMedium), P(d), i32, d, GfkIntegration, P(GfkGrid)]),

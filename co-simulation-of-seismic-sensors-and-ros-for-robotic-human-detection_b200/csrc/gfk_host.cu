@@ -871,6 +871,23 @@ int64_t gfk_kernel_launches(const gfk_ctx* ctx) { return ctx ? ctx->launches : 0
 
 void* gfk_stream(const gfk_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
 
+int gfk_selftest_wait_timeout(gfk_ctx* ctx, int64_t wait_cycles, int32_t* rows_timed_out) {
+    if (!ctx || !rows_timed_out || wait_cycles <= 0) return GFK_EARG;
+    *rows_timed_out = 0;
+    cudaSetDevice(ctx->device);
+    int rows = 0;
+    const int rc = gfk::quad_tc_selftest_timeout(ctx->stream, wait_cycles, &rows);
+    ctx->launches++;
+    if (rc) return fail(ctx, GFK_ECUDA, "wait self-test: CUDA failure (step %d): %s", rc,
+                        cudaGetErrorString(cudaGetLastError()));
+    *rows_timed_out = rows;
+    if (rows == 0) {
+        ctx->last_error.clear();
+        return GFK_OK;
+    }
+    return fail(ctx, GFK_ETIMEOUT, "a device-side wait in the tensor-core quadrature timed out (self-test)");
+}
+
 int gfk_stack_validate(const gfk_medium* m) { return validate(nullptr, m); }
 
 int gfk_check_layer_phase(const gfk_medium* m, double freq_hz) { return check_layer_phase(nullptr, m, freq_hz); }

@@ -71,6 +71,8 @@ struct Args {
     cd* G;              // [nf][N]
     int* status;        // [nf] status bits
     cd* part;           // split partial sums [gridDim.z][M/2][N], or null (one split)
+    long long wait_cycles;  // bound on each mbarrier wait (kWaitCycles)
+    int starve;         // self-test only: the producer issues no loads, so the first wait runs out
 };
 
 __global__ void __launch_bounds__(THREADS, 1)
@@ -114,10 +116,10 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (warp == 0) {
         if (lane == 0) {
             int issued = 0;
-            for (int kb = 0; kb < nkb; kb++) {
+            for (int kb = 0; kb < (a.starve ? 0 : nkb); kb++) {
                 const int st = kb % STAGES;
                 const uint32_t ph = (kb / STAGES) & 1;
-                if (!mbar_wait(&empty[st], ph ^ 1)) {
+                if (!mbar_wait(&empty[st], ph ^ 1, a.wait_cycles)) {
                     *abort_flag = 1;
                     break;
                 }
@@ -134,7 +136,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
             // drain: the last loads of each stage land before the CTA may exit
             for (int kb = issued - 1; kb >= 0 && kb >= issued - STAGES; kb--)
-                if (!mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1)) *abort_flag = 1;
+                if (!mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, a.wait_cycles)) *abort_flag = 1;
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -142,7 +144,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             bool init[S] = {false, false, false, false};
             for (int kb = 0; kb < nkb; kb++) {
                 const int st = kb % STAGES;
-                if (!mbar_wait(&full[st], (kb / STAGES) & 1)) {
+                if (!mbar_wait(&full[st], (kb / STAGES) & 1, a.wait_cycles)) {
                     *abort_flag = 1;
                     break;
                 }
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     } else {
         // epilogue: warps 2..5 cover TMEM lane quarters 2, 3, 0, 1
-        const bool ok = mbar_wait(accf, 0);
+        const bool ok = mbar_wait(accf, 0, a.wait_cycles);
         tc_fence_after();
         const int q = warp & 3;
         const int row = m0 + q * 32 + lane;
@@ -367,7 +369,7 @@ int quad_tc_splits(int M, int N, int Kp) {
 
 int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int N, int Mp, int Np, int Kp,
                    const int* row_exp, int col_exp, const cd* C, const double* ranges, double dk, cd* G, int* status,
-                   int splits, cd* part) {
+                   int splits, cd* part, long long wait_cycles, int starve) {
     if (Mp % tc::BM || Np % tc::BN || Kp % tc::BK || M > Mp || N > Np) return 1;
     if (splits < 1 || !part) splits = 1;
     if (splits > Kp / tc::BK) return 1;
@@ -380,11 +382,50 @@ int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int 
             return 3;
         attr_set = true;
     }
-    tc::Args a{M, N, Mp, Np, Kp, row_exp, col_exp, C, ranges, dk, G, status, splits > 1 ? part : nullptr};
+    tc::Args a{M, N, Mp, Np, Kp, row_exp, col_exp, C, ranges, dk, G, status, splits > 1 ? part : nullptr,
+               wait_cycles > 0 ? wait_cycles : tc::kWaitCycles, starve};
     dim3 grid(Np / tc::BN, Mp / tc::BM, splits);
     tc::k_quad_tc<<<grid, tc::THREADS, tc::SMEM_BYTES, s>>>(ta, tb, a);
     if (splits > 1) launch_quad_finish(s, part, splits, C, ranges, M >> 1, N, dk, G);
     return 0;
+}
+
+// A starved launch of the tensor-core sum on one 128 x 128 x 64 tile: the
+// producer issues no loads, so the MMA issuer's first wait runs out after
+// wait_cycles, the kernel drains, frees its TMEM and marks the tile's rows
+// timed out. Returns 0 with *timed_out the number of the 64 rows so marked,
+// or a nonzero launch/CUDA error code.
+int quad_tc_selftest_timeout(cudaStream_t s, long long wait_cycles, int* timed_out) {
+    *timed_out = 0;
+    const int M = 128, N = 128, Kp = 64, nf = M / 2;
+    int8_t *A = nullptr, *B = nullptr;
+    int *row_exp = nullptr, *status = nullptr;
+    cd *C = nullptr, *G = nullptr;
+    double* ranges = nullptr;
+    int rc = 0;
+    auto alloc = [&](void** p, size_t bytes) {
+        if (!rc && cudaMallocAsync(p, bytes, s) != cudaSuccess) rc = 10;
+        if (!rc && cudaMemsetAsync(*p, 0, bytes, s) != cudaSuccess) rc = 11;
+    };
+    alloc((void**)&A, (size_t)tc::S * M * Kp);
+    alloc((void**)&B, (size_t)tc::S * N * Kp);
+    alloc((void**)&row_exp, sizeof(int) * M);
+    alloc((void**)&status, sizeof(int) * nf);
+    alloc((void**)&C, sizeof(cd) * nf);
+    alloc((void**)&G, sizeof(cd) * nf * N);
+    alloc((void**)&ranges, sizeof(double) * N);
+    if (!rc) rc = launch_quad_tc(s, A, B, M, N, M, N, Kp, row_exp, 0, C, ranges, 1.0, G, status, 1, nullptr,
+                                 wait_cycles, 1);
+    if (!rc && cudaGetLastError() != cudaSuccess) rc = 12;
+    int host[64] = {0};
+    if (!rc && cudaMemcpyAsync(host, status, sizeof(int) * nf, cudaMemcpyDeviceToHost, s) != cudaSuccess) rc = 13;
+    void* bufs[] = {A, B, row_exp, status, C, G, ranges};
+    for (void* p : bufs)
+        if (p) cudaFreeAsync(p, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess && !rc) rc = 14;
+    for (int f = 0; f < nf && !rc; f++)
+        if (host[f] & kStTimeout) (*timed_out)++;
+    return rc;
 }
 
 }  // namespace gfk

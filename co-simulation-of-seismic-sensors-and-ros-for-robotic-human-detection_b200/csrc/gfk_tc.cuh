@@ -42,12 +42,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
     return ok != 0;
 }
 
-// Waits for the phase of the given parity to complete; false after ~1 s.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+// Waits for the phase of the given parity to complete; false after `limit`
+// SM clocks (~1 s by default).
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, long long limit = kWaitCycles) {
     if (mbar_try_wait(b, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(b, parity))
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 

@@ -139,6 +139,15 @@ int64_t gfk_kernel_launches(const gfk_ctx *ctx);
  * (a cudaStream_t, non-blocking) every call of this context is queued on, so
  * a caller can order its own device work and timing events with libgfk's. */
 void *gfk_stream(const gfk_ctx *ctx);
+/* No counterpart in the reference: a self-test of the bounded device waits.
+ * Launches the tensor-core wavenumber sum on one 128 x 128 x 64 tile with its
+ * producer told to issue no loads, so the MMA issuer's wait runs out after
+ * wait_cycles SM clocks (use a few million: ~1-2 ms). The kernel then drains,
+ * frees its tensor memory, exits and marks the tile's 64 rows timed out, as a
+ * real stall would. Returns GFK_ETIMEOUT with *rows_timed_out = 64 when the
+ * timeout was detected and reported; GFK_OK (0 rows) would mean the wait did
+ * not run out. The context stays usable afterwards. */
+int gfk_selftest_wait_timeout(gfk_ctx *ctx, int64_t wait_cycles, int32_t *rows_timed_out);
 
 /* ---- host-only helpers (no device work) ---------------------------------- */
 /* layer.Stack.Validate (internal/layer/layer.go:53-73). */

@@ -3,6 +3,7 @@ high-precision golden values. Tolerances: rel-L2 <= 1e-9 for the FP64 Dunkin
 path (same algorithm, different rounding), <= 1e-6 for the reference-direct
 path (the direct eigenbasis loses digits at large k/k_body in both
 implementations, differently)."""
+import ctypes
 import json
 import math
 
@@ -534,3 +535,22 @@ def test_split_sum_on_hardest_batched_soils(gfk, engine):
         worst_bin = max(worst_bin, float(np.max(np.linalg.norm(s - a, axis=1) / np.linalg.norm(a, axis=1))))
     assert worst_soil < 1e-6, worst_soil
     assert worst_bin < 1e-5, worst_bin
+
+
+def test_tensor_core_wait_timeout_is_reported_and_context_survives(gfk, engine):
+    """Failure detection without a GPU fault: the tensor-core sum's producer is
+    told to issue no loads, so the MMA issuer's bounded mbarrier wait runs out
+    (after 2^22 SM clocks, ~2 ms). The kernel must drain, free its tensor
+    memory, exit and mark the tile's 64 rows GFK_ETIMEOUT, and the same context
+    must then compute a split-sum bank as before."""
+    N = gfk._native
+    rows = ctypes.c_int32()
+    st = N.lib().gfk_selftest_wait_timeout(engine.ctx, 1 << 22, ctypes.byref(rows))
+    assert st == N.ETIMEOUT and rows.value == 64, (N.status_string(st), rows.value)
+    wl = gfk.workloads.single_soil()
+    split = wl.medium(gfk.DUNKIN, engine=engine, quadrature=gfk.SPLIT_INT8)
+    plain = wl.medium(gfk.DUNKIN, engine=engine)
+    a, sa = split.bank_spectra(wl.ranges, wl.freqs[::8], wl.integration())
+    b, sb = plain.bank_spectra(wl.ranges, wl.freqs[::8], wl.integration())
+    assert (sa == 0).all() and (sb == 0).all()
+    assert rel_l2(a, b) < 1e-6
