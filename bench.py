@@ -428,6 +428,77 @@ def single_leg(gfk, torch, eng, local, world, fp64_peak, steps=20, warmup=5, cpu
     return out
 
 
+def learned_leg(gfk, torch, eng, world, steps=200, warmup=10):
+    """The learned part at a size that fits the default bench run.
+
+    Training throughput (config 4's network and batch): FP64 labels for 8192
+    soils of the 11-scalar family from the batched solver, then `steps`
+    timed AdamW steps of the BF16 6 x 512 network (batch 8192, one CUDA graph
+    per step). Surrogate gain (config 5's sweep at N = 256): three members
+    trained 20,000 steps on 16,384 Sobol-box soils at the sensor range answer
+    the 2560-soil Saltelli sweep; the row gate re-solves disputed and
+    energetic rows with the plain f-k solve; reported against the all-plain
+    run: rows solved, wall time of both runs, and Sobol index errors."""
+    U, S = gfk.surrogate, gfk.sobol
+    out = {}
+    params = U.draw(8192, 20240611)
+    t0 = time.perf_counter()
+    ds = U.Dataset(params, U.LabelGrid(), floor_rel=1e-6, engine=eng).fill(batch_soils=8192)
+    label_s = time.perf_counter() - t0
+    train, _ = U.split_soils(len(params), 0.05, 0)
+    net = U.Net(U.NetConfig(total_steps=warmup + steps, loss_mode=gfk._native.LOSS_PLAIN), eng)
+    net.scales_from(ds)
+    net.train(ds, train, warmup)
+    launches0 = eng.kernel_launches()
+    t0 = time.perf_counter()
+    net.train(ds, train, steps)  # returns after the stream is synchronised
+    dt = allmax(time.perf_counter() - t0, world)
+    launches = eng.kernel_launches() - launches0
+    B = net.config.batch
+    flops = 2 * B * (128 * 512 + 4 * 512 * 512 + 2 * 512) * 3 - 2 * B * 128 * 512  # fwd + dX + dW, no dX0
+    ms = 1e3 * dt / steps
+    pk = measured_peaks()
+    out["train"] = {"workload": "surrogate training: 8192 3-layer soils x 64 ranges x 512 bins of FP64 labels "
+                                f"({label_s:.1f} s), batch 8192, 128 features -> 5 x 512 SiLU -> 2, AdamW",
+                    "value": B * steps * world / dt, "unit": "samples/s", "ms_per_step": ms, "steps": steps,
+                    "warmup": warmup, "gpu_launches": int(launches), "dtype": "bf16",
+                    "roofline": {"bound": "tensor", "achieved": flops / (ms * 1e-3) / 1e12,
+                                 "peak": pk.get("bf16_tflops"), "unit": "TFLOP/s",
+                                 "frac": flops / (ms * 1e-3) / 1e12 / pk["bf16_tflops"] if pk.get("bf16_tflops") else None,
+                                 "peak_source": pk["source"]}}
+    net.close()
+    ds.close()
+    rng = np.random.default_rng(20240611)
+    p11 = U.from_sobol(S.unit_to_params(rng.random((16384, 8))))
+    ds = U.Dataset(p11, U.LabelGrid(), floor_rel=1e-6, engine=eng).fill(batch_soils=8192)
+    train, _ = U.split_soils(len(p11), 0.05, 0)
+    t0 = time.perf_counter()
+    cfg = U.NetConfig(total_steps=20000, lr_max=1e-3, warmup_steps=200)
+    nets = U.train_ensemble(ds, train, members=3, steps=20000, config=cfg, engine=eng, ranges=(9, 10))
+    train_s = time.perf_counter() - t0
+    ds.close()
+    S.run_plain(eng, n=256, seed=0)  # warm-up of both paths (allocator, first launches)
+    S.run_surrogate(eng, nets, n=256, seed=0, threshold=0.01, gate="rows", amp_threshold=0.001)
+    plain = S.run_plain(eng, n=256, seed=0)
+    sur = S.run_surrogate(eng, nets, n=256, seed=0, threshold=0.01, gate="rows", amp_threshold=0.001)
+    for n_ in nets:
+        n_.close()
+    err = max(abs(getattr(sur, kind)[o][q] - getattr(plain, kind)[o][q])
+              for kind in ("s1", "st") for o in ("peak", "centroid") for q in getattr(sur, kind)[o])
+    out["surrogate"] = {"workload": "Saltelli N=256, d=8 (2560 soils x 512 bins at 10 m); 3 members trained 20,000 "
+                                    f"steps on 16,384 Sobol-box soils at the sensor range ({train_s:.1f} s, not counted); "
+                                    "row gate: members disagree by > 1% of the trace-spectrum peak or predicted "
+                                    "|G S| > 0.1% of it",
+                        "fk_rows_fraction": sur.seconds["fallback_fraction"],
+                        "speedup_wall": plain.seconds["total"] / sur.seconds["total"],
+                        "timing": "wall time of each whole run after one untimed run of each",
+                        "plain_s": plain.seconds["total"], "surrogate_s": sur.seconds["total"],
+                        "max_index_abs_error": err,
+                        "peak_metric_rel_error_p90": float(np.percentile(
+                            np.abs(sur.metrics["peak"] / plain.metrics["peak"] - 1), 90))}
+    return out
+
+
 def batched_leg(gfk, torch, eng, local, rank, world, fp64_peak, steps=3, cpu=True):
     """The 4096 seeded uneven soils (256-2048 bins each, 8192 wavenumbers, 128
     ranges; this rank's share) as one batch plan with the split sum, for the
@@ -1028,7 +1099,7 @@ def main():
     ap.add_argument("--quadrature", default="split", choices=["split", "fp64"],
                     help="split: exact int8-slice tensor-core sum (default); fp64: the plain FP64 sum")
     ap.add_argument("--no-batched", action="store_true",
-                    help="default workload: skip the single-soil and batched uneven-soils objects in the line")
+                    help="default workload: skip the single-soil, batched, training and surrogate objects in the line")
     ap.add_argument("--profile", action="store_true",
                     help="profiling only: skip the e2e leg, the FP64 peak probe and the CPU baseline")
     args = ap.parse_args()
@@ -1203,8 +1274,9 @@ def main():
         cb.pop("status_ok", None)
     plan.close()
     del flush
-    single = batched = None
+    single = batched = learned = None
     if not args.no_batched and args.workload == "graded" and args.freq_stride == 1:
+        learned = learned_leg(gfk, torch, eng, world)
         single = single_leg(gfk, torch, eng, local, world, fp64_peak,
                             cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
         batched = batched_leg(gfk, torch, eng, local, rank, world, fp64_peak,
@@ -1228,6 +1300,8 @@ def main():
             out["cpu_baseline"] = cb
         if plain_leg:
             out["plain_fp64"] = plain_leg
+        if learned:
+            out.update(learned)
         if single:
             out["single"] = single
         if batched:
