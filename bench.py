@@ -522,7 +522,9 @@ def batched_leg(gfk, torch, eng, local, rank, world, fp64_peak, steps=3, cpu=Tru
     t0 = time.perf_counter()
     plan = gfk.Batch(media(gfk.SPLIT_INT8), freqs, ranges, opt, engine=eng)
     build_s = time.perf_counter() - t0
-    plan.execute()  # first execute: launch-shape tuning and the Hankel weights
+    plan.execute()  # first execute: launch-shape and tile-shape tuning, the Hankel weights
+    prop_shape = plan.tuning()
+    tc_shape = plan.quad_shape()
     plan.kernel_times(reset=True)
     plan.execute()  # one execute timed kernel by kernel
     prop_ms, quad_ms, other_ms = plan.kernel_times(reset=True)
@@ -604,6 +606,9 @@ def batched_leg(gfk, torch, eng, local, rank, world, fp64_peak, steps=3, cpu=Tru
                      "over ranks; the 9.7 GB result and the 4 GB integrand chunks exceed L2, so no flush",
            "soils_per_rank": len(mine), "rows_per_rank": nrows, "cells_per_step": cells_all,
            "plan_build_s": build_s, "gpu_launches": launches,
+           "autotuned": {"propagator_launch_shape": prop_shape[0], "propagator_tuning_ms": prop_shape[1],
+                         "tensor_core_tile": {"ranges_per_cta": tc_shape[0], "stages": tc_shape[1],
+                                              "tuning_ms_per_shape": tc_shape[2]}},
            "kernel_ms": {"propagator": prop_ms, "quadrature": quad_ms, "other": other_ms},
            "e2e": {"value": cells_all / e2e_s, "unit": UNIT, "s_per_step": e2e_s, "steps": 1,
                    "h2d_bytes_per_step": layers * 48 + nrows * 8,
@@ -1143,6 +1148,7 @@ def main():
     assert (status == 0).all() and np.isfinite(got).all()
     plan.kernel_times(reset=True)
     variant, tune_ms = plan.tuning()
+    tc_tn, tc_stages, tc_tune_ms = plan.quad_shape()
 
     # --- device-resident timing: the stream span of each execute ----------
     clocks = ClockSampler(local)
@@ -1263,7 +1269,11 @@ def main():
                 "kernel_ms": {"propagator": prop_ms, "quadrature": quad_ms, "other": other_ms},
                 "propagator_launch_shape": {"chosen": variant, "tuning_ms": tune_ms},
                 "quadrature": {"path": "split int8 slices on tcgen05 (10 slice GEMMs)" if quad == gfk.SPLIT_INT8
-                               else "plain FP64", "ms": quad_ms,
+                               else "plain FP64 on the FP64 tensor cores", "ms": quad_ms,
+                               "tile_shape": {"ranges_per_cta": tc_tn, "stages": tc_stages,
+                                              "tuning_ms_per_shape": tc_tune_ms,
+                                              "shapes": "(128, 3), (128, 2), (64, 4), (64, 3)"}
+                               if quad == gfk.SPLIT_INT8 else None,
                                "useful_tflops": f_quad / (quad_ms * 1e-3) / 1e12,
                                "int8_tops_executed": (10 * 2 * 2 * len(f) * len(r) * wl.samples) / (quad_ms * 1e-3) / 1e12
                                if quad == gfk.SPLIT_INT8 else None},

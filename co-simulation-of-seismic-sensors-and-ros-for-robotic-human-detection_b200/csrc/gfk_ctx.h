@@ -27,6 +27,11 @@ struct gfk_ctx {
         int nl, nk, variant;
     };
     std::vector<Tuned> tuned;
+    // tensor-core sum tile shape chosen by tuning, per padded (rows, ranges, wavenumbers)
+    struct TunedTc {
+        int Mp, Np, Kp, variant;
+    };
+    std::vector<TunedTc> tuned_tc;
 };
 
 // Frees every surrogate object the context still holds (gfk_surrogate.cu).

@@ -227,6 +227,8 @@ struct gfk_plan {
     bool weights_ready = false;
     int prop_variant = -1;       // Dunkin launch shape; -1 until the first execute tunes it
     std::vector<float> tune_ms;  // per variant, from the tuning run
+    int tc_variant = -1;            // tensor-core sum tile shape; -1 until the first execute tunes it
+    std::vector<float> tc_tune_ms;  // per shape, from the tuning run
     // end-to-end call into pinned host memory: each chunk's rows are copied
     // out on the context's copy stream while the next chunk computes
     double* async_out = nullptr;
@@ -639,6 +641,57 @@ int tune_prop(gfk_plan* p) {
     return GFK_OK;
 }
 
+// Times every tile shape of the tensor-core sum on the first row chunk (its
+// slices are in place) and keeps the fastest; the context remembers the
+// choice per padded (rows, ranges, wavenumbers). The timed launches write the
+// chunk's result rows, which the real launch then recomputes.
+// GFK_QUAD_TC_VARIANT=<index> forces a shape.
+int tune_tc(gfk_plan* p, int fb, int cnf, double dk) {
+    gfk_ctx* ctx = p->ctx;
+    cudaStream_t s = ctx->stream;
+    const int nv = gfk::quad_tc_variant_count();
+    p->tc_variant = 0;
+    if (const char* env = getenv("GFK_QUAD_TC_VARIANT")) {
+        p->tc_variant = std::max(0, std::min(nv - 1, atoi(env)));
+        return GFK_OK;
+    }
+    for (const auto& t : ctx->tuned_tc)
+        if (t.Mp == p->Mp && t.Np == p->Np && t.Kp == p->Kp) {
+            p->tc_variant = t.variant;
+            return GFK_OK;
+        }
+    cudaEvent_t a, b;
+    GFK_CUDA(ctx, cudaEventCreate(&a));
+    GFK_CUDA(ctx, cudaEventCreate(&b));
+    p->tc_tune_ms.assign(nv, INFINITY);
+    for (int rep = 0; rep < 2; rep++)
+        for (int v = 0; v < nv; v++) {
+            cudaEventRecord(a, s);
+            const int rc = gfk::launch_quad_tc(s, p->d_A, p->d_B, 2 * cnf, p->nr, p->Mp, p->Np, p->Kp, p->d_rowexp,
+                                               p->col_exp, p->d_C + fb, p->d_ranges, dk, p->d_G + (size_t)fb * p->nr,
+                                               p->d_status + fb, p->ksplit, p->d_ksum, v);
+            cudaEventRecord(b, s);
+            ctx->launches += 1 + (p->ksplit > 1 ? 1 : 0);
+            cudaError_t e = rc ? cudaErrorInvalidValue : cudaEventSynchronize(b);
+            if (e != cudaSuccess) {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+                return fail(ctx, GFK_ECUDA, "tensor-core sum tuning (shape %d): %s", v, cudaGetErrorString(e));
+            }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            p->tc_tune_ms[v] = std::min(p->tc_tune_ms[v], ms);
+        }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    int best = 0;
+    for (int v = 1; v < nv; v++)
+        if (p->tc_tune_ms[v] < p->tc_tune_ms[best]) best = v;
+    p->tc_variant = best;
+    ctx->tuned_tc.push_back({p->Mp, p->Np, p->Kp, best});
+    return GFK_OK;
+}
+
 // With async_out set, queues the download of rows [fb, fb + n) on the copy
 // stream once the compute stream has finished them.
 int copy_chunk_out(gfk_plan* p, int fb, int n) {
@@ -703,9 +756,10 @@ int plan_enqueue(gfk_plan* p, bool timed) {
         if (timed && (st = begin_seg(p, 1, &seg))) return st;
         if (p->tc) {
             gfk::launch_slice_rem(s, p->d_rem, p->g_n, p->Kp, p->Mp, cnf, p->d_rowmax, p->d_rowexp, p->d_A);
+            if (timed && p->tc_variant < 0 && (st = tune_tc(p, fb, cnf, dk))) return st;
             if (gfk::launch_quad_tc(s, p->d_A, p->d_B, 2 * cnf, p->nr, p->Mp, p->Np, p->Kp, p->d_rowexp, p->col_exp,
                                     p->d_C + fb, p->d_ranges, dk, p->d_G + (size_t)fb * p->nr, p->d_status + fb,
-                                    p->ksplit, p->d_ksum))
+                                    p->ksplit, p->d_ksum, std::max(p->tc_variant, 0)))
                 return fail(ctx, GFK_ECUDA, "tensor-core quadrature launch setup failed");
             ctx->launches += 1 + (p->ksplit > 1 ? 1 : 0);
         } else if (p->shared) {
@@ -731,7 +785,7 @@ int plan_exec(gfk_plan* p) {
         return GFK_OK;
     }
     int st = GFK_OK;
-    if (p->use_graph && p->executed && p->prop_variant >= 0) {
+    if (p->use_graph && p->executed && p->prop_variant >= 0 && (!p->tc || p->tc_variant >= 0)) {
         if (!p->gexec) {  // capture one whole execute, once
             const int64_t before = ctx->launches;
             cudaGraph_t g = nullptr;
@@ -933,6 +987,17 @@ int gfk_plan_tuning(const gfk_plan* p, int32_t* variant, float* ms_per_variant, 
     *variant = p->prop_variant;
     const int n = (int)p->tune_ms.size();
     for (int i = 0; ms_per_variant && i < std::min(n, (int)capacity); i++) ms_per_variant[i] = p->tune_ms[i];
+    return n;
+}
+
+int gfk_plan_quad_shape(const gfk_plan* p, int32_t* tile_n, int32_t* stages, float* ms_per_shape, int32_t capacity) {
+    if (!p || !tile_n || !stages) return GFK_EARG;
+    int tn = 0, ns = 0;
+    if (p->tc && p->tc_variant >= 0) gfk::quad_tc_variant_shape(p->tc_variant, &tn, &ns);
+    *tile_n = tn;
+    *stages = ns;
+    const int n = (int)p->tc_tune_ms.size();
+    for (int i = 0; ms_per_shape && i < std::min(n, (int)capacity); i++) ms_per_shape[i] = p->tc_tune_ms[i];
     return n;
 }
 

@@ -38,11 +38,15 @@ void launch_slice_rem(cudaStream_t s, const cd* rem, int nk, int Kp, int Mp, int
                       int* row_exp, int8_t* A);
 // splits > 1 divides the K blocks among blockIdx.z and writes the head-free
 // partial sums to part [splits][M/2][N]; launch_quad_finish then adds them.
-// wait_cycles bounds each mbarrier wait (<= 0: the default ~1 s); starve is
-// the self-test's: the producer issues nothing, so the waits run out.
+// variant picks the tile shape (quad_tc_variant_shape: ranges per CTA and
+// pipeline stages); wait_cycles bounds each mbarrier wait (<= 0: the default
+// ~1 s); starve is the self-test's: the producer issues nothing, so the waits
+// run out.
 int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int N, int Mp, int Np, int Kp,
                    const int* row_exp, int col_exp, const cd* C, const double* ranges, double dk, cd* G, int* status,
-                   int splits, cd* part, long long wait_cycles = 0, int starve = 0);
+                   int splits, cd* part, int variant = 0, long long wait_cycles = 0, int starve = 0);
+int quad_tc_variant_count();
+void quad_tc_variant_shape(int variant, int* tile_n, int* stages);
 int quad_tc_selftest_timeout(cudaStream_t s, long long wait_cycles, int* timed_out);
 int quad_tc_splits(int M, int N, int Kp);  // split count filling the SMs for one chunk shape
 

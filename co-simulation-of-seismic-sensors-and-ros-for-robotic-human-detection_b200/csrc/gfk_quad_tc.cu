@@ -35,19 +35,26 @@
 namespace gfk {
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 64;  // BK in int8 elements (bytes)
-constexpr int S = 4;                        // slices per operand
-constexpr int STAGES = 3;
-constexpr int TILE = BM * BK;               // 8192 bytes, A and B tiles alike
-constexpr int STAGE_BYTES = 2 * S * TILE;   // 65536
-constexpr int TMEM_COLS = S * BN;           // 512: one 128-column s32 accumulator per level
+constexpr int BM = 128, BK = 64;  // BK in int8 elements (bytes)
+constexpr int S = 4;              // slices per operand
+constexpr int TILE_A = BM * BK;   // 8192 bytes per A slice tile
 constexpr int THREADS = 192;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 
-static_assert(BN == BM, "A and B tiles share one size");
+// Tile shapes the plan's tuner chooses among: TN output ranges per CTA (64 or
+// 128; four TN-column s32 accumulators in TMEM) and NST pipeline stages.
+template <int TN, int NST>
+struct Shape {
+    static constexpr int TILE_B = TN * BK;
+    static constexpr int STAGE_BYTES = S * (TILE_A + TILE_B);
+    static constexpr int TMEM_COLS = S * TN;
+    static constexpr int SMEM_BYTES = NST * STAGE_BYTES + 1024 + 256;
+    static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per CTA");
+    static_assert(TMEM_COLS == 256 || TMEM_COLS == 512, "TMEM allocation");
+};
 
-// Instruction descriptor: s8 x s8 -> s32, both K-major, M = 128, N = 128.
-__host__ __device__ inline uint32_t idesc_i8_128x128() {
+// Instruction descriptor: s8 x s8 -> s32, both K-major, M = 128, N = TN.
+template <int TN>
+__host__ __device__ inline uint32_t idesc_i8() {
     cute::UMMA::InstrDescriptor id;
     id.desc_ = 0;
     id.c_format_ = 2;  // S32
@@ -55,7 +62,7 @@ __host__ __device__ inline uint32_t idesc_i8_128x128() {
     id.b_format_ = 1;
     id.a_major_ = 0;   // K-major
     id.b_major_ = 0;
-    id.n_dim_ = BN >> 3;
+    id.n_dim_ = TN >> 3;
     id.m_dim_ = BM >> 4;
     return id.desc_;
 }
@@ -75,8 +82,12 @@ struct Args {
     int starve;         // self-test only: the producer issues no loads, so the first wait runs out
 };
 
+template <int TN, int NST>
 __global__ void __launch_bounds__(THREADS, 1)
     k_quad_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Args a) {
+    using Sh = Shape<TN, NST>;
+    constexpr int STAGES = NST, STAGE_BYTES = Sh::STAGE_BYTES, TMEM_COLS = Sh::TMEM_COLS;
+    constexpr int BN = TN, TILE_B = Sh::TILE_B;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -128,10 +139,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                 uint8_t* base = smem + st * STAGE_BYTES;
 #pragma unroll
                 for (int s = 0; s < S; s++)
-                    tma_load_2d(base + s * TILE, &tmA, &full[st], (kb0 + kb) * BK, s * a.Mp + m0);
+                    tma_load_2d(base + s * TILE_A, &tmA, &full[st], (kb0 + kb) * BK, s * a.Mp + m0);
 #pragma unroll
                 for (int t = 0; t < S; t++)
-                    tma_load_2d(base + (S + t) * TILE, &tmB, &full[st], (kb0 + kb) * BK, t * a.Np + n0);
+                    tma_load_2d(base + S * TILE_A + t * TILE_B, &tmB, &full[st], (kb0 + kb) * BK, t * a.Np + n0);
                 issued = kb + 1;
             }
             // drain: the last loads of each stage land before the CTA may exit
@@ -140,7 +151,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t idesc = idesc_i8_128x128();
+            const uint32_t idesc = idesc_i8<TN>();
             bool init[S] = {false, false, false, false};
             for (int kb = 0; kb < nkb; kb++) {
                 const int st = kb % STAGES;
@@ -158,8 +169,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                         const int t = lvl - s;
 #pragma unroll
                         for (int kk = 0; kk < BK / 32; kk++) {
-                            const uint64_t da = sdesc_k_sw64(base + s * TILE + kk * 32);
-                            const uint64_t db = sdesc_k_sw64(base + (S + t) * TILE + kk * 32);
+                            const uint64_t da = sdesc_k_sw64(base + s * TILE_A + kk * 32);
+                            const uint64_t db = sdesc_k_sw64(base + S * TILE_A + t * TILE_B + kk * 32);
                             tc_mma_i8(tmem + lvl * BN, da, db, idesc, init[lvl] ? 1u : 0u);
                             init[lvl] = true;
                         }
@@ -329,20 +340,42 @@ __global__ void k_j0_slices(const double* __restrict__ ranges, int nr, int nk, i
 // ------------------------------------------------------------------ host --
 
 namespace {
-// A [planes*rows_p][Kp] int8 plane stack; box = 128 rows x 64 bytes, SWIZZLE_64B.
-bool make_map(CUtensorMap* map, const int8_t* base, int rows_total, int Kp) {
+// A [planes*rows_p][Kp] int8 plane stack; box = box_rows x 64 bytes, SWIZZLE_64B.
+bool make_map(CUtensorMap* map, const int8_t* base, int rows_total, int Kp, int box_rows) {
     auto fn = tc::encode_fn();
     if (!fn) return false;
     cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows_total};
     cuuint64_t strides[1] = {(cuuint64_t)Kp};
-    cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)tc::BM};
+    cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(base), dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
+
+// The tile shapes a plan's tuner times: (ranges per CTA, pipeline stages).
+struct TcVariant {
+    void (*fn)(const CUtensorMap, const CUtensorMap, tc::Args);
+    int tn, stages, smem;
+    bool attr;
+};
+TcVariant g_tc_variants[] = {
+    {tc::k_quad_tc<128, 3>, 128, 3, tc::Shape<128, 3>::SMEM_BYTES, false},
+    {tc::k_quad_tc<128, 2>, 128, 2, tc::Shape<128, 2>::SMEM_BYTES, false},
+    {tc::k_quad_tc<64, 4>, 64, 4, tc::Shape<64, 4>::SMEM_BYTES, false},
+    {tc::k_quad_tc<64, 3>, 64, 3, tc::Shape<64, 3>::SMEM_BYTES, false},
+};
+constexpr int kTcVariants = sizeof(g_tc_variants) / sizeof(g_tc_variants[0]);
 }  // namespace
+
+int quad_tc_variant_count() { return kTcVariants; }
+
+void quad_tc_variant_shape(int variant, int* tile_n, int* stages) {
+    const TcVariant& v = g_tc_variants[(variant >= 0 && variant < kTcVariants) ? variant : 0];
+    *tile_n = v.tn;
+    *stages = v.stages;
+}
 
 int tc_col_exp(double dk) { return ilogb(dk * (128.0 / 127.0)) + 1; }
 
@@ -359,8 +392,9 @@ void launch_slice_rem(cudaStream_t s, const cd* rem, int nk, int Kp, int Mp, int
 }
 
 int quad_tc_splits(int M, int N, int Kp) {
-    // one CTA per SM (its shared memory); each split keeps at least 4 K blocks
-    const long long tiles = (long long)((M + tc::BM - 1) / tc::BM) * ((N + tc::BN - 1) / tc::BN);
+    // one CTA per SM (its shared memory); each split keeps at least 4 K blocks.
+    // Counted with the widest tile, so every shape's splits fit the plan's workspace.
+    const long long tiles = (long long)((M + tc::BM - 1) / tc::BM) * ((N + 127) / 128);
     const int nkb = Kp / tc::BK;
     if (tiles >= 74 || nkb < 8) return 1;
     const int want = (int)((148 + tiles - 1) / tiles);
@@ -369,23 +403,22 @@ int quad_tc_splits(int M, int N, int Kp) {
 
 int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int N, int Mp, int Np, int Kp,
                    const int* row_exp, int col_exp, const cd* C, const double* ranges, double dk, cd* G, int* status,
-                   int splits, cd* part, long long wait_cycles, int starve) {
-    if (Mp % tc::BM || Np % tc::BN || Kp % tc::BK || M > Mp || N > Np) return 1;
+                   int splits, cd* part, int variant, long long wait_cycles, int starve) {
+    if (variant < 0 || variant >= kTcVariants) variant = 0;
+    TcVariant& v = g_tc_variants[variant];
+    if (Mp % tc::BM || Np % v.tn || Kp % tc::BK || M > Mp || N > Np) return 1;
     if (splits < 1 || !part) splits = 1;
     if (splits > Kp / tc::BK) return 1;
     CUtensorMap ta, tb;
-    if (!make_map(&ta, A, tc::S * Mp, Kp) || !make_map(&tb, B, tc::S * Np, Kp)) return 2;
-    static bool attr_set = false;
-    if (!attr_set) {
-        if (cudaFuncSetAttribute(tc::k_quad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES) !=
-            cudaSuccess)
-            return 3;
-        attr_set = true;
+    if (!make_map(&ta, A, tc::S * Mp, Kp, tc::BM) || !make_map(&tb, B, tc::S * Np, Kp, v.tn)) return 2;
+    if (!v.attr) {
+        if (cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, v.smem) != cudaSuccess) return 3;
+        v.attr = true;
     }
     tc::Args a{M, N, Mp, Np, Kp, row_exp, col_exp, C, ranges, dk, G, status, splits > 1 ? part : nullptr,
                wait_cycles > 0 ? wait_cycles : tc::kWaitCycles, starve};
-    dim3 grid(Np / tc::BN, Mp / tc::BM, splits);
-    tc::k_quad_tc<<<grid, tc::THREADS, tc::SMEM_BYTES, s>>>(ta, tb, a);
+    dim3 grid((N + v.tn - 1) / v.tn, Mp / tc::BM, splits);
+    v.fn<<<grid, tc::THREADS, v.smem, s>>>(ta, tb, a);
     if (splits > 1) launch_quad_finish(s, part, splits, C, ranges, M >> 1, N, dk, G);
     return 0;
 }
@@ -414,7 +447,7 @@ int quad_tc_selftest_timeout(cudaStream_t s, long long wait_cycles, int* timed_o
     alloc((void**)&C, sizeof(cd) * nf);
     alloc((void**)&G, sizeof(cd) * nf * N);
     alloc((void**)&ranges, sizeof(double) * N);
-    if (!rc) rc = launch_quad_tc(s, A, B, M, N, M, N, Kp, row_exp, 0, C, ranges, 1.0, G, status, 1, nullptr,
+    if (!rc) rc = launch_quad_tc(s, A, B, M, N, M, N, Kp, row_exp, 0, C, ranges, 1.0, G, status, 1, nullptr, 0,
                                  wait_cycles, 1);
     if (!rc && cudaGetLastError() != cudaSuccess) rc = 12;
     int host[64] = {0};

@@ -347,6 +347,14 @@ class Plan:
         n = N.lib().gfk_plan_tuning(self.p, ctypes.byref(v), ms, 16)
         return int(v.value), [float(ms[i]) for i in range(max(n, 0))]
 
+    def quad_shape(self):
+        """(ranges per CTA, pipeline stages, ms per shape) of the tensor-core
+        sum chosen by the first execute; (0, 0, []) otherwise."""
+        tn, ns = ctypes.c_int32(), ctypes.c_int32()
+        ms = (ctypes.c_float * 16)()
+        n = N.lib().gfk_plan_quad_shape(self.p, ctypes.byref(tn), ctypes.byref(ns), ms, 16)
+        return int(tn.value), int(ns.value), [float(ms[i]) for i in range(max(n, 0))]
+
     def kernel_times(self, reset=False):
         """(propagator, quadrature, other) ms per execute, CUDA-event timed."""
         a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()

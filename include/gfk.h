@@ -216,6 +216,15 @@ int32_t gfk_plan_launches_per_execute(const gfk_plan *p);
  * environment variable GFK_PROP_VARIANT=<index> forces one instead. Writes the chosen index and up
  * to `capacity` measured times (ms); returns the number of shapes. */
 int gfk_plan_tuning(const gfk_plan *p, int32_t *variant, float *ms_per_variant, int32_t capacity);
+/* The tensor-core sum's tile shape (GFK_SPLIT_INT8 on a shared grid): the
+ * plan's first execute times each shape (ranges per CTA: 128 or 64; pipeline
+ * stages: 2-4) on its first row chunk and keeps the fastest; the context
+ * remembers the choice per padded (rows, ranges, wavenumbers).
+ * GFK_QUAD_TC_VARIANT=<index> forces one. Writes the chosen shape (0 and 0
+ * before the first execute or for other sums) and up to `capacity` measured
+ * times (ms); returns the number of shapes timed. */
+int gfk_plan_quad_shape(const gfk_plan *p, int32_t *tile_n, int32_t *stages, float *ms_per_shape,
+                        int32_t capacity);
 /* Average duration in ms of the dominant kernel (the quadrature or the
  * propagator, whichever took longer) over the executes since the last reset,
  * timed with CUDA events on the plan's stream; name receives its label. */

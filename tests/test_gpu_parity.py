@@ -554,3 +554,26 @@ def test_tensor_core_wait_timeout_is_reported_and_context_survives(gfk, engine):
     b, sb = plain.bank_spectra(wl.ranges, wl.freqs[::8], wl.integration())
     assert (sa == 0).all() and (sb == 0).all()
     assert rel_l2(a, b) < 1e-6
+
+
+@pytest.mark.parametrize("shape", [0, 1, 2, 3], ids=["n128_s3", "n128_s2", "n64_s4", "n64_s3"])
+def test_split_sum_every_tile_shape(gfk, engine, shape, monkeypatch):
+    """Every tile shape the plan's tuner can choose for the tensor-core sum
+    (128 or 64 ranges per CTA, 2-4 pipeline stages), forced in turn, on ragged
+    sizes (200 ranges, 3000 wavenumbers, 171 frequencies): the same bank as
+    the FP64 sum within the split sum's 1e-6."""
+    monkeypatch.setenv("GFK_QUAD_TC_VARIANT", str(shape))
+    wl = gfk.workloads.single_soil()
+    ranges = np.arange(1.0, 201.0) * 0.5
+    freqs = wl.freqs[::3]
+    opt = gfk.Integration(3000, 0.0, wl.kmax)
+    split = wl.medium(gfk.DUNKIN, engine=engine, quadrature=gfk.SPLIT_INT8)
+    plan = gfk.Plan(split, ranges, freqs, opt, engine=engine)
+    plan.execute()
+    got, st = plan.download()
+    tn, ns, _ = plan.quad_shape()
+    plan.close()
+    assert (tn, ns) == [(128, 3), (128, 2), (64, 4), (64, 3)][shape]
+    want, sw = wl.medium(gfk.DUNKIN, engine=engine).bank_spectra(ranges, freqs, opt)
+    assert (st == 0).all() and (sw == 0).all()
+    assert rel_l2(got, want) < 1e-6
