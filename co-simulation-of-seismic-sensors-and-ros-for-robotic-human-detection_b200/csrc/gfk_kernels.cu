@@ -400,10 +400,12 @@ template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 }  // namespace qd
 
+// Not volatile: the result is used, and the compiler may move the next
+// step's fragment loads ahead of these MMAs.
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(c0), "+d"(c1)
-                 : "d"(a), "d"(b));
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(c0), "+d"(c1)
+        : "d"(a), "d"(b));
 }
 
 template <int TNW>
@@ -471,17 +473,25 @@ __global__ __launch_bounds__(qd::THREADS, TNW == 8 ? 1 : 2) void k_quad_gemm(con
         qd::cp_commit();
         const double* a = sA + (t % STAGES) * BK * ASTR + fa;
         const double* b = sB + (t % STAGES) * BK * BSTR + fb;
+        // fragments of step k4 + 1 are loaded while step k4's MMAs issue
+        double av[2][4], bv[2][TNW];
+#pragma unroll
+        for (int i = 0; i < 4; i++) av[0][i] = a[8 * i];
+#pragma unroll
+        for (int j = 0; j < TNW; j++) bv[0][j] = b[8 * j];
 #pragma unroll
         for (int k4 = 0; k4 < BK / 4; k4++) {
-            double av[4], bv[TNW];
+            const int c = k4 & 1;
+            if (k4 + 1 < BK / 4) {
 #pragma unroll
-            for (int i = 0; i < 4; i++) av[i] = a[4 * k4 * ASTR + 8 * i];
+                for (int i = 0; i < 4; i++) av[c ^ 1][i] = a[4 * (k4 + 1) * ASTR + 8 * i];
 #pragma unroll
-            for (int j = 0; j < TNW; j++) bv[j] = b[4 * k4 * BSTR + 8 * j];
+                for (int j = 0; j < TNW; j++) bv[c ^ 1][j] = b[4 * (k4 + 1) * BSTR + 8 * j];
+            }
 #pragma unroll
             for (int i = 0; i < 4; i++)
 #pragma unroll
-                for (int j = 0; j < TNW; j++) dmma(acc[i][j][0], acc[i][j][1], av[i], bv[j]);
+                for (int j = 0; j < TNW; j++) dmma(acc[i][j][0], acc[i][j][1], av[c][i], bv[c][j]);
         }
     }
     qd::cp_wait<0>();
