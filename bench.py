@@ -357,6 +357,24 @@ def abi_bank_spectra(gfk, eng, med, wl, out_host, status_host):
     eng.check(st)
 
 
+def abi_bank_payload(gfk, eng, med, wl, bins, out_host, status_host):
+    """geobank's own output through the C ABI: gfk_bank_payload, the bank
+    file's float32 range-major payload packed on the device and downloaded
+    into the pinned `out_host` (2 nr bins float32)."""
+    from gfk_b200.fk import _c_medium
+    N = gfk._native
+    r = np.ascontiguousarray(wl.ranges)
+    f = np.ascontiguousarray(wl.freqs)
+    with _c_medium(med) as cm:
+        st = N.lib().gfk_bank_payload(eng.ctx, ctypes.byref(cm), ctypes.byref(med._solve()),
+                                      r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r),
+                                      f.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(f),
+                                      wl.integration().c(), 1, bins,
+                                      ctypes.cast(out_host.data_ptr(), ctypes.POINTER(ctypes.c_float)),
+                                      ctypes.cast(status_host.data_ptr(), ctypes.POINTER(ctypes.c_int32)))
+    eng.check(st)
+
+
 def single_leg(gfk, torch, eng, local, world, fp64_peak, steps=20, warmup=5, cpu=True):
     """The single-soil workload (2 layers over a half-space, 512 bins x 64
     ranges, 4096 wavenumbers) for the default bench line, in the plain FP64
@@ -1199,6 +1217,13 @@ def main():
         e2e_call()
     e2e_s = allmax((time.perf_counter() - t0) / max(args.steps, 1), world)
     e2e_value = cells_all / e2e_s
+    bins = wl.transform_samples // 2 + 1
+    pay_host = torch.empty(2 * len(wl.ranges) * bins, dtype=torch.float32, pin_memory=True)
+    abi_bank_payload(gfk, eng, med, wl, bins, pay_host, status_host)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        abi_bank_payload(gfk, eng, med, wl, bins, pay_host, status_host)
+    pay_s = allmax((time.perf_counter() - t0) / max(args.steps, 1), world)
     nl = len(wl.stack)
     h2d = nl * 48 + len(r) * 8 + len(f) * (8 + 8 + 8 + 4 + 8)
     d2h = len(f) * len(r) * 16 + len(f) * 4
@@ -1304,6 +1329,11 @@ def main():
                           "kernel_sum_ms_per_step": kernel_sum_ms},
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                        "ms_per_step": e2e_s * 1e3},
+               "e2e_bank_payload": {"value": cells_all / pay_s, "unit": UNIT, "ms_per_step": pay_s * 1e3,
+                                    "h2d_bytes_per_step": h2d,
+                                    "d2h_bytes_per_step": 8 * len(wl.ranges) * bins + 4 * len(wl.freqs),
+                                    "note": "geobank's output: gfk_bank_payload packs the bank file's float32 "
+                                            "range-major payload on the device and downloads only that"},
                "gpu_launches": launches, "clocks": clk, "roofline": roofline,
                "wall_s_timed_region": wall}
         if cb:

@@ -29,7 +29,7 @@ EXPORTS = [
     "gfk_open", "gfk_close", "gfk_status_string", "gfk_last_error", "gfk_kernel_launches", "gfk_stream", "gfk_selftest_wait_timeout",
     "gfk_stack_validate", "gfk_check_layer_phase", "gfk_grid_for",
     "gfk_surface_response", "gfk_static_coefficient", "gfk_vertical_displacement",
-    "gfk_vertical_displacement_multi", "gfk_bank_spectra",
+    "gfk_vertical_displacement_multi", "gfk_bank_spectra", "gfk_bank_payload",
     "gfk_plan_create", "gfk_plan_execute", "gfk_plan_result_device", "gfk_plan_download",
     "gfk_plan_launches_per_execute", "gfk_plan_tuning", "gfk_plan_quad_shape", "gfk_plan_kernel_times", "gfk_plan_destroy",
     "gfk_plan_use_graph", "gfk_batch_create",
@@ -120,6 +120,8 @@ def lib():
                                                            GfkIntegration, P(d)]),
         "gfk_bank_spectra": (ctypes.c_int, [vp, P(GfkMedium), P(GfkSolve), P(d), i32, P(d), i32, GfkIntegration,
                                             P(d), P(i32)]),
+        "gfk_bank_payload": (ctypes.c_int, [vp, P(GfkMedium), P(GfkSolve), P(d), i32, P(d), i32, GfkIntegration, i32,
+                                            i32, P(ctypes.c_float), P(i32)]),
         "gfk_plan_create": (ctypes.c_int, [vp, P(GfkMedium), P(GfkSolve), P(d), i32, P(d), i32, GfkIntegration,
                                            P(vp)]),
         "gfk_plan_execute": (ctypes.c_int, [vp]),

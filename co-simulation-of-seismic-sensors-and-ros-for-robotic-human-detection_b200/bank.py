@@ -330,10 +330,12 @@ def open_bank(path):
     return Bank(h, data)
 
 
-def build_bank(medium, header, max_freq, opt=None, check_range_sampling=True):
+def build_bank(medium, header, max_freq, opt=None, check_range_sampling=True, spectra=False):
     """geobank build (cmd/geobank/main.go:51-178) on the GPU: bins 1..topBin are
-    computed in one batched call, DC and bins above max_freq stay zero; the
-    first failing bin aborts the build as geobank does."""
+    computed in one batched call and packed into the float32 payload on the
+    device (gfk_bank_payload); DC and bins above max_freq stay zero; the
+    first failing bin aborts the build as geobank does. Returns (bank, the
+    FP64 spectra [bins, ranges] if spectra=True — a second solve — else None)."""
     header.validate()
     if check_range_sampling:
         header.check_range_sampling(max_freq)
@@ -342,9 +344,10 @@ def build_bank(medium, header, max_freq, opt=None, check_range_sampling=True):
     if top >= header.bins():
         top = header.bins() - 1
     if top < 1:
-        return b, np.zeros((0, header.ranges.count), dtype=np.complex128)
+        return b, (np.zeros((0, header.ranges.count), dtype=np.complex128) if spectra else None)
     freqs = np.array([header.frequency_at(k) for k in range(1, top + 1)])
-    spectra, status = medium.bank_spectra(header.ranges.ranges(), freqs, opt or Integration(), raise_on_error=False)
+    payload, status = medium.bank_payload(header.ranges.ranges(), freqs, 1, header.bins(), opt or Integration(),
+                                          raise_on_error=False)
     bad = np.nonzero(status)[0]
     if len(bad):
         k = int(bad[0]) + 1
@@ -353,12 +356,6 @@ def build_bank(medium, header, max_freq, opt=None, check_range_sampling=True):
         except FkError as e:
             raise FkError(e.status, f"bin {k} ({freqs[bad[0]]:.3f} Hz): {e}") from None
         raise FkError(int(status[bad[0]]), f"bin {k} ({freqs[bad[0]]:.3f} Hz) failed")
-    payload = np.zeros(2 * header.ranges.count * header.bins(), dtype=np.float32)
-    sp = np.ascontiguousarray(np.stack([spectra.real, spectra.imag], axis=-1))
-    st = N.lib().gfk_bank_pack(sp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(freqs),
-                               header.ranges.count, 1, header.bins(),
-                               payload.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
-    if st:
-        raise FkError(st, "bank: packing the payload failed")
-    b.data = payload.reshape(header.ranges.count, header.bins(), 2)
-    return b, spectra
+    sp = medium.bank_spectra(header.ranges.ranges(), freqs, opt or Integration())[0] if spectra else None
+    b.data = payload
+    return b, sp

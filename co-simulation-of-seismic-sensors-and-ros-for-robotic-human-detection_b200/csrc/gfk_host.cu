@@ -1095,6 +1095,59 @@ int gfk_bank_spectra(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, cons
     return st;
 }
 
+int gfk_bank_payload(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const double* ranges, int32_t nr,
+                     const double* freqs, int32_t nf, gfk_integration opt, int32_t first_bin, int32_t bins,
+                     float* payload, int32_t* status_per_f) {
+    if (!ctx) return GFK_EARG;
+    if (!payload || bins <= 0 || first_bin < 0 || nf < 0 || (int64_t)first_bin + nf > bins)
+        return fail(ctx, GFK_EARG, "bank: bins [%d, %d) do not fit a payload of %d bins", first_bin, first_bin + nf,
+                    bins);
+    cudaSetDevice(ctx->device);
+    gfk_plan* p = nullptr;
+    int st = plan_one(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, &p);
+    if (st) return st;
+    st = plan_exec(p);
+    std::vector<int32_t> stv(std::max(p->nf, 1), GFK_OK);
+    int first = GFK_OK;
+    if (!st) first = plan_download(p, nullptr, stv.data());  // statuses only; the first failure in order
+    std::string msg = ctx->last_error;
+    cudaStream_t cs = ctx->stream;
+    float* d_pay = nullptr;
+    const size_t nfloat = (size_t)2 * nr * bins;
+    if (!st) {
+        // failed rows pack as zeros, as the FP64 call returns them
+        for (int f = 0; f < p->nf && !st; f++)
+            if (stv[f] && cudaMemsetAsync(p->d_G + (size_t)f * nr, 0, sizeof(cd) * nr, cs) != cudaSuccess)
+                st = fail(ctx, GFK_ECUDA, "bank: clearing a failed row failed");
+        if (!st && cudaMallocAsync((void**)&d_pay, sizeof(float) * nfloat, cs) != cudaSuccess) {
+            d_pay = nullptr;
+            st = fail(ctx, GFK_ENOMEM, "bank: device payload of %zu bytes", sizeof(float) * nfloat);
+        }
+        if (!st && cudaMemsetAsync(d_pay, 0, sizeof(float) * nfloat, cs) != cudaSuccess)
+            st = fail(ctx, GFK_ECUDA, "bank: clearing the payload failed");
+        if (!st && p->nf > 0) {
+            gfk::launch_bank_pack(cs, p->d_G, p->nf, nr, first_bin, bins, d_pay);
+            ctx->launches++;
+            if (cudaGetLastError() != cudaSuccess) st = fail(ctx, GFK_ECUDA, "bank: packing kernel failed");
+        }
+        if (!st && cudaMemcpyAsync(payload, d_pay, sizeof(float) * nfloat, cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+            st = fail(ctx, GFK_ECUDA, "bank: payload download failed");
+        if (d_pay) cudaFreeAsync(d_pay, cs);
+        if (cudaStreamSynchronize(cs) != cudaSuccess && !st) st = fail(ctx, GFK_ECUDA, "bank: payload download failed");
+    }
+    if (status_per_f)
+        for (int f = 0; f < p->nf; f++) status_per_f[f] = stv[f];
+    if (!st) {
+        st = first;
+        ctx->last_error = msg;
+    }
+    msg = ctx->last_error;
+    plan_free(p);
+    delete p;
+    ctx->last_error = msg;
+    return st;
+}
+
 int gfk_vertical_displacement_multi(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const double* ranges,
                                     int32_t nr, double freq_hz, gfk_integration opt, double* out) {
     int32_t status = 0;

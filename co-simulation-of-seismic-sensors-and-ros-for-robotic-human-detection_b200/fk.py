@@ -225,6 +225,26 @@ class Medium:
         return out[:, 0::2] + 1j * out[:, 1::2], status
 
     # -- helpers -----------------------------------------------------------
+    def bank_payload(self, ranges, freqs, first_bin, bins, opt=None, raise_on_error=True, out=None):
+        """The build ending in the bank file's float32 payload, packed on the
+        device (gfk_bank_payload): [len(ranges), bins, 2] float32 with the
+        spectra at bins first_bin.. and zeros elsewhere; per-frequency status."""
+        opt = opt or Integration()
+        r = np.ascontiguousarray(ranges, dtype=np.float64)
+        f = np.ascontiguousarray(freqs, dtype=np.float64)
+        if out is None:
+            out = np.zeros((len(r), bins, 2), dtype=np.float32)
+        status = np.zeros(len(f), dtype=np.int32)
+        eng = self._engine()
+        with _c_medium(self) as cm:
+            st = N.lib().gfk_bank_payload(eng.ctx, ctypes.byref(cm), ctypes.byref(self._solve()), _dp(r), len(r),
+                                          _dp(f), len(f), opt.c(), int(first_bin), int(bins),
+                                          out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                          status.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        if st and raise_on_error:
+            eng.check(st)
+        return out, status
+
     def _solve(self):
         return N.GfkSolve(int(self.formulation), int(self.quadrature), 1 if self.guard else 0, 0,
                           float(self.omega_imag))

@@ -190,6 +190,18 @@ int gfk_bank_spectra(gfk_ctx *ctx, const gfk_medium *m, const gfk_solve *s,
                      const double *freqs_hz, int32_t nf, gfk_integration opt,
                      double *out, int32_t *status_per_f);
 
+/* The same build ending in the bank file's payload (cmd/geobank/main.go:116-121,
+ * 133-167; internal/bank/format.go:185-193): the
+ * spectra of bins first_bin .. first_bin + nf - 1 (frequencies freqs_hz) are
+ * packed on the device into the float32 range-major payload, [nr][bins]
+ * (re, im) pairs, and only that is downloaded: half the bytes of the FP64
+ * result and no host-side packing. Other bins and failed frequencies hold
+ * zeros. payload: host, 2 * nr * bins floats. Statuses as gfk_bank_spectra. */
+int gfk_bank_payload(gfk_ctx *ctx, const gfk_medium *m, const gfk_solve *s,
+                     const double *ranges_m, int32_t nr, const double *freqs_hz, int32_t nf,
+                     gfk_integration opt, int32_t first_bin, int32_t bins, float *payload,
+                     int32_t *status_per_f);
+
 /* ---- plans: device-resident repeated builds ------------------------------ */
 /* A plan fixes (medium, solve, ranges, frequencies, integration) and owns the
  * device buffers; executing it recomputes everything (layer constants, static

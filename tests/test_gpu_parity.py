@@ -252,7 +252,7 @@ def test_build_and_write_bank(gfk, engine, tmp_path):
                    gfk.RangeGrid(1.0, 10.0, 40), "vertical surface displacement per unit vertical surface point force",
                    "m/N")
     m = gfk.Medium(st, default_q=30, engine=engine)
-    b, spectra = gfk.build_bank(m, h, 100.0)
+    b, spectra = gfk.build_bank(m, h, 100.0, spectra=True)
     path = tmp_path / "g.bank"
     b.write(path)
     r = gfk.open_bank(path)
@@ -577,3 +577,38 @@ def test_split_sum_every_tile_shape(gfk, engine, shape, monkeypatch):
     want, sw = wl.medium(gfk.DUNKIN, engine=engine).bank_spectra(ranges, freqs, opt)
     assert (st == 0).all() and (sw == 0).all()
     assert rel_l2(got, want) < 1e-6
+
+
+def test_bank_payload_packed_on_device(gfk, engine):
+    """gfk_bank_payload: the bank file's float32 range-major payload packed on
+    the device equals the host packing (gfk_bank_pack) of the FP64 spectra,
+    bins outside the computed ones stay zero, and frequencies the reference
+    formulation's guard refuses come back with their status and zero columns,
+    the call returning the first failure as geobank aborts on it."""
+    N = gfk._native
+    st = gfk.Stack([gfk.Layer(2.0, 400, 160, 1600, 20), gfk.Layer(0, 900, 400, 2000, 40)])
+    ranges = np.linspace(1.0, 30.0, 37)
+    bins, first = 300, 5
+    freqs = (np.arange(first, first + 250) * 1.0)  # 5..254 Hz, the guard refuses the top ones
+    for form in (N.DUNKIN, N.REFERENCE_DIRECT):
+        m = gfk.Medium(st, formulation=form, engine=engine)
+        pay, status = m.bank_payload(ranges, freqs, first, bins, raise_on_error=False)
+        spec, sst = m.bank_spectra(ranges, freqs, raise_on_error=False)
+        assert np.array_equal(status, sst)
+        host = np.zeros(2 * len(ranges) * bins, dtype=np.float32)
+        sp = np.ascontiguousarray(np.stack([spec.real, spec.imag], axis=-1))
+        assert N.lib().gfk_bank_pack(sp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(freqs), len(ranges),
+                                     first, bins, host.ctypes.data_as(ctypes.POINTER(ctypes.c_float))) == 0
+        assert np.array_equal(pay.ravel(), host)
+        assert (pay[:, :first] == 0).all() and (pay[:, first + len(freqs):] == 0).all()
+        if form == N.REFERENCE_DIRECT:
+            refused = status == N.EGUARD
+            assert refused.any() and not refused.all()
+            assert (pay[:, first + np.nonzero(refused)[0]] == 0).all()
+            with pytest.raises(gfk.FkError) as e:
+                m.bank_payload(ranges, freqs, first, bins)
+            assert e.value.status == N.EGUARD
+        else:
+            assert (status == 0).all()
+    with pytest.raises(gfk.FkError):
+        gfk.Medium(st, engine=engine).bank_payload(ranges, freqs, 100, bins)  # bins beyond the payload
