@@ -549,7 +549,7 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
         st = dalloc(ctx, &p->d_A, (size_t)4 * p->Mp * p->Kp);
         if (!st) st = dalloc(ctx, &p->d_B, (size_t)4 * p->Np * p->Kp);
         if (!st) st = dalloc(ctx, &p->d_rowexp, (size_t)p->Mp);
-        if (!st) st = dalloc(ctx, &p->d_rowmax, (size_t)2 * max_cnf);
+        if (!st) st = dalloc(ctx, &p->d_rowmax, (size_t)3 * max_cnf);  // row maxima, then finished-block counts
         if (!st && cudaMemsetAsync(p->d_A, 0, (size_t)4 * p->Mp * p->Kp, ctx->stream) != cudaSuccess)
             st = fail(ctx, GFK_ECUDA, "clearing the slice planes failed");
     }
@@ -577,17 +577,25 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
     int nchunks = 0;
     for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
         if (p->chunk_begin[c + 1] > p->chunk_begin[c]) nchunks++;
-    p->launches_per_exec = p->nf > 0 ? (p->tc ? 2 + 3 * nchunks : 2 + 2 * nchunks) : 0;
+    p->launches_per_exec = p->nf > 0 ? 2 + 2 * nchunks : 0;
     if (p->nf > 0 && p->ksplit > 1) p->launches_per_exec += nchunks;
     if (p->fused) p->prop_variant = 0;  // one launch shape; nothing to tune
     *out = p;
     return GFK_OK;
 }
 
-// Times every Dunkin launch shape on a window of up to 256 rows of the first
-// chunk (its middle) and keeps the fastest (64-row windows could not tell
-// shapes 4% apart at full size). The window's integrand rows are
-// recomputed by the real launch afterwards.
+// Where the propagator cuts the digit planes of a chunk of `rows` rows: its
+// maxima in d_rowmax[0, 2 rows), its finished-block counts after them.
+gfk::SliceOut slice_out(const gfk_plan* p, int rows) {
+    return gfk::SliceOut{p->d_rowmax, p->d_rowmax + 2 * (size_t)rows, p->d_rowexp, p->d_A, p->Mp, p->Kp};
+}
+
+// Times every Dunkin launch shape on a window of up to 1024 rows of the first
+// chunk (its middle) and keeps the fastest. Small windows rank the shapes
+// by their launch tails: 64 rows could not tell shapes 4% apart at full size,
+// and 256 rows ranked the shapes with several wavenumber runs per block last
+// although they are the fastest on the graded soil's 2048 rows. The window's
+// integrand rows are recomputed by the real launch afterwards.
 int tune_prop(gfk_plan* p) {
     gfk_ctx* ctx = p->ctx;
     cudaStream_t s = ctx->stream;
@@ -604,12 +612,16 @@ int tune_prop(gfk_plan* p) {
             return GFK_OK;
         }
     const int c0 = p->chunk_begin[0], c1 = p->chunk_begin[1];
-    const int win = std::min(256, c1 - c0);
+    const int win = std::min(1024, c1 - c0);
     if (win <= 0) return GFK_OK;
     const int fb = c0 + (c1 - c0 - win) / 2;
     int cmax = 0;
     for (int f = fb; f < fb + win; f++) cmax = std::max(cmax, p->fd[f].kfar > 0 ? p->fd[f].nk : 0);
     if ((int64_t)win * cmax < 4096) return GFK_OK;  // too little work to tell shapes apart
+    // with the tensor-core sum the shapes are timed with their slicing (the
+    // window's digit planes are cut again by the real launch)
+    const gfk::SliceOut so = slice_out(p, win);
+    if (p->tc) GFK_CUDA(ctx, cudaMemsetAsync(p->d_rowmax, 0, sizeof(unsigned long long) * 3 * win, s));
     cudaEvent_t a, b;
     GFK_CUDA(ctx, cudaEventCreate(&a));
     GFK_CUDA(ctx, cudaEventCreate(&b));
@@ -618,7 +630,7 @@ int tune_prop(gfk_plan* p) {
         for (int v = 0; v < nv; v++) {
             cudaEventRecord(a, s);
             gfk::launch_prop(s, p->d_lc, p->d_media, p->d_fd + fb, p->d_wc2 + fb, win, cmax, p->d_C + fb,
-                             GFK_DUNKIN, p->d_rem, p->d_status + fb, v);
+                             GFK_DUNKIN, p->d_rem, p->d_status + fb, v, p->tc ? &so : nullptr);
             cudaEventRecord(b, s);
             ctx->launches++;
             cudaError_t e = cudaEventSynchronize(b);
@@ -748,14 +760,15 @@ int plan_enqueue(gfk_plan* p, bool timed) {
             if ((st = copy_chunk_out(p, fb, cnf))) return st;
             continue;
         }
-        if (p->tc) GFK_CUDA(ctx, cudaMemsetAsync(p->d_rowmax, 0, sizeof(unsigned long long) * 2 * cnf, s));
+        // the tensor-core sum's digit planes are cut by the propagator itself
+        const gfk::SliceOut so = slice_out(p, cnf);
+        if (p->tc) GFK_CUDA(ctx, cudaMemsetAsync(p->d_rowmax, 0, sizeof(unsigned long long) * 3 * cnf, s));
         if (timed && (st = begin_seg(p, 0, &seg))) return st;
         gfk::launch_prop(s, p->d_lc, p->d_media, p->d_fd + fb, p->d_wc2 + fb, cnf, cmax, p->d_C + fb, form, p->d_rem,
-                         p->d_status + fb, std::max(p->prop_variant, 0), p->tc ? p->d_rowmax : nullptr);
+                         p->d_status + fb, std::max(p->prop_variant, 0), p->tc ? &so : nullptr);
         if (timed && (st = end_seg(p, seg))) return st;
         if (timed && (st = begin_seg(p, 1, &seg))) return st;
         if (p->tc) {
-            gfk::launch_slice_rem(s, p->d_rem, p->g_n, p->Kp, p->Mp, cnf, p->d_rowmax, p->d_rowexp, p->d_A);
             if (timed && p->tc_variant < 0 && (st = tune_tc(p, fb, cnf, dk))) return st;
             if (gfk::launch_quad_tc(s, p->d_A, p->d_B, 2 * cnf, p->nr, p->Mp, p->Np, p->Kp, p->d_rowexp, p->col_exp,
                                     p->d_C + fb, p->d_ranges, dk, p->d_G + (size_t)fb * p->nr, p->d_status + fb,
@@ -771,7 +784,7 @@ int plan_enqueue(gfk_plan* p, bool timed) {
                                     p->d_G + (size_t)fb * p->nr);
         }
         if (timed && (st = end_seg(p, seg))) return st;
-        ctx->launches += 2;
+        ctx->launches += p->tc ? 1 : 2;
         if ((st = copy_chunk_out(p, fb, cnf))) return st;
     }
     GFK_CUDA(ctx, cudaGetLastError());

@@ -130,19 +130,21 @@ void launch_static(cudaStream_t s, const LayerC* lc, const MediumP* media, const
 
 // ------------------------------------------------------------ propagator --
 //
-// One thread per (f, k) (ILP = 1) or per (f, k, k + half-block) pair (ILP = 2,
-// two wavenumbers in lockstep). The block's layer constants are staged in
-// shared memory; every block serves one frequency. Launch shapes are template
+// One thread per (f, k) (ILP = 1) or per (f, k, k + THREADS) pair (ILP = 2,
+// two wavenumbers in lockstep), SWEEPS times over consecutive runs of
+// THREADS x ILP wavenumbers. The block's layer constants are staged in shared
+// memory; every block serves one frequency. Launch shapes are template
 // parameters; the plan times them once and keeps the fastest.
 
-template <int FORM, int THREADS, int MINB, int ILP>
+template <int FORM, int THREADS, int MINB, int ILP, int SWEEPS, bool SLICE>
 __global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict__ lc,
                                                        const MediumP* __restrict__ media,
                                                        const FreqDesc* __restrict__ fd, const cd* __restrict__ wc2,
                                                        const cd* __restrict__ C, cd* __restrict__ rem,
-                                                       int* __restrict__ status,
-                                                       unsigned long long* __restrict__ rowmax) {
+                                                       int* __restrict__ status, SliceOut so) {
     __shared__ LayerC s_lc[kMaxLayers];
+    __shared__ cd s_tile[SLICE ? THREADS * 8 : 1];
+    __shared__ int s_last;
     const int f = blockIdx.y;
     const FreqDesc fdesc = fd[f];
     const MediumP med = media[fdesc.soil];
@@ -153,11 +155,14 @@ __global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict
     const int n = fdesc.kfar > 0 ? fdesc.nk : 0;
     const double d = fdesc.dk;
     const cd c = C[f];
-    const int i0 = blockIdx.x * (THREADS * ILP) + threadIdx.x + 1;
+    const cd w2 = wc2[f];
     cd* row = rem + fdesc.off;
     int bad = 0;
     double mre = 0.0, mim = 0.0;
-    if (i0 <= n) {
+#pragma unroll 1
+    for (int sw = 0; sw < SWEEPS; sw++) {
+        const int i0 = (blockIdx.x * SWEEPS + sw) * (THREADS * ILP) + threadIdx.x + 1;
+        if (i0 > n) break;
         if (FORM == 0) {
             bool ok;
             const double k = (double)i0 * d;
@@ -166,25 +171,25 @@ __global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict
             cd r = k * u - c;
             if (!finite_cd(r)) { bad |= kStNonfinite; r = mk(0.0); }
             row[i0 - 1] = r;
-            mre = fabs(r.re); mim = fabs(r.im);
+            mre = fmax(mre, fabs(r.re)); mim = fmax(mim, fabs(r.im));
         } else if (ILP == 1) {
             const double k = (double)i0 * d;
-            const cd u = dunkin_u(s_lc, nl, wc2[f], k, mu_ref);
+            const cd u = dunkin_u(s_lc, nl, w2, k, mu_ref);
             cd r = k * u - c;
             if (!finite_cd(r)) { bad |= kStNonfinite; r = mk(0.0); }
             row[i0 - 1] = r;
-            mre = fabs(r.re); mim = fabs(r.im);
+            mre = fmax(mre, fabs(r.re)); mim = fmax(mim, fabs(r.im));
         } else {
             const int i1 = i0 + THREADS;
             const bool has1 = i1 <= n;
             const double k0 = (double)i0 * d;
             const double k1 = has1 ? (double)i1 * d : k0;
             cd u0, u1;
-            dunkin_u2(s_lc, nl, wc2[f], k0, k1, mu_ref, u0, u1);
+            dunkin_u2(s_lc, nl, w2, k0, k1, mu_ref, u0, u1);
             cd r0 = k0 * u0 - c;
             if (!finite_cd(r0)) { bad |= kStNonfinite; r0 = mk(0.0); }
             row[i0 - 1] = r0;
-            mre = fabs(r0.re); mim = fabs(r0.im);
+            mre = fmax(mre, fabs(r0.re)); mim = fmax(mim, fabs(r0.im));
             if (has1) {
                 cd r1 = k1 * u1 - c;
                 if (!finite_cd(r1)) { bad |= kStNonfinite; r1 = mk(0.0); }
@@ -192,52 +197,89 @@ __global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict
                 mre = fmax(mre, fabs(r1.re)); mim = fmax(mim, fabs(r1.im));
             }
         }
-        if (bad) atomicOr(status + f, bad);
     }
-    if (rowmax) {  // per-row maxima for the integer slicing of the tensor-core sum
+    if (bad) atomicOr(status + f, bad);
+    if constexpr (SLICE) {
+        // The tensor-core sum's integer slicing, by the row's last block: the
+        // row's maxima (the bits of a non-negative double order like the value),
+        // then a device-scope fence and the row's count of finished blocks; the
+        // block that finishes the row slices it while it is still in L2. No block
+        // waits for another. (The pattern of a grid barrier's arrival: block
+        // barrier, one thread's fence, the atomic count.)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             mre = fmax(mre, __shfl_xor_sync(0xffffffffu, mre, o));
             mim = fmax(mim, __shfl_xor_sync(0xffffffffu, mim, o));
         }
         if ((threadIdx.x & 31) == 0) {
-            atomicMax(rowmax + 2 * f, (unsigned long long)__double_as_longlong(mre));
-            atomicMax(rowmax + 2 * f + 1, (unsigned long long)__double_as_longlong(mim));
+            atomicMax(so.rowmax + 2 * f, (unsigned long long)__double_as_longlong(mre));
+            atomicMax(so.rowmax + 2 * f + 1, (unsigned long long)__double_as_longlong(mim));
         }
+        // the barrier orders every thread's stores before thread 0's fence
+        // (cumulative), which orders them before the count
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            const bool last = atomicAdd(so.done + f, 1ull) == (unsigned long long)(gridDim.x - 1);
+            if (last) __threadfence();
+            s_last = last;
+        }
+        __syncthreads();
+        if (!s_last) return;
+        const unsigned long long b0 = __ldcg(so.rowmax + 2 * f), b1 = __ldcg(so.rowmax + 2 * f + 1);
+        const int e[2] = {slice_exp(__longlong_as_double((long long)b0)), slice_exp(__longlong_as_double((long long)b1))};
+        if (threadIdx.x == 0) {
+            so.row_exp[2 * f] = e[0];
+            so.row_exp[2 * f + 1] = e[1];
+            so.done[f] = 0;  // every block of the row has counted: ready for the next launch
+        }
+        // a row with no device work (both maxima 0) slices to zeros without
+        // reading its integrand slot
+        slice_row<THREADS>(row, n, b0 != 0 || b1 != 0, e, so, f, s_tile);
     }
 }
 
 namespace {
+using PropFn = void (*)(const LayerC*, const MediumP*, const FreqDesc*, const cd*, const cd*, cd*, int*, SliceOut);
 struct PropVariant {
-    void (*fn)(const LayerC*, const MediumP*, const FreqDesc*, const cd*, const cd*, cd*, int*, unsigned long long*);
-    int threads, ilp;
+    PropFn fn, fn_slice;  // without and with the fused slicing
+    int threads, ilp, sweeps;
 };
+#define GFK_PROP_SHAPE(T, B, I, S) {k_prop<1, T, B, I, S, false>, k_prop<1, T, B, I, S, true>, T, I, S}
 const PropVariant kDunkinVariants[] = {
-    {k_prop<1, 128, 4, 1>, 128, 1},  // <= 128 registers, 16 warps/SM
-    {k_prop<1, 128, 5, 1>, 128, 1},  // <= 96 registers, 20 warps/SM
-    {k_prop<1, 128, 6, 1>, 128, 1},  // <= 80 registers, 24 warps/SM
-    {k_prop<1, 128, 2, 2>, 128, 2},  // two wavenumbers in lockstep, 8 warps/SM
-    {k_prop<1, 64, 4, 2>, 64, 2},
-    {k_prop<1, 256, 2, 1>, 256, 1},
+    GFK_PROP_SHAPE(128, 4, 1, 1),  // <= 128 registers, 16 warps/SM
+    GFK_PROP_SHAPE(128, 5, 1, 1),  // <= 96 registers, 20 warps/SM
+    GFK_PROP_SHAPE(128, 6, 1, 1),  // <= 80 registers, 24 warps/SM
+    GFK_PROP_SHAPE(128, 2, 2, 1),  // two wavenumbers in lockstep, 8 warps/SM
+    GFK_PROP_SHAPE(64, 4, 2, 1),
+    GFK_PROP_SHAPE(256, 2, 1, 1),
+    GFK_PROP_SHAPE(128, 5, 1, 4),  // four runs of 128 wavenumbers per block
+    GFK_PROP_SHAPE(128, 5, 1, 8),
+    GFK_PROP_SHAPE(128, 4, 1, 4),
+    GFK_PROP_SHAPE(128, 4, 1, 8),
 };
+#undef GFK_PROP_SHAPE
 }  // namespace
 
 int prop_variant_count() { return (int)(sizeof(kDunkinVariants) / sizeof(kDunkinVariants[0])); }
 
 void launch_prop(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2, int nf,
-                 int max_nk, const cd* C, int formulation, cd* rem, int* status, int variant,
-                 unsigned long long* rowmax) {
+                 int max_nk, const cd* C, int formulation, cd* rem, int* status, int variant, const SliceOut* slice) {
     if (nf <= 0 || max_nk <= 0) return;
+    const SliceOut so = slice ? *slice : SliceOut{};
     if (formulation == 0) {
         dim3 grid((max_nk + 127) / 128, nf);
-        k_prop<0, 128, 1, 1><<<grid, 128, 0, s>>>(lc, media, fd, wc2, C, rem, status, rowmax);
+        if (slice)
+            k_prop<0, 128, 1, 1, 1, true><<<grid, 128, 0, s>>>(lc, media, fd, wc2, C, rem, status, so);
+        else
+            k_prop<0, 128, 1, 1, 1, false><<<grid, 128, 0, s>>>(lc, media, fd, wc2, C, rem, status, so);
         return;
     }
     if (variant < 0 || variant >= prop_variant_count()) variant = 0;
     const PropVariant& v = kDunkinVariants[variant];
-    const int per_block = v.threads * v.ilp;
+    const int per_block = v.threads * v.ilp * v.sweeps;
     dim3 grid((max_nk + per_block - 1) / per_block, nf);
-    v.fn<<<grid, v.threads, 0, s>>>(lc, media, fd, wc2, C, rem, status, rowmax);
+    (slice ? v.fn_slice : v.fn)<<<grid, v.threads, 0, s>>>(lc, media, fd, wc2, C, rem, status, so);
 }
 
 // ------------------------------------------------- fused propagator + sum --

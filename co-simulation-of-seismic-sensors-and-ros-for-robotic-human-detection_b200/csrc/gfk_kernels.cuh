@@ -1,6 +1,7 @@
 // gfk_kernels.cuh — kernel declarations shared by the host code.
 #pragma once
 #include <stdint.h>
+#include "gfk_slice.cuh"
 #include "gfk_solver.cuh"
 
 namespace gfk {
@@ -23,19 +24,21 @@ void launch_static(cudaStream_t s, const LayerC* lc, const MediumP* media, const
 
 // rem[fd[f].off + i - 1] = k_i u(k_i, f) - C_f for i = 1..nk, k_i = i dk.
 // `variant` picks one of prop_variant_count() launch shapes of the Dunkin kernel.
+// With `slice` (a shared grid, rows fd[f].off = f nk) each row is also cut into
+// the tensor-core sum's int8 digit planes by the block that finishes it;
+// slice->rowmax and slice->done must be zero for the launch's rows (the
+// launch leaves done at zero again).
 void launch_prop(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2, int nf,
                  int max_nk, const cd* C, int formulation, cd* rem, int* status, int variant = 0,
-                 unsigned long long* rowmax = nullptr);
+                 const SliceOut* slice = nullptr);
 int prop_variant_count();
 
 // Tensor-core quadrature (gfk_quad_tc.cu): exact int8 slices of the integrand
-// rows and of the Hankel weights, tcgen05 kind::i8 GEMM, FP64 recombination.
-// rowmax[2f + p] holds the bits of max_k |part p of rem[f][k]| (set by launch_prop).
+// rows (cut by launch_prop) and of the Hankel weights, tcgen05 kind::i8 GEMM,
+// FP64 recombination.
 int tc_col_exp(double dk);
 void launch_j0_slices(cudaStream_t s, const double* ranges, int nr, int nk, int Kp, int Np, double dk, int col_exp,
                       int8_t* B);
-void launch_slice_rem(cudaStream_t s, const cd* rem, int nk, int Kp, int Mp, int nf, const unsigned long long* rowmax,
-                      int* row_exp, int8_t* A);
 // splits > 1 divides the K blocks among blockIdx.z and writes the head-free
 // partial sums to part [splits][M/2][N]; launch_quad_finish then adds them.
 // variant picks the tile shape (quad_tc_variant_shape: ranges per CTA and

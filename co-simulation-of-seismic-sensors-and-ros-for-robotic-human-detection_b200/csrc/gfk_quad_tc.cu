@@ -6,7 +6,7 @@
 // graded-soil workload), so it needs ~28 significant bits end to end. It is
 // computed with exact integer slices (the Ozaki splitting): each operand row
 // (REM) / column (W) is scaled by a power of two into (-1, 1) and written as
-// four signed 7-bit digits,
+// four signed 7-bit digits (gfk_slice.cuh),
 //     a = 2^e_a sum_s a_s 2^-7(s+1),   b = 2^e_b sum_t b_t 2^-7(t+1),
 // the ten digit products with s + t <= 3 run as int8 x int8 -> s32 tensor-core
 // MMAs (tcgen05.mma kind::i8), accumulated EXACTLY in TMEM per level s + t, and
@@ -237,75 +237,6 @@ __global__ void __launch_bounds__(THREADS, 1)
 
 // ------------------------------------------------------------- slicing --
 
-// Four signed 7-bit digits of x in (-1, 1) scaled by 128: x*128 = d0 + d1/128 + ...
-__device__ __forceinline__ void digits4(double x128, int8_t d[4]) {
-#pragma unroll
-    for (int s = 0; s < 4; s++) {
-        const double q = rint(x128);
-        d[s] = static_cast<int8_t>(q);
-        x128 = (x128 - q) * 128.0;
-    }
-}
-
-// Integrand rows: rows 2f (re) and 2f+1 (im) of the A slice planes [4][Mp][Kp].
-// 16 consecutive wavenumbers per thread, one 16-byte store per slice and part.
-// One block of 128 threads per (row, 2048 wavenumbers): the integrand is read
-// coalesced into shared memory (16-byte units XOR-swizzled within each
-// 16-unit run, so both the row-order stores and each thread's 16-unit reads are
-// free of bank conflicts), then each thread slices 16 consecutive values.
-__global__ void __launch_bounds__(128) k_slice_rem(const cd* __restrict__ rem, int nk, int Kp, int Mp, int nf,
-                                                   const unsigned long long* __restrict__ rowmax,
-                                                   int* __restrict__ row_exp, int8_t* __restrict__ A) {
-    __shared__ cd tile[128 * 16];
-    const int f = blockIdx.y;
-    const int kb = blockIdx.x * (128 * 16);
-    const int t = threadIdx.x;
-    if (f >= nf) return;  // uniform over the block
-    int e[2];
-    double sc[2];
-#pragma unroll
-    for (int p = 0; p < 2; p++) {
-        const double mx = __longlong_as_double((long long)rowmax[2 * f + p]);
-        e[p] = mx > 0 ? ilogb(mx * (128.0 / 127.0)) + 1 : 0;  // 2^e >= mx*128/127
-        sc[p] = ldexp(128.0, -e[p]);
-    }
-    if (blockIdx.x == 0 && t == 0) {
-        row_exp[2 * f] = e[0];
-        row_exp[2 * f + 1] = e[1];
-    }
-    // a row with no device work (its maximum stayed 0) slices to zeros
-    // without reading its integrand slot
-    const bool live = rowmax[2 * f] != 0 || rowmax[2 * f + 1] != 0;
-    const cd* src = rem + (size_t)f * nk;
-#pragma unroll 4
-    for (int i = 0; i < 16; i++) {
-        const int el = t + 128 * i, k = kb + el;
-        const int r = el >> 4, c = el & 15;
-        tile[(r << 4) | (c ^ (r & 7))] = (live && k < nk) ? src[k] : mk(0.0);
-    }
-    __syncthreads();
-    const int k0 = kb + 16 * t;
-    if (k0 >= Kp) return;
-    alignas(16) int8_t out[2][4][16];
-#pragma unroll 4
-    for (int i = 0; i < 16; i++) {
-        const cd v = tile[(t << 4) | (i ^ (t & 7))];
-        int8_t d[4];
-        digits4(v.re * sc[0], d);
-#pragma unroll
-        for (int q = 0; q < 4; q++) out[0][q][i] = d[q];
-        digits4(v.im * sc[1], d);
-#pragma unroll
-        for (int q = 0; q < 4; q++) out[1][q][i] = d[q];
-    }
-#pragma unroll
-    for (int p = 0; p < 2; p++)
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-            *reinterpret_cast<int4*>(A + ((size_t)q * Mp + 2 * f + p) * Kp + k0) =
-                *reinterpret_cast<const int4*>(out[p][q]);
-}
-
 // Hankel weights w_i J0(k_i r_j) dk (fk.go:540-546), transposed to [range][k]
 // and sliced with the shared column exponent: |w J0 dk| <= dk always.
 __global__ void k_j0_slices(const double* __restrict__ ranges, int nr, int nk, int Kp, int Np, double dk,
@@ -313,7 +244,7 @@ __global__ void k_j0_slices(const double* __restrict__ ranges, int nr, int nk, i
     const int n = blockIdx.y;
     const int k0 = (blockIdx.x * blockDim.x + threadIdx.x) * 16;
     if (n >= Np || k0 >= Kp) return;
-    const double sc = ldexp(128.0, -col_exp);
+    const double sc = ldexp(1.0, 28 - col_exp);
     const double r = n < nr ? ranges[n] : 0.0;
     alignas(16) int8_t out[4][16];
 #pragma unroll 4
@@ -325,10 +256,9 @@ __global__ void k_j0_slices(const double* __restrict__ ranges, int nr, int nk, i
             const double w = i == nk ? 0.5 : 1.0;
             wv = (w * j0(k * r)) * dk;
         }
-        int8_t d[4];
-        digits4(wv * sc, d);
+        const uint32_t d = digits4(scaled_int(wv, sc));
 #pragma unroll
-        for (int s = 0; s < 4; s++) out[s][q] = d[s];
+        for (int s = 0; s < 4; s++) out[s][q] = (int8_t)(d >> (8 * s));
     }
 #pragma unroll
     for (int s = 0; s < 4; s++)
@@ -383,12 +313,6 @@ void launch_j0_slices(cudaStream_t s, const double* ranges, int nr, int nk, int 
                       int8_t* B) {
     dim3 grid((Kp / 16 + 127) / 128, Np);
     tc::k_j0_slices<<<grid, 128, 0, s>>>(ranges, nr, nk, Kp, Np, dk, col_exp, B);
-}
-
-void launch_slice_rem(cudaStream_t s, const cd* rem, int nk, int Kp, int Mp, int nf, const unsigned long long* rowmax,
-                      int* row_exp, int8_t* A) {
-    dim3 grid((Kp / 16 + 127) / 128, nf);
-    tc::k_slice_rem<<<grid, 128, 0, s>>>(rem, nk, Kp, Mp, nf, rowmax, row_exp, A);
 }
 
 int quad_tc_splits(int M, int N, int Kp) {
