@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -11,6 +13,25 @@ struct gfk_plan;
 struct gfk_dataset;
 struct gfk_net;
 struct gfk_bank_dev;
+
+// The Hankel weights of a shared-grid wavenumber sum (the tensor-core sum's
+// int8 digit planes, or the plain sum's FP64 table). They depend only on the
+// grid and the ranges, so plans with the same ones share one device copy; it
+// is freed, ordered on the context's stream, when its last holder lets go.
+struct gfk_weights {
+    gfk_ctx* ctx = nullptr;
+    bool tc = false;
+    int n = 0;         // wavenumbers
+    double dk = 0.0;   // wavenumber step
+    std::vector<double> ranges;
+    void* d = nullptr;
+    bool built = false;  // its build has been enqueued on the context's stream
+    bool same(bool tc_, int n_, double dk_, const double* r, int nr) const {
+        return tc == tc_ && n == n_ && dk == dk_ && (int)ranges.size() == nr &&
+               std::equal(ranges.begin(), ranges.end(), r);
+    }
+    ~gfk_weights();
+};
 
 struct gfk_ctx {
     int device = 0;
@@ -32,6 +53,8 @@ struct gfk_ctx {
         int Mp, Np, Kp, variant;
     };
     std::vector<TunedTc> tuned_tc;
+    // the most recent plan's Hankel weights, kept for the next plan
+    std::shared_ptr<gfk_weights> weights;
 };
 
 // Frees every surrogate object the context still holds (gfk_surrogate.cu).

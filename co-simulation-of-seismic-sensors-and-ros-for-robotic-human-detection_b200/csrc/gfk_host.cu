@@ -223,8 +223,8 @@ struct gfk_plan {
     // split-K wavenumber sums for chunks too small to fill the SMs
     int ksplit = 1;
     cd* d_ksum = nullptr;  // [ksplit][rows of a chunk][nr] partial sums
-    int32_t launches_per_exec = 0;  // after the first execute (which also builds the Hankel weights)
-    bool weights_ready = false;
+    int32_t launches_per_exec = 0;  // after the first execute (which may also build the Hankel weights)
+    std::shared_ptr<gfk_weights> wts;  // d_W or d_B, shared with other plans on the same grid and ranges
     int prop_variant = -1;       // Dunkin launch shape; -1 until the first execute tunes it
     std::vector<float> tune_ms;  // per variant, from the tuning run
     int tc_variant = -1;            // tensor-core sum tile shape; -1 until the first execute tunes it
@@ -254,11 +254,12 @@ void plan_free(gfk_plan* p) {
     cudaStream_t s = p->ctx ? p->ctx->stream : nullptr;
     if (p->gexec) cudaGraphExecDestroy(p->gexec);
     if (p->ev_chunk) cudaEventDestroy(p->ev_chunk);
-    void* ptrs[] = {p->d_lp,  p->d_media, p->d_fd, p->d_ranges, p->d_W, p->d_lc,     p->d_wc2,
-                    p->d_C,   p->d_rem,   p->d_G,  p->d_status, p->d_A, p->d_B,      p->d_rowexp,
-                    p->d_rowmax, p->d_partial, p->d_ksum};
+    void* ptrs[] = {p->d_lp, p->d_media,  p->d_fd, p->d_ranges, p->d_lc,     p->d_wc2,    p->d_C,
+                    p->d_rem, p->d_G,     p->d_status, p->d_A, p->d_rowexp, p->d_rowmax, p->d_partial,
+                    p->d_ksum};
     for (void* q : ptrs)
         if (q) cudaFreeAsync(q, s);
+    p->wts.reset();  // the weights go with their last plan (or stay in the context's cache)
     for (auto& sg : p->segs) {
         cudaEventDestroy(sg.a);
         cudaEventDestroy(sg.b);
@@ -274,6 +275,30 @@ int dalloc(gfk_ctx* ctx, T** ptr, size_t count) {
         *ptr = nullptr;
         return fail(ctx, GFK_ENOMEM, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
     }
+    return GFK_OK;
+}
+
+// The plan's Hankel weights: the context's cached copy when the grid and the
+// ranges match, else a new device buffer that becomes the cached one.
+int plan_weights(gfk_plan* p, bool tc, int n, double dk, size_t bytes) {
+    gfk_ctx* ctx = p->ctx;
+    const int nr = (int)p->ranges.size();
+    if (ctx->weights && ctx->weights->same(tc, n, dk, p->ranges.data(), nr)) {
+        p->wts = ctx->weights;
+        return GFK_OK;
+    }
+    auto w = std::make_shared<gfk_weights>();
+    w->ctx = ctx;
+    w->tc = tc;
+    w->n = n;
+    w->dk = dk;
+    w->ranges = p->ranges;
+    if (cudaMallocAsync(&w->d, std::max<size_t>(bytes, 1), ctx->stream) != cudaSuccess) {
+        w->d = nullptr;
+        return fail(ctx, GFK_ENOMEM, "device allocation of %zu bytes of Hankel weights failed", bytes);
+    }
+    ctx->weights = w;
+    p->wts = std::move(w);
     return GFK_OK;
 }
 
@@ -537,7 +562,10 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
     } else if (!st) {
         st = dalloc(ctx, &p->d_rem, (size_t)std::max<int64_t>(cap, 1));
     }
-    if (!st && p->shared && !p->tc) st = dalloc(ctx, &p->d_W, (size_t)g_n * nr);
+    if (!st && p->shared && !p->tc) {
+        if (!(st = plan_weights(p, false, g_n, g_kmax / g_n, sizeof(double) * (size_t)g_n * nr)))
+            p->d_W = static_cast<double*>(p->wts->d);
+    }
     if (!st && p->tc) {
         int max_cnf = 0;
         for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
@@ -546,12 +574,14 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
         p->Np = (nr + 127) / 128 * 128;
         p->Kp = (g_n + 63) / 64 * 64;
         p->col_exp = gfk::tc_col_exp(g_kmax / g_n);
+        // the propagator writes every digit of a chunk's rows up to Kp; rows
+        // past a chunk's 2 cnf are computed by the sum but never stored, so
+        // the planes need no clearing
         st = dalloc(ctx, &p->d_A, (size_t)4 * p->Mp * p->Kp);
-        if (!st) st = dalloc(ctx, &p->d_B, (size_t)4 * p->Np * p->Kp);
+        if (!st && !(st = plan_weights(p, true, g_n, g_kmax / g_n, (size_t)4 * p->Np * p->Kp)))
+            p->d_B = static_cast<int8_t*>(p->wts->d);
         if (!st) st = dalloc(ctx, &p->d_rowexp, (size_t)p->Mp);
         if (!st) st = dalloc(ctx, &p->d_rowmax, (size_t)3 * max_cnf);  // row maxima, then finished-block counts
-        if (!st && cudaMemsetAsync(p->d_A, 0, (size_t)4 * p->Mp * p->Kp, ctx->stream) != cudaSuccess)
-            st = fail(ctx, GFK_ECUDA, "clearing the slice planes failed");
     }
     if (!st && p->shared && !p->fused) {
         int max_cnf = 0;
@@ -731,15 +761,16 @@ int plan_enqueue(gfk_plan* p, bool timed) {
                                 p->d_wc2);
     gfk::launch_static(s, p->d_lc, p->d_media, p->d_fd, p->d_wc2, nf, form, p->d_C, p->d_status);
     // the Hankel weights depend only on the plan's grid and ranges: built by
-    // the first execute, kept for the later ones (and out of a captured graph)
-    if (p->shared && !p->weights_ready) {
+    // the first execute of the first plan that holds them, kept for later
+    // executes and plans (and out of a captured graph)
+    if (p->shared && p->wts && !p->wts->built) {
         if (p->tc)
             gfk::launch_j0_slices(s, p->d_ranges, p->nr, p->g_n, p->Kp, p->Np, p->g_kmax / p->g_n, p->col_exp,
                                   p->d_B);
         else
             gfk::launch_j0_table(s, p->d_ranges, p->nr, p->g_n, p->g_kmax / p->g_n, p->d_W);
         ctx->launches++;
-        p->weights_ready = true;
+        p->wts->built = true;
     }
     if (timed && (st = end_seg(p, seg))) return st;
     ctx->launches += 2;
@@ -910,6 +941,10 @@ int gfk_open(int device, gfk_ctx** out) {
     return GFK_OK;
 }
 
+gfk_weights::~gfk_weights() {
+    if (d) cudaFreeAsync(d, ctx->stream);
+}
+
 int gfk_close(gfk_ctx* ctx) {
     if (!ctx) return GFK_OK;
     cudaSetDevice(ctx->device);
@@ -918,6 +953,7 @@ int gfk_close(gfk_ctx* ctx) {
         delete p;
     }
     ctx->plans.clear();
+    ctx->weights.reset();
     gfk_release_surrogates(ctx);
     gfk_release_banks(ctx);
     if (ctx->copy_stream) {

@@ -244,6 +244,45 @@ def test_plan_is_deterministic_and_timed(gfk, engine):
     p.close()
 
 
+@pytest.mark.parametrize("quadrature", ["fp64", "split"])
+def test_plans_share_hankel_weights(gfk, engine, quadrature):
+    """Plans on the same grid and ranges share one device copy of the Hankel
+    weights: the second plan's first execute builds none, and every plan keeps
+    giving its bank after the plan that built them is closed and after the
+    context's cached copy has moved on to other ranges."""
+    wl = gfk.workloads.single_soil()
+    q = gfk.SPLIT_INT8 if quadrature == "split" else gfk.PLAIN_FP64
+    m = wl.medium(gfk.DUNKIN, engine=engine, quadrature=q)
+    ranges = wl.ranges * 1.37  # not any other test's ranges
+    opt = wl.integration()
+    a = gfk.Plan(m, ranges, wl.freqs, opt, engine=engine)
+    before = engine.kernel_launches()
+    a.execute()
+    assert engine.kernel_launches() - before >= a.launches_per_execute() + 1  # the weights were built
+    a.download()
+    # as many rows as a (the tuned launch shapes are the ones a chose), other frequencies
+    freqs_b = wl.freqs * 1.01
+    b = gfk.Plan(m, ranges, freqs_b, opt, engine=engine)
+    before = engine.kernel_launches()
+    b.execute()
+    assert engine.kernel_launches() - before == b.launches_per_execute()  # and reused
+    got_b, _ = b.download()
+    fp64_b, _ = wl.medium(gfk.DUNKIN, engine=engine).bank_spectra(ranges, freqs_b, opt)
+    assert rel_l2(got_b, fp64_b) < (1e-6 if quadrature == "split" else 1e-12)
+    a.close()
+    other = ranges[:17] * 0.5
+    c = gfk.Plan(m, other, wl.freqs, opt, engine=engine)
+    c.execute()
+    got_c, _ = c.download()
+    ref_c, _ = wl.medium(gfk.DUNKIN, engine=engine).bank_spectra(other, wl.freqs, opt)
+    assert rel_l2(got_c, ref_c) < (1e-6 if quadrature == "split" else 1e-12)
+    b.execute()
+    again, _ = b.download()
+    assert np.array_equal(again, got_b)
+    b.close()
+    c.close()
+
+
 def test_build_and_write_bank(gfk, engine, tmp_path):
     """geobank build on the GPU (cmd/geobank/main.go:51-178) round-tripped
     through the file format."""
