@@ -624,7 +624,8 @@ def batched_leg(gfk, torch, eng, local, rank, world, fp64_peak, steps=3, cpu=Tru
                      "over ranks; the 9.7 GB result and the 4 GB integrand chunks exceed L2, so no flush",
            "soils_per_rank": len(mine), "rows_per_rank": nrows, "cells_per_step": cells_all,
            "plan_build_s": build_s, "gpu_launches": launches,
-           "autotuned": {"propagator_launch_shape": prop_shape[0], "propagator_tuning_ms": prop_shape[1],
+           "autotuned": {"propagator_launch_shape": gfk.prop_shape(prop_shape[0]),
+                         "propagator_tuning_ms": prop_shape[1],
                          "tensor_core_tile": {"ranges_per_cta": tc_shape[0], "stages": tc_shape[1],
                                               "tuning_ms_per_shape": tc_shape[2]}},
            "kernel_ms": {"propagator": prop_ms, "quadrature": quad_ms, "other": other_ms},
@@ -684,6 +685,8 @@ def run_batched(args, gfk, torch, rank, world, local):
     _, _, graph_ms = plan.kernel_times(reset=True)
     clk = clocks.stop()
     step_ms = allmax(graph_ms, world)
+    prop_choice, prop_tune_ms = plan.tuning()
+    tc_tn, tc_stages, tc_tune_ms = plan.quad_shape()
     cells_all = int(allmax(cells, world) if world == 1 else cells * world)
     value = cells_all / (step_ms * 1e-3)
     # end to end: host media and grids in, the FP64 rows back into pinned host memory
@@ -720,6 +723,10 @@ def run_batched(args, gfk, torch, rank, world, local):
                "e2e": {"value": cells_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": layers * 48 + nrows * 8,
                        "d2h_bytes_per_step": nrows * len(ranges) * 16 + nrows * 4, "s_per_step": e2e_s},
                "gpu_launches": launches, "clocks": clk, "plan_build_s": build_s,
+               "autotuned": {"propagator_launch_shape": gfk.prop_shape(prop_choice),
+                             "propagator_tuning_ms": prop_tune_ms,
+                             "tensor_core_tile": {"ranges_per_cta": tc_tn, "stages": tc_stages,
+                                                  "tuning_ms_per_shape": tc_tune_ms}},
                "propagator_fp64_tflops_algorithmic": flops / (step_ms * 1e-3) / 1e12,
                "propagator_executed": {
                    "note": "the fixed count above assumes every finite layer; the solve starts at the shallowest "
@@ -1292,7 +1299,8 @@ def main():
                                 "frac": f_prop / (prop_ms * 1e-3) / 1e12 / fp64_peak},
                 "step_frac_of_fp64_roofline": roof_time / (step_ms * 1e-3),
                 "kernel_ms": {"propagator": prop_ms, "quadrature": quad_ms, "other": other_ms},
-                "propagator_launch_shape": {"chosen": variant, "tuning_ms": tune_ms},
+                "propagator_launch_shape": {"chosen": variant, "shape": gfk.prop_shape(variant),
+                                            "tuning_ms": tune_ms},
                 "quadrature": {"path": "split int8 slices on tcgen05 (10 slice GEMMs)" if quad == gfk.SPLIT_INT8
                                else "plain FP64 on the FP64 tensor cores", "ms": quad_ms,
                                "tile_shape": {"ranges_per_cta": tc_tn, "stages": tc_stages,

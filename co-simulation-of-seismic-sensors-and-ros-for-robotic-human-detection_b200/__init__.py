@@ -7,7 +7,7 @@ in include/gfk.h). There is no CPU fallback.
 from . import _native
 from ._native import DUNKIN, PLAIN_FP64, REFERENCE_DIRECT, SPLIT_INT8
 from .fk import (Batch, Engine, FkError, Grid, Integration, Layer, MAX_LAYER_PHASE, Medium, Plan, SLS, Stack,
-                 default_engine, uniform)
+                 default_engine, prop_shape, uniform)
 from .bank import (Bank, DeviceBank, Header, Provenance, RangeGrid, build_bank, open_bank, range_nyquist)
 from . import workloads
 from . import sobol
@@ -16,5 +16,5 @@ from . import disp
 from . import fdtd
 
 __all__ = ["Batch", "Engine", "FkError", "Grid", "Integration", "Layer", "MAX_LAYER_PHASE", "Medium", "Plan", "SLS",
-           "Stack", "default_engine", "uniform", "Bank", "DeviceBank", "Header", "Provenance", "RangeGrid", "build_bank",
+           "Stack", "default_engine", "prop_shape", "uniform", "Bank", "DeviceBank", "Header", "Provenance", "RangeGrid", "build_bank",
            "open_bank", "range_nyquist", "workloads", "sobol", "surrogate", "disp", "fdtd", "DUNKIN", "REFERENCE_DIRECT", "PLAIN_FP64", "SPLIT_INT8"]

@@ -211,6 +211,7 @@ struct gfk_plan {
     gfk::LayerC* d_lc = nullptr;
     cd *d_wc2 = nullptr, *d_C = nullptr, *d_rem = nullptr, *d_G = nullptr;
     int* d_status = nullptr;
+    unsigned int* d_queue = nullptr;  // the persistent propagator's work queue (zeroed before each launch)
     // fused propagator + sum for a few ranges (no integrand in HBM)
     bool fused = false;
     cd* d_partial = nullptr;
@@ -256,7 +257,7 @@ void plan_free(gfk_plan* p) {
     if (p->ev_chunk) cudaEventDestroy(p->ev_chunk);
     void* ptrs[] = {p->d_lp, p->d_media,  p->d_fd, p->d_ranges, p->d_lc,     p->d_wc2,    p->d_C,
                     p->d_rem, p->d_G,     p->d_status, p->d_A, p->d_rowexp, p->d_rowmax, p->d_partial,
-                    p->d_ksum};
+                    p->d_ksum, p->d_queue};
     for (void* q : ptrs)
         if (q) cudaFreeAsync(q, s);
     p->wts.reset();  // the weights go with their last plan (or stay in the context's cache)
@@ -553,6 +554,7 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
     if (!st) st = dalloc(ctx, &p->d_C, nfa);
     if (!st) st = dalloc(ctx, &p->d_G, nfa * nr);
     if (!st) st = dalloc(ctx, &p->d_status, nfa);
+    if (!st) st = dalloc(ctx, &p->d_queue, 1);
     if (p->fused) {
         int max_cnf = 0;
         for (size_t c = 0; c + 1 < p->chunk_begin.size(); c++)
@@ -658,9 +660,10 @@ int tune_prop(gfk_plan* p) {
     p->tune_ms.assign(nv, INFINITY);
     for (int rep = 0; rep < 2; rep++)
         for (int v = 0; v < nv; v++) {
+            cudaMemsetAsync(p->d_queue, 0, sizeof(unsigned int), s);
             cudaEventRecord(a, s);
             gfk::launch_prop(s, p->d_lc, p->d_media, p->d_fd + fb, p->d_wc2 + fb, win, cmax, p->d_C + fb,
-                             GFK_DUNKIN, p->d_rem, p->d_status + fb, v, p->tc ? &so : nullptr);
+                             GFK_DUNKIN, p->d_rem, p->d_status + fb, v, p->tc ? &so : nullptr, p->d_queue);
             cudaEventRecord(b, s);
             ctx->launches++;
             cudaError_t e = cudaEventSynchronize(b);
@@ -794,9 +797,11 @@ int plan_enqueue(gfk_plan* p, bool timed) {
         // the tensor-core sum's digit planes are cut by the propagator itself
         const gfk::SliceOut so = slice_out(p, cnf);
         if (p->tc) GFK_CUDA(ctx, cudaMemsetAsync(p->d_rowmax, 0, sizeof(unsigned long long) * 3 * cnf, s));
+        if (gfk::prop_variant_persistent(p->prop_variant))
+            GFK_CUDA(ctx, cudaMemsetAsync(p->d_queue, 0, sizeof(unsigned int), s));
         if (timed && (st = begin_seg(p, 0, &seg))) return st;
         gfk::launch_prop(s, p->d_lc, p->d_media, p->d_fd + fb, p->d_wc2 + fb, cnf, cmax, p->d_C + fb, form, p->d_rem,
-                         p->d_status + fb, std::max(p->prop_variant, 0), p->tc ? &so : nullptr);
+                         p->d_status + fb, std::max(p->prop_variant, 0), p->tc ? &so : nullptr, p->d_queue);
         if (timed && (st = end_seg(p, seg))) return st;
         if (timed && (st = begin_seg(p, 1, &seg))) return st;
         if (p->tc) {
@@ -1037,6 +1042,19 @@ int gfk_plan_tuning(const gfk_plan* p, int32_t* variant, float* ms_per_variant, 
     const int n = (int)p->tune_ms.size();
     for (int i = 0; ms_per_variant && i < std::min(n, (int)capacity); i++) ms_per_variant[i] = p->tune_ms[i];
     return n;
+}
+
+int gfk_prop_shape(int32_t variant, int32_t* threads, int32_t* blocks_per_sm, int32_t* wavenumbers_per_thread,
+                   int32_t* runs_per_item, int32_t* persistent) {
+    if (!threads || !blocks_per_sm || !wavenumbers_per_thread || !runs_per_item || !persistent) return GFK_EARG;
+    int t, b, i, r, q;
+    if (!gfk::prop_variant_shape(variant, &t, &b, &i, &r, &q)) return GFK_EARG;
+    *threads = t;
+    *blocks_per_sm = b;
+    *wavenumbers_per_thread = i;
+    *runs_per_item = r;
+    *persistent = q;
+    return GFK_OK;
 }
 
 int gfk_plan_quad_shape(const gfk_plan* p, int32_t* tile_n, int32_t* stages, float* ms_per_shape, int32_t capacity) {

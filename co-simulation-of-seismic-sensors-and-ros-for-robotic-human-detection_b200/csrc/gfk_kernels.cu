@@ -130,28 +130,39 @@ void launch_static(cudaStream_t s, const LayerC* lc, const MediumP* media, const
 
 // ------------------------------------------------------------ propagator --
 //
-// One thread per (f, k) (ILP = 1) or per (f, k, k + THREADS) pair (ILP = 2,
-// two wavenumbers in lockstep), SWEEPS times over consecutive runs of
-// THREADS x ILP wavenumbers. The block's layer constants are staged in shared
-// memory; every block serves one frequency. Launch shapes are template
-// parameters; the plan times them once and keeps the fastest.
+// The work item is (row f, run): one thread per (f, k) (ILP = 1) or per
+// (f, k, k + THREADS) pair (ILP = 2, two wavenumbers in lockstep), SWEEPS
+// times over consecutive stretches of THREADS x ILP wavenumbers; a row has
+// `runs` items. k_prop serves one item per block (blockIdx = (run, f));
+// k_prop_q is persistent: each resident block takes items from a device
+// queue in row order until none are left. The row's layer constants are
+// staged in shared memory. Launch shapes are template parameters; the plan
+// times them once and keeps the fastest.
 
-template <int FORM, int THREADS, int MINB, int ILP, int SWEEPS, bool SLICE>
-__global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict__ lc,
-                                                       const MediumP* __restrict__ media,
-                                                       const FreqDesc* __restrict__ fd, const cd* __restrict__ wc2,
-                                                       const cd* __restrict__ C, cd* __restrict__ rem,
-                                                       int* __restrict__ status, SliceOut so) {
-    __shared__ LayerC s_lc[kMaxLayers];
-    __shared__ cd s_tile[SLICE ? THREADS * 8 : 1];
-    __shared__ int s_last;
-    const int f = blockIdx.y;
+// Shared memory of one propagator block.
+template <int THREADS, bool SLICE>
+struct PropSmem {
+    LayerC lc[kMaxLayers];
+    cd tile[SLICE ? THREADS * 8 : 1];
+    int last, item;
+};
+
+// `stage`: the block's staged layer constants are not row f's (uniform).
+template <int FORM, int THREADS, int ILP, int SWEEPS, bool SLICE>
+__device__ __forceinline__ void prop_item(const LayerC* __restrict__ lc, const MediumP* __restrict__ media,
+                                          const FreqDesc* __restrict__ fd, const cd* __restrict__ wc2,
+                                          const cd* __restrict__ C, cd* __restrict__ rem, int* __restrict__ status,
+                                          const SliceOut& so, int f, int run, int runs, bool stage,
+                                          PropSmem<THREADS, SLICE>& sm) {
+    LayerC* const s_lc = sm.lc;
     const FreqDesc fdesc = fd[f];
     const MediumP med = media[fdesc.soil];
     const int nl = med.count;
     const double mu_ref = med.mu_ref;
-    for (int l = threadIdx.x; l < nl; l += blockDim.x) s_lc[l] = lc[fdesc.lc_off + l];
-    __syncthreads();
+    if (stage) {
+        for (int l = threadIdx.x; l < nl; l += blockDim.x) s_lc[l] = lc[fdesc.lc_off + l];
+        __syncthreads();
+    }
     const int n = fdesc.kfar > 0 ? fdesc.nk : 0;
     const double d = fdesc.dk;
     const cd c = C[f];
@@ -161,7 +172,7 @@ __global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict
     double mre = 0.0, mim = 0.0;
 #pragma unroll 1
     for (int sw = 0; sw < SWEEPS; sw++) {
-        const int i0 = (blockIdx.x * SWEEPS + sw) * (THREADS * ILP) + threadIdx.x + 1;
+        const int i0 = (run * SWEEPS + sw) * (THREADS * ILP) + threadIdx.x + 1;
         if (i0 > n) break;
         if (FORM == 0) {
             bool ok;
@@ -220,12 +231,12 @@ __global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();
-            const bool last = atomicAdd(so.done + f, 1ull) == (unsigned long long)(gridDim.x - 1);
+            const bool last = atomicAdd(so.done + f, 1ull) == (unsigned long long)(runs - 1);
             if (last) __threadfence();
-            s_last = last;
+            sm.last = last;
         }
         __syncthreads();
-        if (!s_last) return;
+        if (!sm.last) return;
         const unsigned long long b0 = __ldcg(so.rowmax + 2 * f), b1 = __ldcg(so.rowmax + 2 * f + 1);
         const int e[2] = {slice_exp(__longlong_as_double((long long)b0)), slice_exp(__longlong_as_double((long long)b1))};
         if (threadIdx.x == 0) {
@@ -235,17 +246,55 @@ __global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict
         }
         // a row with no device work (both maxima 0) slices to zeros without
         // reading its integrand slot
-        slice_row<THREADS>(row, n, b0 != 0 || b1 != 0, e, so, f, s_tile);
+        slice_row<THREADS>(row, n, b0 != 0 || b1 != 0, e, so, f, sm.tile);
+    }
+}
+
+template <int FORM, int THREADS, int MINB, int ILP, int SWEEPS, bool SLICE>
+__global__ __launch_bounds__(THREADS, MINB) void k_prop(const LayerC* __restrict__ lc,
+                                                       const MediumP* __restrict__ media,
+                                                       const FreqDesc* __restrict__ fd, const cd* __restrict__ wc2,
+                                                       const cd* __restrict__ C, cd* __restrict__ rem,
+                                                       int* __restrict__ status, SliceOut so, PropQueue) {
+    __shared__ PropSmem<THREADS, SLICE> sm;
+    prop_item<FORM, THREADS, ILP, SWEEPS, SLICE>(lc, media, fd, wc2, C, rem, status, so, blockIdx.y, blockIdx.x,
+                                                 gridDim.x, true, sm);
+}
+
+// Persistent: items (f, run) in row order from q.next (zero at launch), so a
+// row's items run together and the row is sliced while it is in L2. Blocks
+// never wait for one another; each leaves when the queue is empty.
+template <int FORM, int THREADS, int MINB, int ILP, int SWEEPS, bool SLICE>
+__global__ __launch_bounds__(THREADS, MINB) void k_prop_q(const LayerC* __restrict__ lc,
+                                                         const MediumP* __restrict__ media,
+                                                         const FreqDesc* __restrict__ fd, const cd* __restrict__ wc2,
+                                                         const cd* __restrict__ C, cd* __restrict__ rem,
+                                                         int* __restrict__ status, SliceOut so, PropQueue q) {
+    __shared__ PropSmem<THREADS, SLICE> sm;
+    int cur = -1;
+    for (;;) {
+        __syncthreads();  // every thread is done with the previous item's shared memory
+        if (threadIdx.x == 0) sm.item = (int)atomicAdd(q.next, 1u);
+        __syncthreads();
+        const int item = sm.item;
+        if (item >= q.items) return;
+        const int f = item / q.runs, run = item - f * q.runs;
+        prop_item<FORM, THREADS, ILP, SWEEPS, SLICE>(lc, media, fd, wc2, C, rem, status, so, f, run, q.runs, f != cur,
+                                                     sm);
+        cur = f;
     }
 }
 
 namespace {
-using PropFn = void (*)(const LayerC*, const MediumP*, const FreqDesc*, const cd*, const cd*, cd*, int*, SliceOut);
+using PropFn = void (*)(const LayerC*, const MediumP*, const FreqDesc*, const cd*, const cd*, cd*, int*, SliceOut,
+                        PropQueue);
 struct PropVariant {
     PropFn fn, fn_slice;  // without and with the fused slicing
-    int threads, ilp, sweeps;
+    int threads, minb, ilp, sweeps;
+    bool persistent;  // k_prop_q: one block per resident slot, items from a queue
 };
-#define GFK_PROP_SHAPE(T, B, I, S) {k_prop<1, T, B, I, S, false>, k_prop<1, T, B, I, S, true>, T, I, S}
+#define GFK_PROP_SHAPE(T, B, I, S) {k_prop<1, T, B, I, S, false>, k_prop<1, T, B, I, S, true>, T, B, I, S, false}
+#define GFK_PROP_QUEUE(T, B, I, S) {k_prop_q<1, T, B, I, S, false>, k_prop_q<1, T, B, I, S, true>, T, B, I, S, true}
 const PropVariant kDunkinVariants[] = {
     GFK_PROP_SHAPE(128, 4, 1, 1),  // <= 128 registers, 16 warps/SM
     GFK_PROP_SHAPE(128, 5, 1, 1),  // <= 96 registers, 20 warps/SM
@@ -257,29 +306,74 @@ const PropVariant kDunkinVariants[] = {
     GFK_PROP_SHAPE(128, 5, 1, 8),
     GFK_PROP_SHAPE(128, 4, 1, 4),
     GFK_PROP_SHAPE(128, 4, 1, 8),
+    GFK_PROP_QUEUE(128, 5, 1, 1),  // persistent, items of 128, 256 and 512 wavenumbers
+    GFK_PROP_QUEUE(128, 5, 1, 2),
+    GFK_PROP_QUEUE(128, 5, 1, 4),
 };
+constexpr int kPropVariants = sizeof(kDunkinVariants) / sizeof(kDunkinVariants[0]);
 #undef GFK_PROP_SHAPE
+#undef GFK_PROP_QUEUE
+
+// Resident blocks of a persistent shape on the whole device (once per kernel).
+int persistent_grid(int variant, bool slice) {
+    static int cache[kPropVariants][2] = {};
+    int& g = cache[variant][slice ? 1 : 0];
+    if (g == 0) {
+        const PropVariant& v = kDunkinVariants[variant];
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)(slice ? v.fn_slice : v.fn), v.threads,
+                                                      0);
+        g = std::max(1, sms * std::max(per_sm, 1));
+    }
+    return g;
+}
 }  // namespace
 
-int prop_variant_count() { return (int)(sizeof(kDunkinVariants) / sizeof(kDunkinVariants[0])); }
+int prop_variant_count() { return kPropVariants; }
+
+bool prop_variant_persistent(int variant) {
+    return variant >= 0 && variant < kPropVariants && kDunkinVariants[variant].persistent;
+}
+
+bool prop_variant_shape(int variant, int* threads, int* blocks_per_sm, int* ilp, int* sweeps, int* persistent) {
+    if (variant < 0 || variant >= kPropVariants) return false;
+    const PropVariant& v = kDunkinVariants[variant];
+    *threads = v.threads;
+    *blocks_per_sm = v.minb;
+    *ilp = v.ilp;
+    *sweeps = v.sweeps;
+    *persistent = v.persistent ? 1 : 0;
+    return true;
+}
 
 void launch_prop(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2, int nf,
-                 int max_nk, const cd* C, int formulation, cd* rem, int* status, int variant, const SliceOut* slice) {
+                 int max_nk, const cd* C, int formulation, cd* rem, int* status, int variant, const SliceOut* slice,
+                 unsigned int* queue) {
     if (nf <= 0 || max_nk <= 0) return;
     const SliceOut so = slice ? *slice : SliceOut{};
     if (formulation == 0) {
         dim3 grid((max_nk + 127) / 128, nf);
         if (slice)
-            k_prop<0, 128, 1, 1, 1, true><<<grid, 128, 0, s>>>(lc, media, fd, wc2, C, rem, status, so);
+            k_prop<0, 128, 1, 1, 1, true><<<grid, 128, 0, s>>>(lc, media, fd, wc2, C, rem, status, so, PropQueue{});
         else
-            k_prop<0, 128, 1, 1, 1, false><<<grid, 128, 0, s>>>(lc, media, fd, wc2, C, rem, status, so);
+            k_prop<0, 128, 1, 1, 1, false><<<grid, 128, 0, s>>>(lc, media, fd, wc2, C, rem, status, so, PropQueue{});
         return;
     }
-    if (variant < 0 || variant >= prop_variant_count()) variant = 0;
+    if (variant < 0 || variant >= kPropVariants) variant = 0;
+    if (kDunkinVariants[variant].persistent && !queue) variant = 1;  // no queue: the same block shape, one item each
     const PropVariant& v = kDunkinVariants[variant];
-    const int per_block = v.threads * v.ilp * v.sweeps;
-    dim3 grid((max_nk + per_block - 1) / per_block, nf);
-    (slice ? v.fn_slice : v.fn)<<<grid, v.threads, 0, s>>>(lc, media, fd, wc2, C, rem, status, so);
+    const int per_item = v.threads * v.ilp * v.sweeps;
+    const int runs = (max_nk + per_item - 1) / per_item;
+    const PropFn fn = slice ? v.fn_slice : v.fn;
+    if (v.persistent) {
+        const PropQueue q{queue, nf * runs, runs};
+        fn<<<std::min(persistent_grid(variant, slice != nullptr), nf * runs), v.threads, 0, s>>>(lc, media, fd, wc2, C,
+                                                                                              rem, status, so, q);
+    } else {
+        fn<<<dim3(runs, nf), v.threads, 0, s>>>(lc, media, fd, wc2, C, rem, status, so, PropQueue{});
+    }
 }
 
 // ------------------------------------------------- fused propagator + sum --

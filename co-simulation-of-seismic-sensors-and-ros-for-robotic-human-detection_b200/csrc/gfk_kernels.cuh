@@ -22,16 +22,29 @@ void launch_layer_consts_fl(cudaStream_t s, const LayerP* lp, const MediumP* med
 void launch_static(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2, int nf,
                    int formulation, cd* C, int* status);
 
+// The work queue of the persistent propagator shapes: next (zero at launch)
+// counts the items taken; a row has `runs` items.
+struct PropQueue {
+    unsigned int* next;
+    int items, runs;
+};
+
 // rem[fd[f].off + i - 1] = k_i u(k_i, f) - C_f for i = 1..nk, k_i = i dk.
-// `variant` picks one of prop_variant_count() launch shapes of the Dunkin kernel.
+// `variant` picks one of prop_variant_count() launch shapes of the Dunkin
+// kernel; the persistent ones (prop_variant_persistent) take their items from
+// `queue`, one zeroed word (without one they run as one item per block).
 // With `slice` (a shared grid, rows fd[f].off = f nk) each row is also cut into
 // the tensor-core sum's int8 digit planes by the block that finishes it;
 // slice->rowmax and slice->done must be zero for the launch's rows (the
 // launch leaves done at zero again).
 void launch_prop(cudaStream_t s, const LayerC* lc, const MediumP* media, const FreqDesc* fd, const cd* wc2, int nf,
                  int max_nk, const cd* C, int formulation, cd* rem, int* status, int variant = 0,
-                 const SliceOut* slice = nullptr);
+                 const SliceOut* slice = nullptr, unsigned int* queue = nullptr);
 int prop_variant_count();
+bool prop_variant_persistent(int variant);
+// threads per block, blocks per SM it is compiled for, wavenumbers per thread
+// at a time, 128-wavenumber runs per item, persistent or one item per block
+bool prop_variant_shape(int variant, int* threads, int* blocks_per_sm, int* ilp, int* sweeps, int* persistent);
 
 // Tensor-core quadrature (gfk_quad_tc.cu): exact int8 slices of the integrand
 // rows (cut by launch_prop) and of the Hankel weights, tcgen05 kind::i8 GEMM,

@@ -304,6 +304,18 @@ def default_engine():
     return _default
 
 
+def prop_shape(variant):
+    """gfk_prop_shape: launch shape `variant` of the Dunkin propagator as a dict."""
+    v = [ctypes.c_int32() for _ in range(5)]
+    st = N.lib().gfk_prop_shape(int(variant), *[ctypes.byref(x) for x in v])
+    if st != 0:
+        raise FkError(st, f"no propagator launch shape {variant}")
+    keys = ("threads", "blocks_per_sm", "wavenumbers_per_thread", "runs_per_item")
+    d = {"index": int(variant), **{k: int(x.value) for k, x in zip(keys, v)}}
+    d["persistent"] = bool(v[4].value)
+    return d
+
+
 class Plan:
     """gfk_plan: a fixed (medium, ranges, frequencies, integration) build that
     recomputes everything on the device per execute()."""
@@ -366,6 +378,10 @@ class Plan:
         ms = (ctypes.c_float * 16)()
         n = N.lib().gfk_plan_tuning(self.p, ctypes.byref(v), ms, 16)
         return int(v.value), [float(ms[i]) for i in range(max(n, 0))]
+
+    def prop_shape(self):
+        """The chosen propagator launch shape, described (prop_shape())."""
+        return prop_shape(self.tuning()[0])
 
     def quad_shape(self):
         """(ranges per CTA, pipeline stages, ms per shape) of the tensor-core

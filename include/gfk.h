@@ -222,12 +222,19 @@ int gfk_plan_download(gfk_plan *p, double *out, int32_t *status_per_f);
  * also runs the propagator tuning below). */
 int32_t gfk_plan_launches_per_execute(const gfk_plan *p);
 /* The plan's first execute times each launch shape of the Dunkin propagator
- * (threads per block, blocks per SM, wavenumbers per thread) on a window of
- * its own frequencies and keeps the fastest; the context remembers the choice
+ * (gfk_prop_shape) on a window of up to 1024 of its own frequencies and keeps
+ * the fastest; the context remembers the choice
  * per (layer count, wavenumber count) for later plans and calls. The
  * environment variable GFK_PROP_VARIANT=<index> forces one instead. Writes the chosen index and up
  * to `capacity` measured times (ms); returns the number of shapes. */
 int gfk_plan_tuning(const gfk_plan *p, int32_t *variant, float *ms_per_variant, int32_t capacity);
+/* Launch shape `variant` of the Dunkin propagator: threads per block, the
+ * blocks per SM it is compiled for, wavenumbers per thread at a time, runs of
+ * `threads` wavenumbers per work item, and whether it is persistent (one
+ * block per resident slot taking (row, run) items from a device queue in row
+ * order; otherwise one item per block). GFK_EARG for an unknown index. */
+int gfk_prop_shape(int32_t variant, int32_t *threads, int32_t *blocks_per_sm, int32_t *wavenumbers_per_thread,
+                   int32_t *runs_per_item, int32_t *persistent);
 /* The tensor-core sum's tile shape (GFK_SPLIT_INT8 on a shared grid): the
  * plan's first execute times each shape (ranges per CTA: 128 or 64; pipeline
  * stages: 2-4) on its first row chunk and keeps the fastest; the context

@@ -36,6 +36,27 @@ def test_status_strings(gfk):
     assert lib.gfk_status_string(99) == b"unknown status"
 
 
+def test_propagator_launch_shapes(gfk):
+    """gfk_prop_shape describes every tuned launch shape (host table, no GPU);
+    the persistent ones are among them and unknown indices are refused."""
+    shapes = []
+    v = 0
+    while True:
+        try:
+            shapes.append(gfk.prop_shape(v))
+        except gfk.FkError as e:
+            assert e.status == gfk._native.EARG
+            break
+        v += 1
+    assert len(shapes) >= 10
+    assert any(s["persistent"] for s in shapes) and any(not s["persistent"] for s in shapes)
+    for s in shapes:
+        assert s["threads"] % 32 == 0 and s["blocks_per_sm"] >= 1
+        assert s["wavenumbers_per_thread"] in (1, 2) and s["runs_per_item"] >= 1
+    with pytest.raises(gfk.FkError):
+        gfk.prop_shape(-1)
+
+
 def test_grid_for_matches_oracle(gfk, oracle):
     m = gfk.Medium(gfk.uniform(*CF.LOAM))
     for ranges, f in (([16.0], 60.0), ([1.0, 50.0], 20.0), ([2, 5, 10, 20], 0.5), (list(range(1, 65)), 300.0)):

@@ -283,6 +283,43 @@ def test_plans_share_hankel_weights(gfk, engine, quadrature):
     c.close()
 
 
+def test_every_propagator_shape_gives_the_same_bank(gfk, engine, monkeypatch):
+    """Every tuned launch shape of the propagator (one item per block or
+    persistent over the device queue; 1-8 runs per item; with and without the
+    fused slicing) computes each (row, k) with the same code, so the banks are
+    bit-identical. 1000 wavenumbers fill no run evenly."""
+    wl = gfk.workloads.single_soil()
+    opt = gfk.Integration(1000, 0.0, wl.kmax)
+    freqs = wl.freqs[1::3]
+    shapes = []
+    v = 0
+    while True:
+        try:
+            shapes.append(gfk.prop_shape(v))
+        except gfk.FkError:
+            break
+        v += 1
+    assert any(s["persistent"] for s in shapes)
+    for q in (gfk.PLAIN_FP64, gfk.SPLIT_INT8):
+        m = wl.medium(gfk.DUNKIN, engine=engine, quadrature=q)
+        banks = []
+        for s in shapes:
+            monkeypatch.setenv("GFK_PROP_VARIANT", str(s["index"]))
+            p = gfk.Plan(m, wl.ranges, freqs, opt, engine=engine)
+            p.execute()
+            assert p.tuning()[0] == s["index"]
+            b, st = p.download()
+            assert (st == 0).all()
+            p.execute()  # a second launch on the same queue and counters
+            again, _ = p.download()
+            assert np.array_equal(again, b)
+            banks.append(b)
+            p.close()
+        for s, b in zip(shapes, banks):
+            assert np.array_equal(b, banks[0]), s
+    monkeypatch.delenv("GFK_PROP_VARIANT")
+
+
 def test_build_and_write_bank(gfk, engine, tmp_path):
     """geobank build on the GPU (cmd/geobank/main.go:51-178) round-tripped
     through the file format."""
