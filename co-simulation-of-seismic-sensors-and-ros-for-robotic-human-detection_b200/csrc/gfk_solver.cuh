@@ -184,7 +184,7 @@ GFK_HD Step layer_step(const Terms& t, double zeta) {
     s.mrb = mu * rb;
     s.mra = mu * t.ra;
     s.mx2 = mu * t.x2;
-    s.mq = mu * (1.0 + rb * rb);
+    s.mq = mu * (2.0 - t.eb);  // 1 + rb^2 with rb^2 = 1 - eb exactly
     const cd Eb = cexp_(-(rb * zeta));
     const cd dz = t.delta * zeta;  // (ra - rb) zeta
     cd Ea, W;
