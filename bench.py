@@ -597,8 +597,7 @@ def batched_leg(gfk, torch, eng, local, rank, world, fp64_peak, steps=3, cpu=Tru
     barrier(world)
     t0 = time.perf_counter()
     e2e_plan = gfk.Batch(media(gfk.SPLIT_INT8), freqs, ranges, opt, engine=eng)
-    e2e_plan.execute()
-    e2e_plan.download(out=host_rows)
+    e2e_plan.execute_download(out=host_rows)  # each chunk's rows copied out while the next computes
     e2e_s = allmax(time.perf_counter() - t0, world)
     e2e_plan.close()
     layers = sum(len(st) for st, _ in mine)
@@ -632,7 +631,8 @@ def batched_leg(gfk, torch, eng, local, rank, world, fp64_peak, steps=3, cpu=Tru
            "e2e": {"value": cells_all / e2e_s, "unit": UNIT, "s_per_step": e2e_s, "steps": 1,
                    "h2d_bytes_per_step": layers * 48 + nrows * 8,
                    "d2h_bytes_per_step": nrows * nr * 16 + nrows * 4,
-                   "note": "plan build from host media, execute, download into pinned host memory"},
+                   "note": "plan build from host media, execute with each row chunk downloaded into pinned host "
+                           "memory while the next computes (gfk_plan_execute_download)"},
            "accuracy": accuracy,
            "roofline": {"bound": "fp64", "kernel": "k_prop (Dunkin propagator)", "achieved": ach,
                         "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach / fp64_peak, "traffic": None,
@@ -695,8 +695,7 @@ def run_batched(args, gfk, torch, rank, world, local):
     host_rows = host_rows.view(np.complex128).reshape(nrows_mine, len(ranges))
     t0 = time.perf_counter()
     e2e_plan = gfk.Batch(media, freqs, ranges, opt, engine=eng)
-    e2e_plan.execute()
-    rows, st = e2e_plan.download(out=host_rows)
+    rows, st = e2e_plan.execute_download(out=host_rows)
     e2e_s = allmax(time.perf_counter() - t0, world)
     e2e_plan.close()
     nrows = sum(len(f) for f in freqs)

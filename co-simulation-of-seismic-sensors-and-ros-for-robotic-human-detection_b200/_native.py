@@ -31,6 +31,7 @@ EXPORTS = [
     "gfk_surface_response", "gfk_static_coefficient", "gfk_vertical_displacement",
     "gfk_vertical_displacement_multi", "gfk_bank_spectra", "gfk_bank_payload",
     "gfk_plan_create", "gfk_plan_execute", "gfk_plan_result_device", "gfk_plan_download",
+    "gfk_plan_execute_download",
     "gfk_plan_launches_per_execute", "gfk_plan_tuning", "gfk_prop_shape", "gfk_plan_quad_shape", "gfk_plan_kernel_times", "gfk_plan_destroy",
     "gfk_plan_use_graph", "gfk_batch_create",
     "gfk_bank_pack", "gfk_bank_write", "gfk_vertical_displacement_multi_noalloc",
@@ -127,6 +128,7 @@ def lib():
         "gfk_plan_execute": (ctypes.c_int, [vp]),
         "gfk_plan_result_device": (ctypes.c_int, [vp, P(vp)]),
         "gfk_plan_download": (ctypes.c_int, [vp, P(d), P(i32)]),
+        "gfk_plan_execute_download": (ctypes.c_int, [vp, P(d), P(i32)]),
         "gfk_plan_launches_per_execute": (i32, [vp]),
         "gfk_plan_tuning": (ctypes.c_int, [vp, P(i32), P(ctypes.c_float), i32]),
         "gfk_plan_quad_shape": (ctypes.c_int, [vp, P(i32), P(i32), P(ctypes.c_float), i32]),

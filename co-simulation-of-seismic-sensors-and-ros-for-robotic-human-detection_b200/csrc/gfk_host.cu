@@ -1106,6 +1106,14 @@ int gfk_batch_create(gfk_ctx* ctx, const gfk_medium* media, int32_t nsoil, const
     return st;
 }
 
+static int exec_download_overlapped(gfk_plan* p, double* out, int32_t* status_per_f);
+
+int gfk_plan_execute_download(gfk_plan* p, double* out, int32_t* status_per_f) {
+    if (!p) return GFK_EARG;
+    cudaSetDevice(p->ctx->device);
+    return exec_download_overlapped(p, out, status_per_f);
+}
+
 int gfk_plan_destroy(gfk_plan* p) {
     if (!p) return GFK_OK;
     cudaSetDevice(p->ctx->device);
@@ -1116,6 +1124,50 @@ int gfk_plan_destroy(gfk_plan* p) {
     return GFK_OK;
 }
 
+// True when `out` is page-locked host memory and the context's copy stream
+// exists (created here on first use).
+static bool pinned_with_copy_stream(gfk_ctx* ctx, const void* out) {
+    if (!out) return false;
+    cudaPointerAttributes pa{};
+    const bool pinned = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();  // a pageable pointer is not an error
+    if (!pinned) return false;
+    if (!ctx->copy_stream && cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        ctx->copy_stream = nullptr;
+        return false;
+    }
+    return true;
+}
+
+// One execute with each row chunk copied into `out` (page-locked) on the copy
+// stream as soon as it is computed, then the statuses, failed rows zeroed, as
+// plan_download gives them. Runs the execute as separate launches (a captured
+// graph carries no copies). Plans of one chunk execute, then download.
+static int exec_download_overlapped(gfk_plan* p, double* out, int32_t* status_per_f) {
+    gfk_ctx* ctx = p->ctx;
+    if (p->chunk_begin.size() <= 2 || !pinned_with_copy_stream(ctx, out)) {
+        const int st = plan_exec(p);
+        return st ? st : plan_download(p, out, status_per_f);
+    }
+    if (!p->ev_chunk && cudaEventCreateWithFlags(&p->ev_chunk, cudaEventDisableTiming) != cudaSuccess)
+        return fail(ctx, GFK_ECUDA, "bank download: event creation failed");
+    const bool graph = p->use_graph;
+    p->use_graph = false;
+    p->async_out = out;
+    int st = plan_exec(p);
+    p->async_out = nullptr;
+    p->use_graph = graph;
+    if (cudaStreamSynchronize(ctx->copy_stream) != cudaSuccess && !st) st = fail(ctx, GFK_ECUDA, "bank download failed");
+    if (st) return st;
+    std::vector<int32_t> stv(std::max(p->nf, 1));
+    st = plan_download(p, nullptr, stv.data());
+    for (int f = 0; f < p->nf; f++) {
+        if (stv[f]) std::memset(out + (size_t)2 * p->nr * f, 0, sizeof(double) * 2 * p->nr);
+        if (status_per_f) status_per_f[f] = stv[f];
+    }
+    return st;
+}
+
 int gfk_bank_spectra(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, const double* ranges, int32_t nr,
                      const double* freqs, int32_t nf, gfk_integration opt, double* out, int32_t* status_per_f) {
     if (!ctx) return GFK_EARG;
@@ -1123,38 +1175,12 @@ int gfk_bank_spectra(gfk_ctx* ctx, const gfk_medium* m, const gfk_solve* s, cons
     // Into page-locked host memory a large bank (>= 8 MB) is computed in two
     // row chunks, the first downloaded on a second stream while the second
     // computes (smaller banks lose more to the extra launches than they hide).
-    bool overlap = false;
-    if (out && nf >= 256 && nr >= 1 && (int64_t)nf * nr * 16 >= (int64_t(8) << 20)) {
-        cudaPointerAttributes pa{};
-        if (cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost) overlap = true;
-        cudaGetLastError();  // a pageable pointer is not an error
-    }
-    if (overlap && !ctx->copy_stream &&
-        cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
-        ctx->copy_stream = nullptr;
-        overlap = false;
-    }
+    const bool overlap = out && nf >= 256 && nr >= 1 && (int64_t)nf * nr * 16 >= (int64_t(8) << 20) &&
+                         pinned_with_copy_stream(ctx, out);
     gfk_plan* p = nullptr;
     int st = plan_one(ctx, m, s, ranges, nr, freqs, nf, opt, kGridMulti, &p, overlap ? (nf + 1) / 2 : 0);
     if (st) return st;
-    if (overlap && p->chunk_begin.size() > 2 &&
-        cudaEventCreateWithFlags(&p->ev_chunk, cudaEventDisableTiming) == cudaSuccess)
-        p->async_out = out;
-    st = plan_exec(p);
-    if (p->async_out) {
-        if (cudaStreamSynchronize(ctx->copy_stream) != cudaSuccess && !st)
-            st = fail(ctx, GFK_ECUDA, "bank download failed");
-        if (!st) {  // statuses, and failed rows zeroed, as plan_download gives them
-            std::vector<int32_t> stv(std::max(p->nf, 1));
-            st = plan_download(p, nullptr, stv.data());
-            for (int f = 0; f < p->nf; f++) {
-                if (stv[f]) std::memset(out + (size_t)2 * nr * f, 0, sizeof(double) * 2 * nr);
-                if (status_per_f) status_per_f[f] = stv[f];
-            }
-        }
-    } else if (!st) {
-        st = plan_download(p, out, status_per_f);
-    }
+    st = exec_download_overlapped(p, out, status_per_f);
     std::string msg = ctx->last_error;
     plan_free(p);
     delete p;

@@ -363,6 +363,21 @@ class Plan:
             self.engine.check(st)
         return out, status
 
+    def execute_download(self, raise_on_error=True, out=None):
+        """execute() then download(), with each row chunk copied into `out`
+        while the next one computes when `out` is page-locked (gfk_plan_execute_download)."""
+        shape = (len(self.freqs), len(self.ranges))
+        if out is None:
+            out = np.empty(shape, dtype=np.complex128)
+        elif out.shape != shape or out.dtype != np.complex128 or not out.flags.c_contiguous:
+            raise FkError(N.EARG, f"download buffer must be a C-contiguous complex128 array of shape {shape}")
+        status = np.zeros(len(self.freqs), dtype=np.int32)
+        st = N.lib().gfk_plan_execute_download(self.p, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                               status.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        if st and raise_on_error:
+            self.engine.check(st)
+        return out, status
+
     def statuses(self):
         """Per-row status codes of the last execute, without moving the result."""
         status = np.zeros(len(self.freqs), dtype=np.int32)

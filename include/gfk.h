@@ -218,6 +218,12 @@ int gfk_plan_execute(gfk_plan *p);
 int gfk_plan_result_device(gfk_plan *p, const double **d_out);
 /* Copies the result (and per-frequency status) of the last execute to the host. */
 int gfk_plan_download(gfk_plan *p, double *out, int32_t *status_per_f);
+/* Execute, then download, as the two calls above, except that into
+ * page-locked `out` a plan of several row chunks copies each chunk's rows out
+ * on a second stream while the next chunk computes (the execute then runs as
+ * separate launches, not as the plan's CUDA graph). Same results, statuses
+ * and zeroed failed rows as gfk_plan_execute + gfk_plan_download. */
+int gfk_plan_execute_download(gfk_plan *p, double *out, int32_t *status_per_f);
 /* Number of kernel launches one execute performs (after the first, which
  * also runs the propagator tuning below). */
 int32_t gfk_plan_launches_per_execute(const gfk_plan *p);

@@ -492,6 +492,39 @@ def test_sobol_banks_and_metrics_against_oracle(gfk, engine, oracle):
         assert abs(pk[0] - pk[1]) / pk[1] < 1e-8 and abs(cen[0] - cen[1]) < 1e-6
 
 
+def test_plan_execute_download_overlaps_chunks(gfk, engine):
+    """gfk_plan_execute_download on a plan of two row chunks (71,680 rows: over
+    the 65,535-row grid limit): into page-locked memory each chunk is copied
+    out while the next computes; the bank, statuses and zeroed failed rows
+    equal execute + download, with the plan's CUDA graph on before and after."""
+    import torch
+    wl = gfk.workloads.single_soil()
+    opt = gfk.Integration(256, 0.0, wl.kmax)
+    ranges = np.array([1.0, 3.0, 7.5, 20.0, 41.0])
+    freqs = wl.freqs.copy()
+    bad = freqs.copy()
+    bad[17] = -5.0
+    media = [wl.medium(gfk.DUNKIN, engine=engine, quadrature=gfk.SPLIT_INT8) for _ in range(140)]
+    fl = [bad if i == 70 else freqs for i in range(140)]
+    p = gfk.Batch(media, fl, ranges, opt, engine=engine)
+    p.use_graph(True)
+    p.execute()
+    want, sw = p.download(raise_on_error=False)
+    rows = len(p.freqs)
+    assert rows == 140 * len(freqs) and (sw != 0).sum() == 1
+    pinned = torch.full((rows, 2 * len(ranges)), 7.0, dtype=torch.float64, pin_memory=True).numpy()
+    pinned = pinned.view(np.complex128)
+    got, sg = p.execute_download(raise_on_error=False, out=pinned)
+    assert np.array_equal(sg, sw) and np.array_equal(got, want)
+    assert (got[70 * len(freqs) + 17] == 0).all()
+    p.execute()  # the captured graph again
+    again, _ = p.download(raise_on_error=False)
+    assert np.array_equal(again, want)
+    plain, _ = p.execute_download(raise_on_error=False)  # pageable memory: execute, then download
+    assert np.array_equal(plain, want)
+    p.close()
+
+
 def test_pinned_bank_download_overlaps_and_matches(gfk, engine):
     """Into page-locked memory gfk_bank_spectra computes a larger bank in row
     chunks and downloads each while the next computes; the bank equals the
