@@ -317,6 +317,17 @@ def test_every_propagator_shape_gives_the_same_bank(gfk, engine, monkeypatch):
             p.close()
         for s, b in zip(shapes, banks):
             assert np.array_equal(b, banks[0]), s
+    # per-frequency grids (GridFor): rows of different lengths in one launch
+    m = gfk.Medium(wl.stack, formulation=gfk.DUNKIN, omega_imag=wl.omega_imag, engine=engine)
+    f2 = wl.freqs[5:300:7]
+    banks = []
+    for s in shapes:
+        monkeypatch.setenv("GFK_PROP_VARIANT", str(s["index"]))
+        b, st = m.bank_spectra(wl.ranges[:9], f2)
+        assert (st == 0).all()
+        banks.append(b)
+    for s, b in zip(shapes, banks):
+        assert np.array_equal(b, banks[0]), s
     monkeypatch.delenv("GFK_PROP_VARIANT")
 
 
