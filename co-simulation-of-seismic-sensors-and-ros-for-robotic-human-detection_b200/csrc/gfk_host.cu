@@ -124,7 +124,8 @@ int check_layer_phase(gfk_ctx* ctx, const gfk_medium* m, double f) {  // fk.go:2
     return GFK_OK;
 }
 
-int grid_for_bounds(const gfk_medium* m, double rmin, double rmax, double f, gfk_integration opt, gfk_grid* out);
+int grid_for_bounds(const gfk_medium* m, double slowest, double rmin, double rmax, double f, gfk_integration opt,
+                    gfk_grid* out);
 
 int grid_for(gfk_ctx* ctx, const gfk_medium* m, const double* ranges, int nr, double f, gfk_integration opt,
              gfk_grid* out) {  // fk.go:464-495
@@ -136,21 +137,25 @@ int grid_for(gfk_ctx* ctx, const gfk_medium* m, const double* ranges, int nr, do
         rmin = std::min(rmin, ranges[i]);
         rmax = std::max(rmax, ranges[i]);
     }
-    return grid_for_bounds(m, rmin, rmax, f, opt, out);
+    return grid_for_bounds(m, slowest_vs(m), rmin, rmax, f, opt, out);
 }
 
-// GridFor's rule once the range bounds are known (a plan computes them once
-// for all its frequencies).
-int grid_for_bounds(const gfk_medium* m, double rmin, double rmax, double f, gfk_integration opt, gfk_grid* out) {
-    const double kbody = kTwoPi * f / slowest_vs(m);
+// GridFor's rule once the range bounds and the medium's slowest shear velocity
+// are known (a plan computes them once per medium, not per frequency). With a
+// fixed sample count the step, and with it the pole Q, does not matter.
+int grid_for_bounds(const gfk_medium* m, double slowest, double rmin, double rmax, double f, gfk_integration opt,
+                    gfk_grid* out) {
+    const double kbody = kTwoPi * f / slowest;
     const double kmf = opt.kmax_factor > 0 ? opt.kmax_factor : 30;
     const double kmax = std::max(opt.kmax > 0 ? opt.kmax : kmf * kbody, 40 / rmin);
-    double dk = kTwoPi / (8 * rmax);
-    const double q = pole_q(m, f);
-    if (kbody > 0 && q > 0) dk = std::min(dk, kbody / (2 * q) / 4);
-    const double nn = std::ceil(kmax / dk);
-    int n = nn > 2.0e9 ? 2000000000 : (int)nn;
-    if (opt.samples > 0) n = opt.samples;
+    int n = opt.samples;
+    if (n <= 0) {
+        double dk = kTwoPi / (8 * rmax);
+        const double q = pole_q(m, f);
+        if (kbody > 0 && q > 0) dk = std::min(dk, kbody / (2 * q) / 4);
+        const double nn = std::ceil(kmax / dk);
+        n = nn > 2.0e9 ? 2000000000 : (int)nn;
+    }
     if (n < 64) n = 64;
     out->kmax = kmax;
     out->samples = n;
@@ -458,7 +463,7 @@ int plan_build(gfk_ctx* ctx, const SoilIn* soils, int nsoil, const gfk_solve* s,
             gfk_grid g{0, 0, 0};
             if (!st && m && m->layers && m->count > 0) {
                 if (mode == kGridMulti) {
-                    st = grid_for_bounds(m, rmin, rmax, fr, opt, &g);  // ranges validated above
+                    st = grid_for_bounds(m, slowest, rmin, rmax, fr, opt, &g);  // ranges validated above
                 } else {  // Medium.VerticalDisplacement's own rule (fk.go:407-421)
                     const double kbody = kTwoPi * fr / slowest;
                     const double kmf = opt.kmax_factor > 0 ? opt.kmax_factor : 30;
