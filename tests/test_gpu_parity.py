@@ -317,6 +317,18 @@ def test_every_propagator_shape_gives_the_same_bank(gfk, engine, monkeypatch):
             p.close()
         for s, b in zip(shapes, banks):
             assert np.array_equal(b, banks[0]), s
+    # one row of the smallest grid (64 wavenumbers, less than one item of any shape)
+    tiny = []
+    for q in (gfk.PLAIN_FP64, gfk.SPLIT_INT8):
+        m = wl.medium(gfk.DUNKIN, engine=engine, quadrature=q)
+        for s in shapes:
+            monkeypatch.setenv("GFK_PROP_VARIANT", str(s["index"]))
+            b, st = m.bank_spectra(wl.ranges[:40], wl.freqs[100:101], gfk.Integration(64, 0.0, wl.kmax))
+            assert (st == 0).all() and np.isfinite(b).all()
+            tiny.append((q, b))
+    for q, b in tiny:
+        ref = next(x for qq, x in tiny if qq == q)
+        assert np.array_equal(b, ref)
     # per-frequency grids (GridFor): rows of different lengths in one launch
     m = gfk.Medium(wl.stack, formulation=gfk.DUNKIN, omega_imag=wl.omega_imag, engine=engine)
     f2 = wl.freqs[5:300:7]
