@@ -1293,7 +1293,7 @@ def main():
                 "algorithmic_flops": {"propagator_fixed": f_prop, "propagator_executed": f_exec,
                                       "quadrature": f_quad},
                 "mean_layers_propagated": l_exec, "finite_layers": lfin,
-                "fixed_count": {"note": "the same launch credited with every finite layer (the survey's count)",
+                "fixed_count": {"note": "the same launch credited with every finite layer (700 flops each) + 300 per (f, k)",
                                 "tflops": f_prop / (prop_ms * 1e-3) / 1e12,
                                 "frac": f_prop / (prop_ms * 1e-3) / 1e12 / fp64_peak},
                 "step_frac_of_fp64_roofline": roof_time / (step_ms * 1e-3),

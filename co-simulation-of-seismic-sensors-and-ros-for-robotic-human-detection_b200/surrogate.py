@@ -3,7 +3,7 @@
 The reference has no learned component; this module serves the Sobol and
 sweep workloads (py/analysis/sobol.py, internal/sweep) with a network trained
 on banks the batched solver produces, the plain GPU f-k solve being both its
-fallback and the judge of its error.
+fallback and the measure of its error.
 
 Soil family (the 11 scalars): three finite layers over a half-space drawn
 from the batched-soil ranges (Vs log-uniform 80-600 m/s, Vp/Vs uniform 1.7-3,
