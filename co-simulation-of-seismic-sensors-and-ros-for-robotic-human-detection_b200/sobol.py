@@ -479,7 +479,7 @@ def _solve_rows(params, bins_per_soil, setup, engine, batch_soils, nk=NK, kmax=K
 def run_surrogate(engine, nets, n=16384, seed=0, setup=None, threshold=0.01, batch_soils=20000, gate="rows",
                   chunk_soils=32768, amp_threshold=0.001):
     """The Sobol run with the surrogate answering and the plain GPU f-k solve
-    as fallback and judge.
+    as fallback and as the measure of its error.
 
     gate="rows": every network predicts each soil's spectrum at the sensor;
     the ensemble mean answers, except on the rows (soil, bin) where the
