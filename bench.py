@@ -314,7 +314,8 @@ def config_of(wl, note):
     else:
         soil = ("10 finite 0.8 m layers (Vs 120->600 m/s, Vp=2Vs, rho 1600->2100, Qs 10->60, Qp=2Qs) over a "
                 "half-space")
-        l2 = "intermediates (537 MB integrand, 134 MB J0 table) exceed L2; L2 also flushed (256 MiB write) between timed steps"
+        l2 = ("intermediates (537 MB integrand, 268 MB int8 digit planes; 134 MB J0 table on the FP64 path) exceed L2; "
+              "L2 also flushed (256 MiB write) between timed steps")
     return {"workload": f"{wl.name}: {soil}; {len(wl.freqs)} bins 0-500 Hz (fs 1 kHz), "
                         f"{wl.samples} wavenumbers to {wl.kmax:.1f} rad/m, {len(wl.ranges)} ranges "
                         f"{wl.ranges[0]:g}-{wl.ranges[-1]:g} m, w_I = pi/T",
