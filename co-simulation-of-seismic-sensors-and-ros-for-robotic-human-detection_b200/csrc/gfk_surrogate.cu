@@ -247,12 +247,14 @@ int enqueue_fwd_bwd(gfk_net* n) {
         SG_TRY(gemm(n, M::kBwdData, n->dZ[l], n->L[l].wt, B, n->L[l].in, kW, 1, g));
         SG_TRY(wgrad(l - 1));
     }
-    SG_CUDA(n->ctx, cudaEventRecord(n->ev_join, n->side));
-    SG_CUDA(n->ctx, cudaStreamWaitEvent(s, n->ev_join, 0));
+    // the bias gradients need only dZ^T, all written on this stream by now:
+    // they run beside the side stream's last weight-gradient GEMMs
     const bf16* dzt[kLayers];
     for (int l = 0; l < kLayers; l++) dzt[l] = n->dZT[l];
     M::launch_bias_grad(s, dzt, kLayers, B, n->gb);
     n->ctx->launches++;
+    SG_CUDA(n->ctx, cudaEventRecord(n->ev_join, n->side));
+    SG_CUDA(n->ctx, cudaStreamWaitEvent(s, n->ev_join, 0));
     return GFK_OK;
 }
 
