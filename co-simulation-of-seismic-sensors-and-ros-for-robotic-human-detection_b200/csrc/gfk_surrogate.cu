@@ -213,7 +213,7 @@ int gemm(gfk_net* n, int mode, const bf16* A, const bf16* Bm, int rowsA, int row
 
 // Forward and backward of one batch already in X, XT, Y; gradient partials
 // in L[].part, gb, gpart; loss partials in lpart.
-int enqueue_fwd_bwd(gfk_net* n) {
+int enqueue_fwd_bwd(gfk_net* n, bool train_step) {
     cudaStream_t s = n->ctx->stream;
     const int B = n->B;
     for (int l = 0; l < kLayers; l++) {
@@ -247,12 +247,18 @@ int enqueue_fwd_bwd(gfk_net* n) {
         SG_TRY(gemm(n, M::kBwdData, n->dZ[l], n->L[l].wt, B, n->L[l].in, kW, 1, g));
         SG_TRY(wgrad(l - 1));
     }
-    // the bias gradients need only dZ^T, all written on this stream by now:
-    // they run beside the side stream's last weight-gradient GEMMs
+    // the bias gradients need only dZ^T and the loss history only the head's
+    // loss partials, all written on this stream by now: they run beside the
+    // side stream's last weight-gradient GEMMs. The history slot is the step
+    // counter's, so only a training step (after k_step_begin) records one.
     const bf16* dzt[kLayers];
     for (int l = 0; l < kLayers; l++) dzt[l] = n->dZT[l];
     M::launch_bias_grad(s, dzt, kLayers, B, n->gb);
     n->ctx->launches++;
+    if (train_step) {
+        M::launch_loss_hist(s, n->lpart, n->B / M::kHeadRows, n->B, n->d_ts, n->hist, kHistCap);
+        n->ctx->launches++;
+    }
     SG_CUDA(n->ctx, cudaEventRecord(n->ev_join, n->side));
     SG_CUDA(n->ctx, cudaStreamWaitEvent(s, n->ev_join, 0));
     return GFK_OK;
@@ -292,10 +298,9 @@ int enqueue_step(gfk_net* n, const gfk_dataset* d) {
     b.C = n->Cw;
     M::launch_batch(s, b);
     n->ctx->launches += 2;
-    SG_TRY(enqueue_fwd_bwd(n));
-    M::launch_loss_hist(s, n->lpart, n->B / M::kHeadRows, n->B, n->d_ts, n->hist, kHistCap);
+    SG_TRY(enqueue_fwd_bwd(n, true));
     M::launch_adam(s, n->adam, n->nparam);
-    n->ctx->launches += 3;
+    n->ctx->launches += 2;
     return GFK_OK;
 }
 
@@ -945,7 +950,7 @@ int gfk_net_probe(gfk_net* n, const float* X, const float* Y, const float* coeff
         cw[2 * b + 1] = coeffs ? coeffs[2 * b + 1] : (std::isnan(Y[2 * b + 1]) ? 0.0f : n->cfg.phase_weight);
     }
     SG_CUDA(ctx, cudaMemcpyAsync(n->Cw, cw.data(), cw.size() * 4, cudaMemcpyHostToDevice, s));
-    SG_TRY(enqueue_fwd_bwd(n));
+    SG_TRY(enqueue_fwd_bwd(n, false));
     M::launch_grad_flat(s, n->adam, n->nparam, n->gflat);
     ctx->launches++;
     SG_CUDA(ctx, cudaGetLastError());
