@@ -13,6 +13,7 @@
 #include "gfk_kernels.cuh"
 
 #include <algorithm>
+#include <atomic>
 
 namespace gfk {
 
@@ -314,10 +315,12 @@ constexpr int kPropVariants = sizeof(kDunkinVariants) / sizeof(kDunkinVariants[0
 #undef GFK_PROP_SHAPE
 #undef GFK_PROP_QUEUE
 
-// Resident blocks of a persistent shape on the whole device (once per kernel).
+// Resident blocks of a persistent shape on the whole device (queried once per
+// kernel; concurrent first calls compute the same value).
 int persistent_grid(int variant, bool slice) {
-    static int cache[kPropVariants][2] = {};
-    int& g = cache[variant][slice ? 1 : 0];
+    static std::atomic<int> cache[kPropVariants][2] = {};
+    std::atomic<int>& slot = cache[variant][slice ? 1 : 0];
+    int g = slot.load(std::memory_order_relaxed);
     if (g == 0) {
         const PropVariant& v = kDunkinVariants[variant];
         int dev = 0, sms = 0, per_sm = 0;
@@ -326,6 +329,7 @@ int persistent_grid(int variant, bool slice) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)(slice ? v.fn_slice : v.fn), v.threads,
                                                       0);
         g = std::max(1, sms * std::max(per_sm, 1));
+        slot.store(g, std::memory_order_relaxed);
     }
     return g;
 }
