@@ -680,8 +680,10 @@ int quad_gemm_splits(int nf, int nk, int nr) {
 
 namespace {
 template <class K>
-void set_smem_once(K kernel, int bytes, bool* done) {
-    if (!*done) *done = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+void set_smem_once(K kernel, int bytes, std::atomic<bool>* done) {
+    if (!done->load(std::memory_order_relaxed) &&
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess)
+        done->store(true, std::memory_order_relaxed);
 }
 }  // namespace
 
@@ -692,7 +694,7 @@ void launch_quad_gemm(cudaStream_t s, const cd* rem, const double* W, const cd* 
     cd* const p = splits > 1 ? part : nullptr;
     // a failed attribute call leaves the launch to fail, and the caller's
     // cudaGetLastError to report it
-    static bool a8 = false, a4 = false;
+    static std::atomic<bool> a8{false}, a4{false};
     if (nr > 64) {
         set_smem_once(k_quad_gemm<8>, qd::smem_bytes<8>(), &a8);
         dim3 grid((nr + 127) / 128, (2 * nf + qd::BM - 1) / qd::BM, splits);

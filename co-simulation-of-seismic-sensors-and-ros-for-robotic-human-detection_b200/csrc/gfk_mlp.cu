@@ -21,6 +21,7 @@
 #include <cudaTypedefs.h>
 #include <math_constants.h>
 
+#include <atomic>
 #include <utility>
 
 #include "gfk_kernels.cuh"
@@ -936,9 +937,11 @@ void launch_mode(cudaStream_t s, const CUtensorMap& ta, const CUtensorMap& tb, d
 }  // namespace
 
 int prepare_gemm() {
-    static bool done = false;
-    if (!done) done = set_attr<kFwdTrain>() && set_attr<kFwdInfer>() && set_attr<kBwdData>() && set_attr<kWgrad>();
-    return done ? 0 : 3;
+    static std::atomic<bool> done{false};
+    if (!done.load(std::memory_order_relaxed) && set_attr<kFwdTrain>() && set_attr<kFwdInfer>() &&
+        set_attr<kBwdData>() && set_attr<kWgrad>())
+        done.store(true, std::memory_order_relaxed);
+    return done.load(std::memory_order_relaxed) ? 0 : 3;
 }
 
 int launch_gemm(cudaStream_t s, int mode, const bf16* A, const bf16* B, int rowsA, int rowsB, int ktotal, int splits,

@@ -67,20 +67,24 @@ unsigned long long g_scratch_ctx[256] = {0};      // ID of the context that addr
 unsigned long long current_context_id() {
     using GetCurrent = CUresult (*)(CUcontext*);
     using GetId = CUresult (*)(CUcontext, unsigned long long*);
-    static GetCurrent get_current = nullptr;
-    static GetId get_id = nullptr;
-    static bool looked_up = false;
-    if (!looked_up) {
+    struct Entry {
+        GetCurrent get_current = nullptr;
+        GetId get_id = nullptr;
+    };
+    static const Entry e = [] {  // looked up once, thread-safely (a function-local static)
+        Entry r;
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            get_current = reinterpret_cast<GetCurrent>(p);
+            r.get_current = reinterpret_cast<GetCurrent>(p);
         if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            get_id = reinterpret_cast<GetId>(p);
-        looked_up = true;
-    }
+            r.get_id = reinterpret_cast<GetId>(p);
+        return r;
+    }();
+    const GetCurrent get_current = e.get_current;
+    const GetId get_id = e.get_id;
     if (!get_current || !get_id) return 0;
     CUcontext c = nullptr;
     unsigned long long id = 0;

@@ -28,6 +28,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "gfk_kernels.cuh"
 #include "gfk_tc.cuh"
@@ -288,7 +289,7 @@ bool make_map(CUtensorMap* map, const int8_t* base, int rows_total, int Kp, int 
 struct TcVariant {
     void (*fn)(const CUtensorMap, const CUtensorMap, tc::Args);
     int tn, stages, smem;
-    bool attr;
+    std::atomic<bool> attr;  // the shared-memory attribute is set (once per process)
 };
 TcVariant g_tc_variants[] = {
     {tc::k_quad_tc<128, 3>, 128, 3, tc::Shape<128, 3>::SMEM_BYTES, false},
@@ -335,9 +336,9 @@ int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int 
     if (splits > Kp / tc::BK) return 1;
     CUtensorMap ta, tb;
     if (!make_map(&ta, A, tc::S * Mp, Kp, tc::BM) || !make_map(&tb, B, tc::S * Np, Kp, v.tn)) return 2;
-    if (!v.attr) {
+    if (!v.attr.load(std::memory_order_relaxed)) {
         if (cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, v.smem) != cudaSuccess) return 3;
-        v.attr = true;
+        v.attr.store(true, std::memory_order_relaxed);
     }
     tc::Args a{M, N, Mp, Np, Kp, row_exp, col_exp, C, ranges, dk, G, status, splits > 1 ? part : nullptr,
                wait_cycles > 0 ? wait_cycles : tc::kWaitCycles, starve};
