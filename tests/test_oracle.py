@@ -240,3 +240,51 @@ def test_layered_causality_known_answers(oracle):
     spectra, status = oracle.bank_spectra(m, CC.RANGES, freqs)
     assert (status == 0).all()
     CC.check_against_logged(CC.metrics(spectra), KA["causality_precursor"])
+
+
+def test_split_sum_restatement_on_the_oracle_integrand(oracle, gfk):
+    """The tensor-core sum's definition (oracle/split_oracle.py: one rounding to
+    28 bits per operand, balanced base-128 digits, exact level sums up to
+    s + t = 3) on the graded soil's own integrand from the oracle: the digits
+    rebuild their integers exactly, every sum stays inside the rigorous bound
+    K 2^(e_a + e_b - 27), and the whole result is within the 1e-6 bar of the
+    FP64 sum (fk.go:534-546 with the oracle's J0)."""
+    import split_oracle as S
+    from conftest import as_tuples, rel_l2
+    rng = np.random.default_rng(5)
+    lim = 127 * 2 ** 21  # |x 2^(28 - e)| <= 127/128 2^28
+    n = np.concatenate([np.array([0, 1, -1, 63, 64, -64, -65, lim, -lim, lim - 1, 1 - lim]),
+                        rng.integers(-lim, lim + 1, 20000)])
+    d = S.digits(n)
+    assert np.array_equal(d[0] * 2 ** 21 + d[1] * 2 ** 14 + d[2] * 2 ** 7 + d[3], n)
+    assert all(((x >= -64) & (x < 64)).all() for x in d[1:]) and (np.abs(d[0]) <= 127).all()
+    mx = np.array([1.0, 127 / 128, 0.5, 3.0, 1e-300, 7e12])
+    e = S.exponent(mx)
+    y = mx * (128 / 127)
+    assert (np.ldexp(1.0, e) > y).all() and (np.ldexp(1.0, e - 1) <= y).all()  # e = ilogb(y) + 1
+    assert S.exponent(0.0) == 0
+
+    wl = gfk.workloads.graded_soil()
+    st = as_tuples(wl.stack)
+    nk = 2048
+    dk = wl.kmax / nk
+    k = np.arange(1, nk + 1) * dk
+    freqs = wl.freqs[[64, 400, 800, 1200, 1600, 2040]]
+    ranges = wl.ranges[::32]
+    vs_min = min(l[2] for l in st)
+    rem = np.empty((len(freqs), nk), dtype=complex)
+    for i, f in enumerate(freqs):
+        kfar = max(200 * 2 * math.pi * f / vs_min, 400 / ranges.min())
+        c = oracle.static_coefficient(st, f, kfar, oracle.DUNKIN, wl.omega_imag)
+        u = np.array([oracle.surface_response(st, kk, f, oracle.DUNKIN, wl.omega_imag) for kk in k])
+        rem[i] = k * u - c
+    w = np.array([[oracle.j0(kk * r) for r in ranges] for kk in k]) * dk
+    w[-1] *= 0.5
+    exact = rem @ w
+    got = S.split_sum(rem, w, dk)
+    for part in (np.real, np.imag):
+        bound = S.error_bound(part(rem), dk, nk)[:, None]
+        assert (np.abs(part(got) - part(exact)) <= bound).all()
+    # heavy cancellation: |sum| far below sum |terms| (the reason 28 bits are needed)
+    assert (np.abs(rem) @ np.abs(w) / np.abs(exact)).max() > 100
+    assert rel_l2(got, exact) < 1e-6
