@@ -342,7 +342,9 @@ int launch_quad_tc(cudaStream_t s, const int8_t* A, const int8_t* B, int M, int 
     }
     tc::Args a{M, N, Mp, Np, Kp, row_exp, col_exp, C, ranges, dk, G, status, splits > 1 ? part : nullptr,
                wait_cycles > 0 ? wait_cycles : tc::kWaitCycles, starve};
-    dim3 grid((N + v.tn - 1) / v.tn, Mp / tc::BM, splits);
+    // row tiles over this launch's M valid rows only: a chunk smaller than the
+    // plan's largest (Mp) would otherwise multiply padding rows it never stores
+    dim3 grid((N + v.tn - 1) / v.tn, (M + tc::BM - 1) / tc::BM, splits);
     v.fn<<<grid, tc::THREADS, v.smem, s>>>(ta, tb, a);
     if (splits > 1) launch_quad_finish(s, part, splits, C, ranges, M >> 1, N, dk, G);
     return 0;
